@@ -1,0 +1,252 @@
+/*
+ * euler_b200 -- C ABI of the B200 (sm_100a) spatial discretization of the 2D Euler ALE
+ * equations on O-grids, a drop-in for the native layer of PyEulerALE v1.1.5.
+ *
+ * The reference reaches its native code through the f2py module
+ * `py_euler_ale.euler_ale.spatial_discretization` (src/spatial_discretization.f90, bound by
+ * meson.build:21-35): 20 procedures plus 4 module variables (aoa, jst_k2, jst_k4, jst_c4,
+ * f90:63-66) that are set before each call (src/py_euler_ale/core.py:258-263). Each entry
+ * point below replaces one of those procedures; the module variables become fields of
+ * `eb_instance`, so calls are reentrant and instances with different parameters can be
+ * batched.
+ *
+ * Conventions
+ *  - All array pointers are DEVICE pointers (FP64). Layouts are the reference's Fortran
+ *    layouts (column-major): vertices / velocities (2, M+1, N+1), states / odes (4, M, N),
+ *    d(odes)/d(states) (4, 4, M, N, 9), d(odes)/d(vertices|velocities) (4, 2, M, N, 4),
+ *    d(odes)/d(mach) (4, 1, M, N), forces (2, N), d(forces)/d(states) (2, 4, N),
+ *    d(forces)/d(vertices) (2, 2, N, 2). Complex arrays are interleaved (re, im) doubles.
+ *  - The states, vertices and velocities are real here: the reference stores them as
+ *    complex128 only to run its complex-step differentiation, and its public API exposes
+ *    their real parts (core.py:159-211).
+ *  - Several grids ("instances") may be packed back to back: instance i owns cells
+ *    [cell_offset, cell_offset + M*N) and vertices [vert_offset, vert_offset + (M+1)(N+1)).
+ *    Per-cell arrays are indexed with the cell offset times the per-cell size (4 for states,
+ *    144 for d(odes)/d(states), ...), per-vertex arrays with the vertex offset times 2, and
+ *    per-wall-face arrays (forces) with the instance's angular offset `wall_offset`.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream). Calls are asynchronous
+ *    unless stated; nothing allocates device memory except where stated.
+ *  - Return value: EB_OK or a negative EB_ERR_* code; eb_last_error() describes it.
+ *  - Grids need M >= 4 radial and N >= 5 angular cells (the 9-point stencil reaches two
+ *    cells in each direction; the reference indexes out of bounds below that).
+ */
+#ifndef EULER_B200_H
+#define EULER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EB_OK 0
+#define EB_ERR_ARG (-1)      /* invalid argument (sizes, null pointer, table) */
+#define EB_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define EB_ERR_NOCONV (-3)   /* an iterative solve hit its iteration limit */
+#define EB_ERR_NAN (-4)      /* a NaN / Inf appeared in a solve */
+
+/* One grid with its flow parameters (104 bytes). */
+typedef struct eb_instance {
+  int32_t M;            /* cells in the radial direction (num_radial) */
+  int32_t N;            /* cells in the angular direction (num_angular) */
+  int64_t cell_offset;  /* first cell of this instance in the packed per-cell arrays */
+  int64_t vert_offset;  /* first vertex of this instance in the packed per-vertex arrays */
+  int64_t wall_offset;  /* first wall face of this instance in the packed per-wall arrays */
+  double mach;          /* free-stream Mach number */
+  double cos_aoa;       /* cos(angle of attack) -- the reference's `aoa` in degrees, f90:253 */
+  double sin_aoa;       /* sin(angle of attack) */
+  double k2, k4, c4;    /* JST constants jst_k2, jst_k4, jst_c4 (f90:64-66) */
+  double chord;         /* coefficient_length (core.py:65) */
+  double xc, zc;        /* coefficient_center (core.py:66) */
+} eb_instance;
+
+/* A set of instances. For a single grid set n_inst = 1, d_table = NULL and fill `single`;
+ * otherwise d_table is a DEVICE array of n_inst instances sorted by cell_offset. */
+typedef struct eb_batch {
+  const eb_instance* d_table;
+  int32_t n_inst;
+  int32_t reserved;
+  int64_t n_cells;      /* total cells over all instances */
+  int64_t n_verts;      /* total vertices over all instances */
+  int64_t n_wall;       /* total wall faces (sum of N) over all instances */
+  eb_instance single;
+} eb_batch;
+
+/* Text of the last error on the calling thread. */
+const char* eb_last_error(void);
+/* Library version string. */
+const char* eb_version(void);
+
+/* ---- residual and forces -------------------------------------------------------------- */
+
+/* set_free_stream_state, f90:471-482: U(:, m, n) = free-stream state of each instance. */
+int eb_set_free_stream_state(const eb_batch* b, double* U, void* stream);
+
+/* compute_odes, f90:496-537: R = R(Ma, U, X, V). V may be NULL (static grid). */
+int eb_compute_odes(const eb_batch* b, const double* X, const double* V, const double* U,
+                    double* R, void* stream);
+
+/* compute_forces, f90:1156-1174: F(:, n) = p(U(:, 1, n)) * normal(X(:, 1, n), X(:, 1, n+1)).
+ * F is real (2, N) per instance at 2*wall_offset. coef (optional, may be NULL) receives per
+ * instance (c_d, c_l, c_m) as core.py:1277-1364 defines them, with the instance's chord and
+ * moment centre; the wall sums are warp-shuffle reductions, one CTA per instance. */
+int eb_compute_forces(const eb_batch* b, const double* X, const double* U, double* F,
+                      double* coef, void* stream);
+
+/* ---- Jacobians (replacing the complex-step procedures) ------------------------------- */
+
+/* compute_odes_wrt_mach, f90:552-593. J: (4, 1, M, N) per instance, 4*cell_offset. */
+int eb_compute_odes_wrt_mach(const eb_batch* b, const double* X, const double* V,
+                             const double* U, double* J, void* stream);
+/* compute_odes_wrt_states, f90:666-750. J: (4, 4, M, N, 9) per instance, 144*cell_offset.
+ * Blocks the reference does not compute (slots reaching past the radial boundary) are 0. */
+int eb_compute_odes_wrt_states(const eb_batch* b, const double* X, const double* V,
+                               const double* U, double* J, void* stream);
+/* compute_odes_wrt_vertices, f90:933-993. J: (4, 2, M, N, 4) per instance, 32*cell_offset. */
+int eb_compute_odes_wrt_vertices(const eb_batch* b, const double* X, const double* V,
+                                 const double* U, double* J, void* stream);
+/* compute_odes_wrt_velocities, f90:1087-1143. Same layout as the vertices. */
+int eb_compute_odes_wrt_velocities(const eb_batch* b, const double* X, const double* V,
+                                   const double* U, double* J, void* stream);
+/* compute_forces_wrt_states, f90:1188-1213. J: (2, 4, N) per instance, 8*wall_offset. */
+int eb_compute_forces_wrt_states(const eb_batch* b, const double* X, const double* U,
+                                 double* J, void* stream);
+/* compute_forces_wrt_vertices, f90:1227-1256. J: (2, 2, N, 2) per instance, 8*wall_offset. */
+int eb_compute_forces_wrt_vertices(const eb_batch* b, const double* X, const double* U,
+                                   double* J, void* stream);
+
+/* ---- Jacobian products (complex vectors, real Jacobians) ------------------------------ */
+
+/* apply_odes_wrt_mach_fwd / _rev, f90:604-650. d_mach: one complex per instance. */
+int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double* d_mach,
+                               double* d_odes, void* stream);
+int eb_apply_odes_wrt_mach_rev(const eb_batch* b, const double* J, const double* d_odes,
+                               double* d_mach, void* stream);
+/* apply_odes_wrt_states_fwd / _rev, f90:825-918. The reverse product gathers the
+ * transposed stencil (no atomics, deterministic). */
+int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const double* d_states,
+                                 double* d_odes, void* stream);
+int eb_apply_odes_wrt_states_rev(const eb_batch* b, const double* J, const double* d_odes,
+                                 double* d_states, void* stream);
+/* apply_odes_wrt_vertices_fwd / _rev, f90:1005-1072 (also used with the velocity
+ * Jacobians, core.py:480-481, 508-509). */
+int eb_apply_odes_wrt_vertices_fwd(const eb_batch* b, const double* J,
+                                   const double* d_vertices, double* d_odes, void* stream);
+int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const double* d_odes,
+                                   double* d_vertices, void* stream);
+/* apply_forces_wrt_states_fwd / _rev, f90:1333-1375. */
+int eb_apply_forces_wrt_states_fwd(const eb_batch* b, const double* J, const double* d_states,
+                                   double* d_forces, void* stream);
+int eb_apply_forces_wrt_states_rev(const eb_batch* b, const double* J, const double* d_forces,
+                                   double* d_states, void* stream);
+/* apply_forces_wrt_vertices_fwd / _rev, f90:1267-1322. */
+int eb_apply_forces_wrt_vertices_fwd(const eb_batch* b, const double* J,
+                                     const double* d_vertices, double* d_forces, void* stream);
+int eb_apply_forces_wrt_vertices_rev(const eb_batch* b, const double* J,
+                                     const double* d_forces, double* d_vertices, void* stream);
+
+/* Matrix-free forward tangent: dR = dR/dU.dU + dR/dX.dX + dR/dV.dV + dR/dMa.dMa in one
+ * stencil pass (forward-mode duals, no stored Jacobian). Complex dU (4,M,N), dX/dV (2,M+1,N+1),
+ * dMa (one complex per instance); any of them may be NULL (zero). R (optional) receives the
+ * residual itself. */
+int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, const double* U,
+                          const double* dU, const double* dX, const double* dV,
+                          const double* dMa, double* dR, double* R, void* stream);
+
+/* ---- BSR form of d(odes)/d(states) --------------------------------------------------- */
+
+/* convert_odes_wrt_states, f90:765-814, for a single instance: data (4, 4, nnzb), 1-based
+ * int32 indices (nnzb) and index_pointers (M*N + 1) exactly as the reference emits them,
+ * nnzb = (9M - 6) N. */
+int eb_convert_odes_wrt_states(const eb_batch* b, const double* J, double* data,
+                               int32_t* indices, int32_t* index_pointers, void* stream);
+/* y = (A - shift*I) x for the BSR matrix A of one instance (complex x, y). */
+int eb_bsr_shifted_spmv(int64_t n_rows, const double* data, const int32_t* indices,
+                        const int32_t* index_pointers, double shift_re, double shift_im,
+                        const double* x, double* y, void* stream);
+
+/* ---- resolvent: restarted complex GMRES ------------------------------------------------ */
+
+typedef struct eb_gmres_options {
+  double tol;              /* relative residual ||b - A x|| / ||b|| to reach (e.g. 1e-10) */
+  int32_t restart;         /* Krylov vectors per cycle */
+  int32_t max_iterations;  /* limit on Arnoldi steps over all cycles (bounded run time) */
+  int32_t check_every;     /* Arnoldi steps between convergence reads on the host */
+  int32_t use_initial_guess; /* 1: start from the given x, 0: from zero */
+} eb_gmres_options;
+
+typedef struct eb_gmres_info {
+  int32_t iterations;      /* Arnoldi steps taken by this system */
+  int32_t cycles;          /* restart cycles of the call */
+  int32_t converged;       /* 1 if the true relative residual reached tol */
+  int32_t reserved;
+  double rel_residual;     /* final true relative residual */
+} eb_gmres_info;
+
+/* Device workspace (bytes) for eb_gmres_solve with these systems. host_table: HOST copy of
+ * the batch's instance table (NULL for a single instance); sys_inst: instance of each system
+ * (NULL: all systems on instance 0). */
+int64_t eb_gmres_workspace_bytes(const eb_batch* b, const eb_instance* host_table, int n_sys,
+                                 const int32_t* sys_inst, int restart);
+
+/* Solves n_sys systems (A_i - shift_s I) x_s = b_s (adjoint = 1: (A_i - shift_s I)^H x_s = b_s,
+ * the transposed solve of solve_odes_wrt_states_adj, core.py:567-599) where A_i is the
+ * d(odes)/d(states) Jacobian J of the system's instance. shifts: HOST array of n_sys complex
+ * (interleaved). rhs / x: DEVICE complex vectors, system-major (system s occupies 4*M*N complex
+ * entries after the previous systems'). Right-preconditioned by the inverse diagonal blocks.
+ * info: HOST array of n_sys. Returns EB_ERR_NOCONV at the iteration limit (x holds the last
+ * iterate) and EB_ERR_NAN if a residual became non-finite. Synchronises `stream`. */
+int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const double* J, int n_sys,
+                   const int32_t* sys_inst, const double* shifts, int adjoint,
+                   const double* rhs, double* x, const eb_gmres_options* opt, void* workspace,
+                   int64_t workspace_bytes, eb_gmres_info* info, void* stream);
+
+/* ---- resolvent: direct ring-block LU ----------------------------------------------------- */
+
+/* Device workspace (bytes) holding the block-LU factors of one M x N instance: 5 M dense
+ * (4N)^2 complex super-blocks plus pivots and solve vectors (about 80 M N^2 bytes). */
+int64_t eb_ringlu_workspace_bytes(int M, int N);
+
+/* Factors A = J - shift I (J: d(odes)/d(states) of the single instance in `b`) by block
+ * Gaussian elimination over the radial rings, pivoting inside each ring block. The factors
+ * serve eb_ringlu_solve for both A and A^H. Synchronises `stream`; EB_ERR_NAN if a ring block
+ * is singular. */
+int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double shift_im,
+                     void* workspace, int64_t workspace_bytes, void* stream);
+
+/* x = A^-1 rhs (adjoint = 1: x = A^-H rhs) with the factors of eb_ringlu_factor for the same
+ * J and shift, then iterative refinement x += A^-1 (rhs - A x) until ||rhs - A x|| / ||rhs||
+ * <= tol or max_refine refinements (EB_ERR_NOCONV). rhs, x: complex (4, M, N) reference
+ * layout; rel_residual (host, optional) receives the final relative residual. This replaces
+ * solve_odes_wrt_states_fwd / _adj (core.py:533-599). Synchronises `stream`. */
+int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double shift_im,
+                    int adjoint, const void* workspace, int64_t workspace_bytes,
+                    const double* rhs, double* x, double tol, int max_refine,
+                    double* rel_residual, void* stream);
+
+/* ---- second-order building blocks ------------------------------------------------------ */
+/* Directional derivatives of the Jacobians: with a complex direction d on the variable
+ * `dir_kind` (0 = states, 1 = vertices, 2 = velocities), these write dJ/de along Re(d) to
+ * J_re and along Im(d) to J_im, in the layout of the corresponding Jacobian. They replace the
+ * four complex-step Jacobian rebuilds of each second-order routine (core.py:718-1275). */
+int eb_odes_wrt_mach_dir(const eb_batch* b, const double* X, const double* V, const double* U,
+                         int dir_kind, const double* d, double* J_re, double* J_im,
+                         void* stream);
+int eb_odes_wrt_states_dir(const eb_batch* b, const double* X, const double* V,
+                           const double* U, int dir_kind, const double* d, double* J_re,
+                           double* J_im, void* stream);
+int eb_odes_wrt_vertices_dir(const eb_batch* b, const double* X, const double* V,
+                             const double* U, int dir_kind, const double* d, double* J_re,
+                             double* J_im, void* stream);
+int eb_forces_wrt_states_dir(const eb_batch* b, const double* X, const double* U,
+                             int dir_kind, const double* d, double* J_re, double* J_im,
+                             void* stream);
+int eb_forces_wrt_vertices_dir(const eb_batch* b, const double* X, const double* U,
+                               int dir_kind, const double* d, double* J_re, double* J_im,
+                               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EULER_B200_H */

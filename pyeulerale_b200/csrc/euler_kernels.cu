@@ -1,0 +1,781 @@
+// FP64 stencil kernels and their C ABI (include/euler_b200.h).
+//
+// One CUDA thread per cell (or per wall face / vertex), grid-stride over the packed cells of
+// all instances. Cells of an instance are numbered m + M*n like the reference's Fortran
+// arrays, so consecutive threads touch consecutive 32-byte states and every stencil load of
+// a warp is a contiguous segment. The instance owning a global cell is found by binary
+// search over the instance table (a single instance is passed by value, no table).
+//
+// Derivatives are forward-mode duals (scalar.cuh) through the same physics source
+// (physics.cuh) that produces the residual; they replace the reference's complex-step
+// procedures (src/spatial_discretization.f90:552-1256).
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+
+namespace eb {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return EB_ERR_CUDA;
+  }
+  return EB_OK;
+}
+
+int validate(const eb_batch* b) {
+  if (!b) return fail(EB_ERR_ARG, "null batch");
+  if (b->n_inst < 1) return fail(EB_ERR_ARG, "batch has no instances");
+  if (b->n_inst > 1 && b->d_table == nullptr)
+    return fail(EB_ERR_ARG, "batch of several instances needs a device table");
+  if (b->n_inst == 1 && b->d_table == nullptr) {
+    const eb_instance& s = b->single;
+    if (s.M < 4 || s.N < 5) return fail(EB_ERR_ARG, "grid needs M >= 4 and N >= 5 cells");
+    if (b->n_cells != (int64_t)s.M * s.N) return fail(EB_ERR_ARG, "n_cells != M*N");
+    if (b->n_verts != (int64_t)(s.M + 1) * (s.N + 1)) return fail(EB_ERR_ARG, "n_verts mismatch");
+    if (b->n_wall != s.N) return fail(EB_ERR_ARG, "n_wall != N");
+  }
+  if (b->n_cells <= 0) return fail(EB_ERR_ARG, "n_cells <= 0");
+  return EB_OK;
+}
+
+// ---- kernels -----------------------------------------------------------------------------
+
+__global__ void k_free_stream(Table t, int64_t n_cells, double* U) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const S4<double> fs = free_stream(in.mach, in);
+    double2* o = reinterpret_cast<double2*>(U + 4 * g);
+    o[0] = make_double2(fs.v[0], fs.v[1]);
+    o[1] = make_double2(fs.v[2], fs.v[3]);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_residual(Table t, int64_t n_cells, const double* X,
+                                                  const double* V, const double* U, double* R) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    Plain p;
+    load_plain(in, g - in.cell_offset, X, V, U, p);
+    Cell<double, double, double, double> c;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      c.x[k] = p.x[k];
+      c.w[k] = p.w[k];
+    }
+#pragma unroll
+    for (int s = 0; s < 9; ++s) c.u[s] = p.u[s];
+    c.mach = in.mach;
+    c.flag = p.flag;
+    const S4<double> o = make_ode(c, in);
+    double2* out = reinterpret_cast<double2*>(R + 4 * g);
+    out[0] = make_double2(o.v[0], o.v[1]);
+    out[1] = make_double2(o.v[2], o.v[3]);
+  }
+}
+
+// Matrix-free forward tangent with a complex direction on every input: Dual<double, 2>
+// carries (Re, Im) of the direction.
+__global__ void __launch_bounds__(128) k_tangent(Table t, int64_t n_cells, const double* X,
+                                                 const double* V, const double* U,
+                                                 const double* dU, const double* dX,
+                                                 const double* dV, const double* dMa,
+                                                 double* dR, double* R) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const int64_t local = g - in.cell_offset;
+    Plain p;
+    load_plain(in, local, X, V, U, p);
+    Direction du, dx, dv;
+    if (dU) load_direction(in, p, kDirStates, dU, du);
+    if (dX) load_direction(in, p, kDirVertices, dX, dx);
+    if (dV) load_direction(in, p, kDirVelocities, dV, dv);
+    Cell<D2, D2, D2, D2> c;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      c.x[k].x = bval<D2>(p.x[k].x, dX ? dx.xr[k].x : 0.0, dX ? dx.xi[k].x : 0.0);
+      c.x[k].z = bval<D2>(p.x[k].z, dX ? dx.xr[k].z : 0.0, dX ? dx.xi[k].z : 0.0);
+      c.w[k].x = bval<D2>(p.w[k].x, dV ? dv.xr[k].x : 0.0, dV ? dv.xi[k].x : 0.0);
+      c.w[k].z = bval<D2>(p.w[k].z, dV ? dv.xr[k].z : 0.0, dV ? dv.xi[k].z : 0.0);
+    }
+#pragma unroll
+    for (int s = 0; s < 9; ++s)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        c.u[s].v[k] = bval<D2>(p.u[s].v[k], dU ? du.ur[s].v[k] : 0.0, dU ? du.ui[s].v[k] : 0.0);
+    double mre = 0.0, mim = 0.0;
+    if (dMa) {
+      // one complex per instance; the instance index is the table position
+      int lo = 0;
+      if (t.dev) {
+        int hi = t.n - 1;
+        while (lo < hi) {
+          int mid = (lo + hi + 1) >> 1;
+          if (t.dev[mid].cell_offset <= g) lo = mid; else hi = mid - 1;
+        }
+      }
+      mre = dMa[2 * lo];
+      mim = dMa[2 * lo + 1];
+    }
+    c.mach = bval<D2>(in.mach, mre, mim);
+    c.flag = p.flag;
+    const S4<D2> o = make_ode(c, in);
+    double* out = dR + 8 * g;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      out[2 * k] = o.v[k].d[0];
+      out[2 * k + 1] = o.v[k].d[1];
+    }
+    if (R) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) R[4 * g + k] = o.v[k].v;
+    }
+  }
+}
+
+// Wall forces and force coefficients: one CTA per instance, warp-shuffle reductions of the
+// three coefficient sums (core.py:1277-1364; c_d omits the chord, as the reference does).
+__global__ void __launch_bounds__(256) k_forces(Table t, const double* X, const double* U,
+                                                double* F, double* coef) {
+  const Instance in = t.dev ? t.dev[blockIdx.x] : t.single;
+  const int M = in.M, N = in.N;
+  const double* Xi = X + 2 * in.vert_offset;
+  const double* Ui = U + 4 * in.cell_offset;
+  double sx = 0.0, sz = 0.0, sm = 0.0;
+  for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    const P2<double> a = ld2(Xi + 2 * ((int64_t)(M + 1) * n));
+    const P2<double> b = ld2(Xi + 2 * ((int64_t)(M + 1) * (n + 1)));
+    const double p = pressure(ld4(Ui + 4 * ((int64_t)M * n)));
+    const P2<double> nv = normal(a, b);
+    const double fx = p * nv.x, fz = p * nv.z;
+    F[2 * (in.wall_offset + n)] = fx;
+    F[2 * (in.wall_offset + n) + 1] = fz;
+    const double px = (a.x + b.x) / 2.0 - in.xc, pz = (a.z + b.z) / 2.0 - in.zc;
+    sx += fx;
+    sz += fz;
+    sm += pz * fx - px * fz;
+  }
+  if (!coef) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+    sm += __shfl_xor_sync(0xffffffffu, sm, o);
+  }
+  __shared__ double red[3][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    red[0][warp] = sx;
+    red[1][warp] = sz;
+    red[2][warp] = sm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ax = 0.0, az = 0.0, am = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      ax += red[0][w];
+      az += red[1][w];
+      am += red[2][w];
+    }
+    const double q = in.mach * in.mach * kGamma / 2.0;  // dynamic pressure, core.py:144-146
+    const int i = t.dev ? blockIdx.x : 0;
+    coef[3 * i + 0] = ax / q;
+    coef[3 * i + 1] = az / (q * in.chord);
+    coef[3 * i + 2] = am / (q * in.chord * in.chord);
+  }
+}
+
+// ---- Jacobian products -------------------------------------------------------------------
+
+// apply_odes_wrt_states_fwd, f90:825-864: y_c = sum_s J_s(c) x_nb(c,s) in the reference's
+// order (c, b, bb, f, ff, then ii, i, oo, o).
+__global__ void __launch_bounds__(128) k_apply_states_fwd(Table t, int64_t n_cells,
+                                                          const double* J, const double* x,
+                                                          double* y) {
+  const int order[9] = {kC, kB, kBB, kF, kFF, kII, kI, kOO, kO};
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const int M = in.M, N = in.N;
+    const int64_t local = g - in.cell_offset;
+    const int m = (int)(local % M), n = (int)(local / M);
+    const int64_t slot_stride = 16 * (int64_t)M * N;
+    const double* Jc = J + 144 * in.cell_offset + 16 * local;
+    const double* xi = x + 8 * in.cell_offset;
+    C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const int s = order[q];
+      if (!slot_active(s, m, M)) continue;
+      const double* blk = Jc + slot_stride * s;
+      const int64_t j = (m + slot_dm(s)) + (int64_t)M * wrap(n + slot_dn(s), N);
+      C2 xv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) xv[i] = ldc(xi + 8 * j + 2 * i);
+      double bl[16];
+#pragma unroll
+      for (int e = 0; e < 16; e += 2) {
+        const double2 v = *reinterpret_cast<const double2*>(blk + e);
+        bl[e] = v.x;
+        bl[e + 1] = v.y;
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        double tr = 0.0, ti = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          tr += bl[r + 4 * i] * xv[i].re;
+          ti += bl[r + 4 * i] * xv[i].im;
+        }
+        acc[r].re += tr;
+        acc[r].im += ti;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) stc(y + 8 * g + 2 * r, acc[r]);
+  }
+}
+
+// apply_odes_wrt_states_rev, f90:875-918, as a gather over the transposed stencil: the
+// output state j collects J_s(c)^T w_c from every cell c whose slot s reads j.
+__global__ void __launch_bounds__(128) k_apply_states_rev(Table t, int64_t n_cells,
+                                                          const double* J, const double* w,
+                                                          double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const int M = in.M, N = in.N;
+    const int64_t local = g - in.cell_offset;
+    const int m = (int)(local % M), n = (int)(local / M);
+    const int64_t slot_stride = 16 * (int64_t)M * N;
+    const double* Ji = J + 144 * in.cell_offset;
+    const double* wi = w + 8 * in.cell_offset;
+    C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+    for (int s = 0; s < 9; ++s) {
+      const int mc = m - slot_dm(s);
+      if (mc < 0 || mc >= M || !slot_active(s, mc, M)) continue;
+      const int64_t c = mc + (int64_t)M * wrap(n - slot_dn(s), N);
+      const double* blk = Ji + slot_stride * s + 16 * c;
+      C2 wv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) wv[r] = ldc(wi + 8 * c + 2 * r);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        double tr = 0.0, ti = 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          tr += wv[r].re * blk[r + 4 * i];
+          ti += wv[r].im * blk[r + 4 * i];
+        }
+        acc[i].re += tr;
+        acc[i].im += ti;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) stc(y + 8 * g + 2 * i, acc[i]);
+  }
+}
+
+// apply_odes_wrt_vertices_fwd, f90:1005-1032.
+__global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, int64_t n_cells,
+                                                            const double* J, const double* x,
+                                                            double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const int M = in.M, N = in.N;
+    const int64_t local = g - in.cell_offset;
+    const int m = (int)(local % M), n = (int)(local / M);
+    const int64_t slot_stride = 8 * (int64_t)M * N;
+    const double* Jc = J + 32 * in.cell_offset + 8 * local;
+    const double* xi = x + 4 * in.vert_offset;
+    const int64_t v[4] = {m + (int64_t)(M + 1) * n, m + (int64_t)(M + 1) * (n + 1),
+                          m + 1 + (int64_t)(M + 1) * (n + 1), m + 1 + (int64_t)(M + 1) * n};
+    C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double* blk = Jc + slot_stride * k;
+      const C2 a = ldc(xi + 4 * v[k]), b = ldc(xi + 4 * v[k] + 2);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        acc[r].re += blk[r] * a.re + blk[r + 4] * b.re;
+        acc[r].im += blk[r] * a.im + blk[r + 4] * b.im;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) stc(y + 8 * g + 2 * r, acc[r]);
+  }
+}
+
+// apply_odes_wrt_vertices_rev, f90:1044-1072, gathered per vertex (no wrap: the closing
+// vertex column n = N is distinct from n = 0, as in the reference).
+__global__ void __launch_bounds__(128) k_apply_vertices_rev(Table t, int64_t n_verts,
+                                                            const double* J, const double* w,
+                                                            double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_verts;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.vert(g);
+    const int M = in.M, N = in.N;
+    const int64_t local = g - in.vert_offset;
+    const int m = (int)(local % (M + 1)), n = (int)(local / (M + 1));
+    const int64_t slot_stride = 8 * (int64_t)M * N;
+    const double* Ji = J + 32 * in.cell_offset;
+    const double* wi = w + 8 * in.cell_offset;
+    // (corner, cell offset): the vertex is corner BI of (m, n), FI of (m, n-1),
+    // FO of (m-1, n-1) and BO of (m-1, n).
+    const int cm[4] = {m, m, m - 1, m - 1};
+    const int cn[4] = {n, n - 1, n - 1, n};
+    C2 acc[2] = {{0, 0}, {0, 0}};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (cm[k] < 0 || cm[k] >= M || cn[k] < 0 || cn[k] >= N) continue;
+      const int64_t c = cm[k] + (int64_t)M * cn[k];
+      const double* blk = Ji + slot_stride * k + 8 * c;
+      C2 wv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) wv[r] = ldc(wi + 8 * c + 2 * r);
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        double tr = 0.0, ti = 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          tr += wv[r].re * blk[r + 4 * d];
+          ti += wv[r].im * blk[r + 4 * d];
+        }
+        acc[d].re += tr;
+        acc[d].im += ti;
+      }
+    }
+    stc(y + 4 * g, acc[0]);
+    stc(y + 4 * g + 2, acc[1]);
+  }
+}
+
+// apply_odes_wrt_mach_fwd, f90:604-621.
+__global__ void k_apply_mach_fwd(Table t, int64_t n_cells, const double* J, const double* dm,
+                                 double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    int idx = 0;
+    if (t.dev) {
+      int lo = 0, hi = t.n - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (t.dev[mid].cell_offset <= g) lo = mid; else hi = mid - 1;
+      }
+      idx = lo;
+    }
+    const C2 d = ldc(dm + 2 * idx);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) stc(y + 8 * g + 2 * r, C2{J[4 * g + r] * d.re, J[4 * g + r] * d.im});
+  }
+}
+
+// apply_odes_wrt_mach_rev, f90:632-650: one CTA per instance, warp-shuffle reduction.
+__global__ void __launch_bounds__(256) k_apply_mach_rev(Table t, const double* J,
+                                                        const double* w, double* dm) {
+  const Instance in = t.dev ? t.dev[blockIdx.x] : t.single;
+  const int64_t cells = (int64_t)in.M * in.N;
+  double sr = 0.0, si = 0.0;
+  for (int64_t c = threadIdx.x; c < cells; c += blockDim.x) {
+    const int64_t g = in.cell_offset + c;
+    double tr = 0.0, ti = 0.0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      tr += w[8 * g + 2 * r] * J[4 * g + r];
+      ti += w[8 * g + 2 * r + 1] * J[4 * g + r];
+    }
+    sr += tr;
+    si += ti;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    si += __shfl_xor_sync(0xffffffffu, si, o);
+  }
+  __shared__ double red[2][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    red[0][warp] = sr;
+    red[1][warp] = si;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a += red[0][k];
+      b += red[1][k];
+    }
+    const int i = t.dev ? blockIdx.x : 0;
+    dm[2 * i] = a;
+    dm[2 * i + 1] = b;
+  }
+}
+
+// apply_forces_wrt_states_fwd, f90:1333-1348.
+__global__ void k_apply_forces_states_fwd(Table t, int64_t n_wall, const double* J,
+                                          const double* x, double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_wall;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.wall(g);
+    const int n = (int)(g - in.wall_offset);
+    const double* xv = x + 8 * (in.cell_offset + (int64_t)in.M * n);
+    const double* jb = J + 8 * g;
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      double tr = 0.0, ti = 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        tr += jb[d + 2 * i] * xv[2 * i];
+        ti += jb[d + 2 * i] * xv[2 * i + 1];
+      }
+      stc(y + 4 * g + 2 * d, C2{tr, ti});
+    }
+  }
+}
+
+// apply_forces_wrt_states_rev, f90:1359-1375: only the wall row is non-zero.
+__global__ void k_apply_forces_states_rev(Table t, int64_t n_cells, const double* J,
+                                          const double* w, double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const int64_t local = g - in.cell_offset;
+    const int m = (int)(local % in.M), n = (int)(local / in.M);
+    if (m != 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) stc(y + 8 * g + 2 * i, C2{0.0, 0.0});
+      continue;
+    }
+    const int64_t f = in.wall_offset + n;
+    const double* jb = J + 8 * f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      double tr = 0.0, ti = 0.0;
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        tr += w[4 * f + 2 * d] * jb[d + 2 * i];
+        ti += w[4 * f + 2 * d + 1] * jb[d + 2 * i];
+      }
+      stc(y + 8 * g + 2 * i, C2{tr, ti});
+    }
+  }
+}
+
+// apply_forces_wrt_vertices_fwd, f90:1267-1288.
+__global__ void k_apply_forces_vertices_fwd(Table t, int64_t n_wall, const double* J,
+                                            const double* x, double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_wall;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.wall(g);
+    const int n = (int)(g - in.wall_offset), M = in.M, N = in.N;
+    const double* xa = x + 4 * (in.vert_offset + (int64_t)(M + 1) * n);
+    const double* xb = x + 4 * (in.vert_offset + (int64_t)(M + 1) * (n + 1));
+    const double* J0 = J + 8 * in.wall_offset + 4 * n;
+    const double* J1 = J + 8 * in.wall_offset + 4 * (n + (int64_t)N);
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const double t0r = J0[d] * xa[0] + J0[d + 2] * xa[2];
+      const double t0i = J0[d] * xa[1] + J0[d + 2] * xa[3];
+      const double t1r = J1[d] * xb[0] + J1[d + 2] * xb[2];
+      const double t1i = J1[d] * xb[1] + J1[d + 2] * xb[3];
+      stc(y + 4 * g + 2 * d, C2{t0r + t1r, t0i + t1i});
+    }
+  }
+}
+
+// apply_forces_wrt_vertices_rev, f90:1299-1322, gathered per vertex.
+__global__ void k_apply_forces_vertices_rev(Table t, int64_t n_verts, const double* J,
+                                            const double* w, double* y) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_verts;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.vert(g);
+    const int M = in.M, N = in.N;
+    const int64_t local = g - in.vert_offset;
+    const int m = (int)(local % (M + 1)), n = (int)(local / (M + 1));
+    C2 acc[2] = {{0, 0}, {0, 0}};
+    if (m == 0) {
+      // vertex n is `bi` of wall face n (k = 0) and `fi` of wall face n-1 (k = 1)
+      for (int k = 0; k < 2; ++k) {
+        const int f = n - k;
+        if (f < 0 || f >= N) continue;
+        const double* jb = J + 8 * in.wall_offset + 4 * (f + (int64_t)N * k);
+        const double* wv = w + 4 * (in.wall_offset + f);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          acc[e].re += wv[0] * jb[2 * e] + wv[2] * jb[2 * e + 1];
+          acc[e].im += wv[1] * jb[2 * e] + wv[3] * jb[2 * e + 1];
+        }
+      }
+    }
+    stc(y + 4 * g, acc[0]);
+    stc(y + 4 * g + 2, acc[1]);
+  }
+}
+
+// convert_odes_wrt_states, f90:765-814, one thread per block row. For N >= 5 and M >= 4 the
+// nine stencil columns of a row are distinct, so the row holds 5 + [m>=1] + [m>=2] +
+// [m<=M-2] + [m<=M-3] blocks, emitted in ascending column order with 1-based indices.
+__global__ void k_convert_bsr(int M, int N, const double* J, double* data, int32_t* indices,
+                              int32_t* indptr) {
+  const int64_t rows = (int64_t)M * N;
+  const int64_t line = 9 * (int64_t)M - 6;  // blocks per angular line
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(r % M), n = (int)(r / M);
+    // blocks in the rows m' < m of this line
+    int64_t before = 5 * (int64_t)m + (m > 1 ? m - 1 : 0) + (m > 2 ? m - 2 : 0) +
+                     (m < M - 1 ? m : M - 1) + (m < M - 2 ? m : M - 2);
+    int64_t ptr = (int64_t)n * line + before;
+    int64_t col[9];
+    int slot[9];
+    int cnt = 0;
+    for (int s = 0; s < 9; ++s) {
+      const int mm = m + slot_dm(s);
+      if (mm < 0 || mm >= M) continue;
+      col[cnt] = mm + (int64_t)M * wrap(n + slot_dn(s), N);
+      slot[cnt] = s;
+      ++cnt;
+    }
+    for (int a = 1; a < cnt; ++a) {  // insertion sort by column
+      const int64_t c = col[a];
+      const int sl = slot[a];
+      int b = a - 1;
+      while (b >= 0 && col[b] > c) {
+        col[b + 1] = col[b];
+        slot[b + 1] = slot[b];
+        --b;
+      }
+      col[b + 1] = c;
+      slot[b + 1] = sl;
+    }
+    indptr[r] = (int32_t)(ptr + 1);
+    if (r == rows - 1) indptr[rows] = (int32_t)(ptr + cnt + 1);
+    const int64_t slot_stride = 16 * rows;
+    for (int a = 0; a < cnt; ++a) {
+      const double* blk = J + slot_stride * slot[a] + 16 * r;
+      double* dst = data + 16 * (ptr + a);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) dst[e] = blk[e];
+      indices[ptr + a] = (int32_t)(col[a] + 1);
+    }
+  }
+}
+
+// y = (A - shift I) x for a BSR matrix with 1-based indices (complex x, y).
+__global__ void k_bsr_spmv(int64_t rows, const double* data, const int32_t* indices,
+                           const int32_t* indptr, double sr, double si, const double* x,
+                           double* y) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    for (int32_t p = indptr[r] - 1; p < indptr[r + 1] - 1; ++p) {
+      const double* blk = data + 16 * (int64_t)p;
+      const int64_t c = indices[p] - 1;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const C2 xv = ldc(x + 8 * c + 2 * i);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[q].re += blk[q + 4 * i] * xv.re;
+          acc[q].im += blk[q + 4 * i] * xv.im;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const C2 xv = ldc(x + 8 * r + 2 * q);
+      acc[q].re -= sr * xv.re - si * xv.im;
+      acc[q].im -= sr * xv.im + si * xv.re;
+      stc(y + 8 * r + 2 * q, acc[q]);
+    }
+  }
+}
+
+}  // namespace eb
+
+// =========================================================================================
+// C ABI
+// =========================================================================================
+using namespace eb;
+
+extern "C" {
+
+const char* eb_last_error(void) { return g_last_error.c_str(); }
+const char* eb_version(void) { return "euler_b200 1.0 (sm_100a, FP64)"; }
+
+int eb_set_free_stream_state(const eb_batch* b, double* U, void* stream) {
+  EB_VALIDATE(b);
+  if (!U) return fail(EB_ERR_ARG, "null states");
+  const Table t = make_table(b);
+  k_free_stream<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, U);
+  return check_launch("set_free_stream_state");
+}
+
+int eb_compute_odes(const eb_batch* b, const double* X, const double* V, const double* U,
+                    double* R, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !R) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_residual<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U, R);
+  return check_launch("compute_odes");
+}
+
+int eb_compute_forces(const eb_batch* b, const double* X, const double* U, double* F,
+                      double* coef, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !F) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_forces<<<b->n_inst, 256, 0, EB_STREAM(stream)>>>(t, X, U, F, coef);
+  return check_launch("compute_forces");
+}
+
+int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double* d_mach,
+                               double* d_odes, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_mach || !d_odes) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_mach_fwd<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J,
+                                                                              d_mach, d_odes);
+  return check_launch("apply_odes_wrt_mach_fwd");
+}
+
+int eb_apply_odes_wrt_mach_rev(const eb_batch* b, const double* J, const double* d_odes,
+                               double* d_mach, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_mach || !d_odes) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_mach_rev<<<b->n_inst, 256, 0, EB_STREAM(stream)>>>(t, J, d_odes, d_mach);
+  return check_launch("apply_odes_wrt_mach_rev");
+}
+
+int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const double* d_states,
+                                 double* d_odes, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_states_fwd<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, J, d_states, d_odes);
+  return check_launch("apply_odes_wrt_states_fwd");
+}
+
+int eb_apply_odes_wrt_states_rev(const eb_batch* b, const double* J, const double* d_odes,
+                                 double* d_states, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_states_rev<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, J, d_odes, d_states);
+  return check_launch("apply_odes_wrt_states_rev");
+}
+
+int eb_apply_odes_wrt_vertices_fwd(const eb_batch* b, const double* J,
+                                   const double* d_vertices, double* d_odes, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_vertices_fwd<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, J, d_vertices, d_odes);
+  return check_launch("apply_odes_wrt_vertices_fwd");
+}
+
+int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const double* d_odes,
+                                   double* d_vertices, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_vertices_rev<<<grid_for(b->n_verts, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_verts, J, d_odes, d_vertices);
+  return check_launch("apply_odes_wrt_vertices_rev");
+}
+
+int eb_apply_forces_wrt_states_fwd(const eb_batch* b, const double* J, const double* d_states,
+                                   double* d_forces, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_states || !d_forces) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_forces_states_fwd<<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_wall, J, d_states, d_forces);
+  return check_launch("apply_forces_wrt_states_fwd");
+}
+
+int eb_apply_forces_wrt_states_rev(const eb_batch* b, const double* J, const double* d_forces,
+                                   double* d_states, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_states || !d_forces) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_forces_states_rev<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, J, d_forces, d_states);
+  return check_launch("apply_forces_wrt_states_rev");
+}
+
+int eb_apply_forces_wrt_vertices_fwd(const eb_batch* b, const double* J,
+                                     const double* d_vertices, double* d_forces, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_vertices || !d_forces) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_forces_vertices_fwd<<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_wall, J, d_vertices, d_forces);
+  return check_launch("apply_forces_wrt_vertices_fwd");
+}
+
+int eb_apply_forces_wrt_vertices_rev(const eb_batch* b, const double* J,
+                                     const double* d_forces, double* d_vertices, void* stream) {
+  EB_VALIDATE(b);
+  if (!J || !d_vertices || !d_forces) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_apply_forces_vertices_rev<<<grid_for(b->n_verts, 256), 256, 0, EB_STREAM(stream)>>>(
+      t, b->n_verts, J, d_forces, d_vertices);
+  return check_launch("apply_forces_wrt_vertices_rev");
+}
+
+int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, const double* U,
+                          const double* dU, const double* dX, const double* dV,
+                          const double* dMa, double* dR, double* R, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !dR) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_tangent<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
+                                                                       dU, dX, dV, dMa, dR, R);
+  return check_launch("apply_odes_tangent");
+}
+
+int eb_convert_odes_wrt_states(const eb_batch* b, const double* J, double* data,
+                               int32_t* indices, int32_t* index_pointers, void* stream) {
+  EB_VALIDATE(b);
+  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "convert takes a single instance");
+  if (!J || !data || !indices || !index_pointers) return fail(EB_ERR_ARG, "null array");
+  const int M = b->single.M, N = b->single.N;
+  k_convert_bsr<<<grid_for((int64_t)M * N, 128), 128, 0, EB_STREAM(stream)>>>(
+      M, N, J, data, indices, index_pointers);
+  return check_launch("convert_odes_wrt_states");
+}
+
+int eb_bsr_shifted_spmv(int64_t n_rows, const double* data, const int32_t* indices,
+                        const int32_t* index_pointers, double shift_re, double shift_im,
+                        const double* x, double* y, void* stream) {
+  if (n_rows <= 0 || !data || !indices || !index_pointers || !x || !y)
+    return fail(EB_ERR_ARG, "bad BSR arguments");
+  k_bsr_spmv<<<grid_for(n_rows, 128), 128, 0, EB_STREAM(stream)>>>(
+      n_rows, data, indices, index_pointers, shift_re, shift_im, x, y);
+  return check_launch("bsr_shifted_spmv");
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// C ABI of the first-order Jacobians (dual-number kernels of jacobian_kernels.cuh with
+// B = double), replacing the complex-step procedures of src/spatial_discretization.f90.
+
+#include "jacobian_kernels.cuh"
+
+using namespace eb;
+
+extern "C" {
+
+int eb_compute_odes_wrt_mach(const eb_batch* b, const double* X, const double* V,
+                             const double* U, double* J, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_jac_mach<double, kDirNone><<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, X, V, U, nullptr, J, nullptr, nullptr);
+  return check_launch("compute_odes_wrt_mach");
+}
+
+int eb_compute_odes_wrt_states(const eb_batch* b, const double* X, const double* V,
+                               const double* U, double* J, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_jac_states<double, kDirNone><<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, X, V, U, nullptr, J, nullptr, nullptr);
+  return check_launch("compute_odes_wrt_states");
+}
+
+int eb_compute_odes_wrt_vertices(const eb_batch* b, const double* X, const double* V,
+                                 const double* U, double* J, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_jac_vertexlike<double, kDirNone, false>
+      <<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
+                                                                  nullptr, J, nullptr, nullptr);
+  return check_launch("compute_odes_wrt_vertices");
+}
+
+int eb_compute_odes_wrt_velocities(const eb_batch* b, const double* X, const double* V,
+                                   const double* U, double* J, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_jac_vertexlike<double, kDirNone, true>
+      <<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
+                                                                  nullptr, J, nullptr, nullptr);
+  return check_launch("compute_odes_wrt_velocities");
+}
+
+int eb_compute_forces_wrt_states(const eb_batch* b, const double* X, const double* U,
+                                 double* J, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_jac_forces_states<double, kDirNone><<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_wall, X, U, nullptr, J, nullptr, nullptr);
+  return check_launch("compute_forces_wrt_states");
+}
+
+int eb_compute_forces_wrt_vertices(const eb_batch* b, const double* X, const double* U,
+                                   double* J, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_jac_forces_vertices<double, kDirNone>
+      <<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_wall, X, U, nullptr, J,
+                                                                 nullptr, nullptr);
+  return check_launch("compute_forces_wrt_vertices");
+}
+
+}  // extern "C"

@@ -1,0 +1,173 @@
+"""Python side of the device resolvent (``eb_gmres_solve`` in csrc/gmres.cu).
+
+``solve_shifted`` solves ``(dR/dU - s I) x = b`` (or the Hermitian-adjoint system) for any
+number of (instance, shift, right-hand side) systems in one native call. All vectors are
+torch complex128-compatible float64 device tensors in the interleaved layout of the C ABI.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class GmresOptions(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("restart", ctypes.c_int32),
+                ("max_iterations", ctypes.c_int32), ("check_every", ctypes.c_int32),
+                ("use_initial_guess", ctypes.c_int32)]
+
+
+class GmresInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("cycles", ctypes.c_int32),
+                ("converged", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("rel_residual", ctypes.c_double)]
+
+
+_bound = False
+
+
+def _bind() -> ctypes.CDLL:
+    global _bound
+    lib = _lib.load()
+    if not _bound:
+        lib.eb_gmres_workspace_bytes.restype = ctypes.c_int64
+        lib.eb_gmres_workspace_bytes.argtypes = [
+            ctypes.POINTER(_lib.Batch), ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_int]
+        lib.eb_gmres_solve.restype = ctypes.c_int
+        lib.eb_gmres_solve.argtypes = [
+            ctypes.POINTER(_lib.Batch), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.POINTER(GmresOptions), ctypes.c_void_p, ctypes.c_int64,
+            ctypes.POINTER(GmresInfo), ctypes.c_void_p]
+        _bound = True
+    return lib
+
+
+class SolveInfo(list):
+    """Per-system GMRES statistics (iterations, cycles, converged, rel_residual)."""
+
+    @property
+    def iterations(self) -> list[int]:
+        return [i["iterations"] for i in self]
+
+    @property
+    def max_rel_residual(self) -> float:
+        return max(i["rel_residual"] for i in self)
+
+
+def solve_shifted(batch: _lib.Batch, J, rhs, shifts, *, adjoint: bool = False,
+                  tol: float = 1e-10, restart: int = 60, maxiter: int = 3000,
+                  check_every: int = 10, x0=None, sys_inst=None, host_table=None,
+                  workspace=None, raise_on_failure: bool = True):
+    """Solves the shifted systems; returns ``(x, SolveInfo)``.
+
+    Args:
+        batch: the instances (``_lib.Batch``).
+        J: device d(odes)/d(states) of the batch (float64, 144 per cell).
+        rhs: device float64 tensor, system-major interleaved complex right-hand sides.
+        shifts: one complex shift per system.
+        adjoint: solve with ``(A - s I)^H`` (the reference's ``solve_odes_wrt_states_adj``).
+        sys_inst: instance index of each system (default: all on instance 0).
+        host_table: host ``_lib.Instance`` array for batches of several instances.
+    """
+    import torch
+
+    lib = _bind()
+    n_sys = len(shifts)
+    sh = np.zeros(2 * n_sys)
+    sh[0::2] = np.real(shifts)
+    sh[1::2] = np.imag(shifts)
+    inst = None if sys_inst is None else np.ascontiguousarray(sys_inst, dtype=np.int32)
+    tab_ptr = None if host_table is None else ctypes.addressof(host_table)
+    inst_ptr = None if inst is None else inst.ctypes.data
+    bref = ctypes.byref(batch)
+    need = lib.eb_gmres_workspace_bytes(bref, tab_ptr, n_sys, inst_ptr, int(restart))
+    if need < 0:
+        raise ValueError("invalid GMRES systems")
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty(int(need), dtype=torch.uint8, device=rhs.device)
+    x = torch.zeros_like(rhs) if x0 is None else x0
+    opts = GmresOptions(float(tol), int(restart), int(maxiter), int(check_every),
+                        0 if x0 is None else 1)
+    infos = (GmresInfo * n_sys)()
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.eb_gmres_solve(bref, tab_ptr, J.data_ptr(), n_sys, inst_ptr, sh.ctypes.data,
+                            1 if adjoint else 0, rhs.data_ptr(), x.data_ptr(),
+                            ctypes.byref(opts), workspace.data_ptr(), int(workspace.numel()),
+                            infos, stream)
+    info = SolveInfo({"iterations": i.iterations, "cycles": i.cycles,
+                      "converged": bool(i.converged), "rel_residual": i.rel_residual}
+                     for i in infos)
+    if rc != _lib.EB_OK and raise_on_failure:
+        raise _lib.EulerB200Error("eb_gmres_solve", rc, lib.eb_last_error().decode()
+                                  + f" (rel. residuals {[i['rel_residual'] for i in info]})")
+    return x, info
+
+
+class RingLU:
+    """Direct resolvent of one instance: ring-block LU factors of ``J - shift I`` on the device.
+
+    ``factor(J, shift)`` builds the factors (``eb_ringlu_factor``); ``solve(rhs, adjoint)``
+    returns ``(J - shift I)^-1 rhs`` or ``(J - shift I)^-H rhs`` refined to ``tol``
+    (``eb_ringlu_solve``). One factorisation serves both solve directions.
+    """
+
+    def __init__(self, batch: _lib.Batch, tol: float = 1e-10, max_refine: int = 4) -> None:
+        import torch
+
+        self._torch = torch
+        self.batch = batch
+        self.tol = tol
+        self.max_refine = max_refine
+        lib = _lib.load()
+        if not getattr(lib, "_ringlu_bound", False):
+            lib.eb_ringlu_workspace_bytes.restype = ctypes.c_int64
+            lib.eb_ringlu_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+            lib.eb_ringlu_factor.restype = ctypes.c_int
+            lib.eb_ringlu_factor.argtypes = [ctypes.POINTER(_lib.Batch), ctypes.c_void_p,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                             ctypes.c_int64, ctypes.c_void_p]
+            lib.eb_ringlu_solve.restype = ctypes.c_int
+            lib.eb_ringlu_solve.argtypes = [
+                ctypes.POINTER(_lib.Batch), ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+            lib._ringlu_bound = True
+        self._lib = lib
+        need = lib.eb_ringlu_workspace_bytes(batch.single.M, batch.single.N)
+        if need < 0:
+            raise ValueError("ring LU needs a single instance with M >= 4, N >= 5")
+        self.workspace = torch.empty(int(need), dtype=torch.uint8, device="cuda")
+        self.J = None
+        self.shift = None
+
+    def factor(self, J, shift: complex) -> None:
+        shift = complex(shift)
+        stream = self._torch.cuda.current_stream().cuda_stream
+        rc = self._lib.eb_ringlu_factor(ctypes.byref(self.batch), J.data_ptr(), shift.real,
+                                        shift.imag, self.workspace.data_ptr(),
+                                        self.workspace.numel(), stream)
+        if rc != _lib.EB_OK:
+            raise _lib.EulerB200Error("eb_ringlu_factor", rc, self._lib.eb_last_error().decode())
+        self.J, self.shift = J, shift
+
+    def solve(self, rhs, adjoint: bool = False, out=None):
+        """Solves with the current factors; returns ``(x, rel_residual)``."""
+        if self.J is None:
+            raise RuntimeError("factor() first")
+        x = self._torch.empty_like(rhs) if out is None else out
+        rel = ctypes.c_double(0.0)
+        stream = self._torch.cuda.current_stream().cuda_stream
+        rc = self._lib.eb_ringlu_solve(ctypes.byref(self.batch), self.J.data_ptr(),
+                                       self.shift.real, self.shift.imag, 1 if adjoint else 0,
+                                       self.workspace.data_ptr(), self.workspace.numel(),
+                                       rhs.data_ptr(), x.data_ptr(), self.tol, self.max_refine,
+                                       ctypes.byref(rel), stream)
+        if rc != _lib.EB_OK:
+            raise _lib.EulerB200Error("eb_ringlu_solve", rc,
+                                      self._lib.eb_last_error().decode() + f" (rel {rel.value})")
+        return x, rel.value

@@ -1,0 +1,154 @@
+"""Parity of the CUDA kernels with the oracle, through the C ABI (GPU)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import Gpu, crandn, make_case, oracle_eval, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129"]
+
+# Tolerances: residual / forces differ from the reference arithmetic by summation order and
+# the real-vs-complex evaluation only; Jacobians are exact dual-number derivatives compared
+# with h = 1e-12 complex-step derivatives.
+TOL_R = 1e-12
+TOL_J = 1e-10
+TOL_APPLY = 1e-13
+
+
+@pytest.fixture(scope="module", params=CASES)
+def evaluated(request, cuda, oracle, golden_grids):
+    case = make_case(request.param, golden_grids, seed=7)
+    gpu = Gpu(cuda, case)
+    return request.param, case, gpu, gpu.evaluate(), oracle_eval(oracle, case)
+
+
+def test_residual(evaluated):
+    name, _, _, g, o = evaluated
+    assert rel_err(g["R"], o["R"]) <= TOL_R, name
+
+
+def test_forces(evaluated):
+    name, _, _, g, o = evaluated
+    assert rel_err(g["F"], o["F"]) <= TOL_R, name
+
+
+@pytest.mark.parametrize("key", ["J_ma", "J_u", "J_x", "J_v", "JF_u", "JF_x"])
+def test_jacobians(evaluated, key):
+    name, _, _, g, o = evaluated
+    assert rel_err(g[key], o[key]) <= TOL_J, (name, key, rel_err(g[key], o[key]))
+
+
+def test_apply_products(evaluated, oracle):
+    """GPU Jacobian products against the oracle's products on the same (GPU) Jacobians."""
+    name, case, gpu, g, _ = evaluated
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(3)
+    torch = gpu.torch
+    sh = {"odes": (4, M, N), "states": (4, M, N), "vertices": (2, M + 1, N + 1),
+          "forces": (2, N), "mach": (1,)}
+    products = [
+        ("eb_apply_odes_wrt_mach_fwd", "apply_odes_wrt_mach_fwd", "J_ma", "mach", "odes"),
+        ("eb_apply_odes_wrt_mach_rev", "apply_odes_wrt_mach_rev", "J_ma", "odes", "mach"),
+        ("eb_apply_odes_wrt_states_fwd", "apply_odes_wrt_states_fwd", "J_u", "states", "odes"),
+        ("eb_apply_odes_wrt_states_rev", "apply_odes_wrt_states_rev", "J_u", "odes", "states"),
+        ("eb_apply_odes_wrt_vertices_fwd", "apply_odes_wrt_vertices_fwd", "J_x", "vertices",
+         "odes"),
+        ("eb_apply_odes_wrt_vertices_rev", "apply_odes_wrt_vertices_rev", "J_x", "odes",
+         "vertices"),
+        ("eb_apply_odes_wrt_vertices_fwd", "apply_odes_wrt_vertices_fwd", "J_v", "vertices",
+         "odes"),
+        ("eb_apply_forces_wrt_states_fwd", "apply_forces_wrt_states_fwd", "JF_u", "states",
+         "forces"),
+        ("eb_apply_forces_wrt_states_rev", "apply_forces_wrt_states_rev", "JF_u", "forces",
+         "states"),
+        ("eb_apply_forces_wrt_vertices_fwd", "apply_forces_wrt_vertices_fwd", "JF_x",
+         "vertices", "forces"),
+        ("eb_apply_forces_wrt_vertices_rev", "apply_forces_wrt_vertices_rev", "JF_x", "forces",
+         "vertices"),
+    ]
+    for cname, oname, jkey, src, dst in products:
+        x = crandn(rng, sh[src])
+        y = torch.zeros(2 * int(np.prod(sh[dst])), dtype=torch.float64, device="cuda")
+        gpu.call(cname, g["_dev"][jkey], gpu.dev(x), y)
+        got = gpu.host(y, sh[dst], complex_=True)
+        ref = np.asfortranarray(np.zeros(sh[dst], dtype=complex))
+        getattr(oracle, oname)(g[jkey], x, ref)
+        assert rel_err(got, ref) <= TOL_APPLY, (name, cname, rel_err(got, ref))
+
+
+def test_tangent_kernel(evaluated):
+    """Matrix-free forward tangent == sum of the Jacobian products (complex direction)."""
+    name, case, gpu, g, o = evaluated
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(5)
+    dU = crandn(rng, (4, M, N))
+    dX = crandn(rng, (2, M + 1, N + 1))
+    dV = crandn(rng, (2, M + 1, N + 1))
+    dMa = np.array([0.3 - 0.2j])
+    torch = gpu.torch
+    dR = torch.zeros(8 * M * N, dtype=torch.float64, device="cuda")
+    gpu.call("eb_apply_odes_tangent", gpu.X, gpu.V, gpu.U, gpu.dev(dU), gpu.dev(dX),
+             gpu.dev(dV), gpu.dev(dMa), dR, None)
+    got = gpu.host(dR, (4, M, N), complex_=True)
+    # reference: complex-step Jacobians applied with the oracle's own routines
+    from oracle.shim import SpatialDiscretizationModule
+
+    ora = SpatialDiscretizationModule()
+    parts = []
+    for fn, J, x in [("apply_odes_wrt_states_fwd", o["J_u"], dU),
+                     ("apply_odes_wrt_vertices_fwd", o["J_x"], dX),
+                     ("apply_odes_wrt_vertices_fwd", o["J_v"], dV),
+                     ("apply_odes_wrt_mach_fwd", o["J_ma"], dMa)]:
+        y = np.asfortranarray(np.zeros((4, M, N), dtype=complex))
+        getattr(ora, fn)(J, x, y)
+        parts.append(y)
+    ref = parts[0] + parts[1] + parts[2] + parts[3]
+    assert rel_err(got, ref) <= TOL_J, (name, rel_err(got, ref))
+
+
+def test_bsr_conversion_bit_exact(evaluated, oracle):
+    """convert_odes_wrt_states: identical data, indices and index pointers."""
+    name, _, gpu, g, _ = evaluated
+    M, N = gpu.M, gpu.N
+    nnzb = (9 * M - 6) * N
+    torch = gpu.torch
+    data = torch.zeros(16 * nnzb, dtype=torch.float64, device="cuda")
+    idx = torch.zeros(nnzb, dtype=torch.int32, device="cuda")
+    ptr = torch.zeros(M * N + 1, dtype=torch.int32, device="cuda")
+    gpu.call("eb_convert_odes_wrt_states", g["_dev"]["J_u"], data, idx, ptr)
+    r_data = np.asfortranarray(np.zeros((4, 4, nnzb)))
+    r_idx = np.zeros(nnzb, dtype=np.int32)
+    r_ptr = np.zeros(M * N + 1, dtype=np.int32)
+    oracle.convert_odes_wrt_states(g["J_u"], r_data, r_idx, r_ptr)
+    np.testing.assert_array_equal(idx.cpu().numpy(), r_idx)
+    np.testing.assert_array_equal(ptr.cpu().numpy(), r_ptr)
+    np.testing.assert_array_equal(np.reshape(data.cpu().numpy(), (4, 4, nnzb), order="F"),
+                                  r_data)
+
+
+def test_bsr_shifted_spmv(evaluated, oracle):
+    name, _, gpu, g, _ = evaluated
+    M, N = gpu.M, gpu.N
+    nnzb = (9 * M - 6) * N
+    torch = gpu.torch
+    data = torch.zeros(16 * nnzb, dtype=torch.float64, device="cuda")
+    idx = torch.zeros(nnzb, dtype=torch.int32, device="cuda")
+    ptr = torch.zeros(M * N + 1, dtype=torch.int32, device="cuda")
+    gpu.call("eb_convert_odes_wrt_states", g["_dev"]["J_u"], data, idx, ptr)
+    rng = np.random.default_rng(11)
+    x = crandn(rng, (4, M, N))
+    y = torch.zeros(8 * M * N, dtype=torch.float64, device="cuda")
+    shift = 0.25 - 1.5j
+    from pyeulerale_b200 import _lib
+
+    _lib.call("eb_bsr_shifted_spmv", M * N, data.data_ptr(), idx.data_ptr(), ptr.data_ptr(),
+              shift.real, shift.imag, gpu.dev(x).data_ptr(), y.data_ptr(), None)
+    got = gpu.host(y, (4, M, N), complex_=True)
+    ref = np.asfortranarray(np.zeros((4, M, N), dtype=complex))
+    oracle.apply_odes_wrt_states_fwd(g["J_u"], x, ref)
+    ref = ref - shift * x
+    assert rel_err(got, ref) <= TOL_APPLY, name

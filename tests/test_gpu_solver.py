@@ -1,0 +1,102 @@
+"""Device GMRES resolvent against the direct sparse solve of the oracle Jacobian (GPU)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from helpers import Gpu, crandn, make_case, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def bsr_matrix(oracle, J: np.ndarray) -> sp.csr_matrix:
+    """The reference's CSR assembly (core.py:512-531) from the oracle's BSR conversion."""
+    M, N = J.shape[2], J.shape[3]
+    nnzb = (9 * M - 6) * N
+    data = np.asfortranarray(np.zeros((4, 4, nnzb)))
+    idx = np.zeros(nnzb, dtype=np.int32)
+    ptr = np.zeros(M * N + 1, dtype=np.int32)
+    oracle.convert_odes_wrt_states(J, data, idx, ptr)
+    return sp.bsr_matrix((np.moveaxis(data, -1, 0), idx - 1, ptr - 1)).tocsr()
+
+
+@pytest.mark.parametrize("name,shift", [("ref8x9", 0.3 + 0.7j), ("ref8x9", 2.0),
+                                        ("ref8x9", 0.05j), ("naca0012_33", 60.0)])
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_gmres_matches_direct_solve(cuda, oracle, golden_grids, name, shift, adjoint):
+    """Block-Jacobi GMRES where it converges (small grids, or large shifts)."""
+    from pyeulerale_b200 import solver
+
+    case = make_case(name, golden_grids, seed=2)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(9)
+    b = crandn(rng, (4, M, N))
+    x, info = solver.solve_shifted(gpu.batch, g["_dev"]["J_u"], gpu.dev(b), [shift],
+                                   adjoint=adjoint, tol=1e-10, restart=60, maxiter=5000)
+    got = gpu.host(x, (4, M, N), complex_=True)
+    A = bsr_matrix(oracle, g["J_u"]).astype(complex)
+    n = A.shape[0]
+    if adjoint:
+        op = (A - np.conj(shift) * sp.eye(n)).T.tocsc()
+    else:
+        op = (A - shift * sp.eye(n)).tocsc()
+    bf = b.ravel(order="F")
+    res = np.linalg.norm(bf - op @ got.ravel(order="F")) / np.linalg.norm(bf)
+    assert res <= 1e-10, (info, res)
+    ref = spla.spsolve(op, bf)
+    assert rel_err(got.ravel(order="F"), ref) <= 1e-7, info
+
+
+def test_gmres_batched_shifts_match_single(cuda, golden_grids):
+    """Several shifts in one call give the same solutions as one call per shift."""
+    from pyeulerale_b200 import solver
+
+    case = make_case("ref8x9", golden_grids, seed=4)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(1)
+    shifts = [0.5j, 1.0 + 0.2j, 3.0, 0.1 - 0.4j]
+    rhs = [crandn(rng, (4, M, N)) for _ in shifts]
+    packed = cuda.cat([gpu.dev(r) for r in rhs])
+    xb, info_b = solver.solve_shifted(gpu.batch, g["_dev"]["J_u"], packed, shifts,
+                                      sys_inst=[0] * len(shifts))
+    n = 8 * M * N
+    for k, (s, r) in enumerate(zip(shifts, rhs)):
+        x1, _ = solver.solve_shifted(gpu.batch, g["_dev"]["J_u"], gpu.dev(r), [s])
+        a = xb[k * n:(k + 1) * n].cpu().numpy()
+        c = x1.cpu().numpy()
+        assert rel_err(a, c) <= 1e-8, (k, info_b)
+
+
+@pytest.mark.parametrize("name", ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129"])
+@pytest.mark.parametrize("shift", [0.3 + 0.7j, 2.0, 0.0, 0.0012j])
+def test_ringlu_direct_solve(cuda, oracle, golden_grids, name, shift):
+    """Ring-block LU resolvent: 1e-10 residual and agreement with SuperLU, both directions."""
+    from pyeulerale_b200 import solver
+
+    case = make_case(name, golden_grids, seed=2)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(9)
+    b = crandn(rng, (4, M, N))
+    lu = solver.RingLU(gpu.batch, tol=1e-10)
+    lu.factor(g["_dev"]["J_u"], shift)
+    A = bsr_matrix(oracle, g["J_u"]).astype(complex)
+    n = A.shape[0]
+    bf = b.ravel(order="F")
+    for adjoint in (False, True):
+        x, rel = lu.solve(gpu.dev(b), adjoint=adjoint)
+        got = gpu.host(x, (4, M, N), complex_=True).ravel(order="F")
+        op = ((A - np.conj(shift) * sp.eye(n)).T if adjoint else (A - shift * sp.eye(n))).tocsc()
+        res = np.linalg.norm(bf - op @ got) / np.linalg.norm(bf)
+        assert res <= 1e-10 and rel <= 1e-10, (name, shift, adjoint, res, rel)
+        if n <= 20000:
+            ref = spla.spsolve(op, bf)
+            assert rel_err(got, ref) <= 1e-7, (name, shift, adjoint)

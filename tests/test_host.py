@@ -1,0 +1,84 @@
+"""Host-side logic and the C ABI surface (CPU only, no kernel launches)."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from pyeulerale_b200 import _lib, grid
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def header_symbols() -> set[str]:
+    text = (ROOT / "include" / "euler_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(eb_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_exports_every_declared_symbol():
+    from pyeulerale_b200.build import build_library
+
+    build_library()
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    declared = header_symbols()
+    assert len(declared) >= 30
+    missing = [s for s in sorted(declared) if not hasattr(lib, s)]
+    assert not missing, missing
+    bound = set(_lib.exported_symbols()) | {"eb_gmres_solve", "eb_gmres_workspace_bytes"}
+    assert declared <= bound, declared - bound
+
+
+def test_struct_layouts_match_header():
+    assert ctypes.sizeof(_lib.Instance) == 104
+    assert _lib.Instance.wall_offset.offset == 24
+    assert _lib.Instance.mach.offset == 32
+    assert _lib.Batch.single.offset == 40
+
+
+def test_plot3d_round_trip(tmp_path, golden_grids):
+    X = golden_grids["naca0012_8x9"]
+    grid.write_plot3d(tmp_path / "g.plot3d", X)
+    Y = grid.read_plot3d(tmp_path / "g.plot3d")
+    np.testing.assert_array_equal(X, Y)
+    assert Y.flags.f_contiguous
+
+
+def test_naca_ogrid_is_closed_and_sized():
+    X = grid.naca_ogrid(33, 41, thickness=0.04, chord=10.0, far_radius=200.0,
+                        first_spacing=0.1)
+    assert X.shape == (2, 33, 41)
+    np.testing.assert_array_equal(X[:, :, 0], X[:, :, -1])
+    r = np.hypot(X[0, -1, :] - 5.0, X[1, -1, :])
+    np.testing.assert_allclose(r, 200.0)
+    first = np.hypot(*(X[:, 1, :] - X[:, 0, :]))
+    assert np.all(first > 0.05) and np.all(first < 0.2)
+    # trailing edge -> lower side first
+    assert X[1, 0, X.shape[2] // 4] < 0 < X[1, 0, 3 * X.shape[2] // 4]
+
+
+def test_free_stream_state_matches_formula():
+    s = grid.free_stream_state(0.5, 0.0)
+    assert s[0] == 1.0 and s[2] == 0.0
+    np.testing.assert_allclose(s[3], 1 / 0.4 + 1.4 * 0.25 / 2)
+
+
+def test_make_instance_angle_factor():
+    inst = _lib.make_instance(8, 9, 0.5, 90.0)
+    assert abs(inst.cos_aoa) < 1e-15 and inst.sin_aoa == 1.0
+    b = _lib.single_batch(inst)
+    assert (b.n_cells, b.n_verts, b.n_wall) == (72, 90, 9)
+
+
+def test_dropin_requires_cuda(golden_grids):
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("CUDA present")
+    from pyeulerale_b200 import SpatialDiscretization
+
+    with pytest.raises(RuntimeError, match="CUDA"):
+        SpatialDiscretization(golden_grids["naca0012_8x9"])
