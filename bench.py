@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Throughput of the B200 spatial discretization on the 129x129 NACA-0004 workload.
+
+Workload (seeded synthetic inputs; the reference publishes no benchmark dataset): the
+129x129 NACA-0004 O-grid of chord 10 with a far field at radius 200 (first spacing 0.1),
+Ma 0.5, alpha 0, moment centre (2.5, 0); states = free stream x (1 + 1 % Gaussian noise),
+a smooth seeded grid-velocity field. A batch of B instances (default 256 per GPU, 4.2 M cells,
+~400 MB of residual inputs + outputs, well above the 126 MB L2) is packed into one instance
+table.
+
+One timed "step" is one residual evaluation R(Ma, U, X, V) of the whole batch (one launch).
+The JSON line reports cell-residual evaluations per second (``value``), and beside it the VJP
+rate (full set of reverse products per instance: d/dU, d/dX, d/dV, d/dMa) and the resolvent
+rate (ring-block LU factor + refined solve to 1e-10 relative residual per shift).
+
+``--impl reference`` times the CPU restatement of the reference (complex arithmetic, all host
+threads) on a bounded sample of the same workload. Under torchrun every rank processes its own
+B instances (weak scaling; instances are independent, no data-path collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-residual evals/s; VJP/s; batched resolvent solves/s vs plain at 1e-10 rel"
+UNIT = "cell-residual evals/s"
+BYTES_PER_CELL_RESIDUAL = 96          # U 32 + X 16 + V 16 + R 32 (FP64)
+BYTES_PER_CELL_VJP = 1152 + 256 + 256 + 32 + 4 * 64 + 64 + 2 * 32 + 8
+GRID = dict(radial_pts=129, angular_pts=129, thickness=0.04, chord=10.0, far_radius=200.0,
+            first_spacing=0.1)
+FLOW = dict(mach=0.5, aoa_deg=0.0, center=(2.5, 0.0))
+PROFILE_SUMMARY = ROOT / "profiles" / "residual_naca0004_129x129.md"
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--instances", type=int, default=256, help="instances per GPU")
+    p.add_argument("--shifts", type=int, default=4, help="resolvent shifts timed")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline budget")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---- workload -------------------------------------------------------------------------------
+
+def workload(n_inst: int, seed: int):
+    from pyeulerale_b200 import grid
+
+    X = grid.naca_ogrid(GRID["radial_pts"], GRID["angular_pts"], GRID["thickness"],
+                        GRID["chord"], GRID["far_radius"], GRID["first_spacing"])
+    M, N = X.shape[1] - 1, X.shape[2] - 1
+    rng = np.random.default_rng(seed)
+    Us = [grid.perturbed_states(M, N, FLOW["mach"], FLOW["aoa_deg"], 0.01, rng)
+          for _ in range(n_inst)]
+    V = grid.smooth_velocities(X, rng, amplitude=0.01)
+    return X, V, Us
+
+
+# ---- clocks ---------------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int) -> None:
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit()
+                else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- CPU baseline (the oracle) --------------------------------------------------------------
+
+def cpu_residual_rate(X, V, Us, threads: int, budget_s: float) -> tuple[float, str]:
+    """Cells/s of the complex-arithmetic oracle residual on a bounded sample."""
+    from oracle.shim import SpatialDiscretizationModule, load_library
+
+    lib = load_library()
+    lib.sdo_set_threads(threads)
+    ora = SpatialDiscretizationModule()
+    ora.aoa[...] = FLOW["aoa_deg"]
+    Xc = np.asfortranarray(X, dtype=complex)
+    Vc = np.asfortranarray(V, dtype=complex)
+    M, N = Us[0].shape[1], Us[0].shape[2]
+    R = np.asfortranarray(np.zeros((4, M, N), dtype=complex))
+    Uc = [np.asfortranarray(u, dtype=complex) for u in Us]
+    ora.compute_odes(FLOW["mach"], Xc, Vc, Uc[0], R)  # warm-up
+    cells, t0, k = 0, time.perf_counter(), 0
+    while time.perf_counter() - t0 < budget_s:
+        ora.compute_odes(FLOW["mach"], Xc, Vc, Uc[k % len(Uc)], R)
+        cells += M * N
+        k += 1
+    dt = time.perf_counter() - t0
+    lib.sdo_set_threads(1)
+    return cells / dt, f"{k} residual evaluations of one {M}x{N} instance in {dt:.1f} s"
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.shim import load_library
+
+    threads = load_library().sdo_max_threads()
+    X, V, Us = workload(4, seed=0)
+    per_step = max(1.0, args.cpu_seconds / max(args.steps, 1))
+    from oracle.shim import SpatialDiscretizationModule
+
+    # warm-up steps, then timed steps (each a bounded sample of the workload)
+    for _ in range(args.warmup):
+        cpu_residual_rate(X, V, Us, threads, 0.2)
+    rates = []
+    sample = ""
+    for _ in range(args.steps):
+        r, sample = cpu_residual_rate(X, V, Us, threads, per_step)
+        rates.append(r)
+    value = statistics.median(rates)
+    del SpatialDiscretizationModule
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * 129 * 129 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded NACA-0004 O-grid)",
+        "config": {"workload": "residual of the 129x129 NACA-0004 O-grid (128x128 cells), "
+                               "Ma 0.5, alpha 0, complex arithmetic as the reference",
+                   "cells_per_instance": 128 * 128},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"per step: {sample}; C++ restatement of "
+                                   "src/spatial_discretization.f90 (oracle/sd_oracle.cpp)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- B200 arm -------------------------------------------------------------------------------
+
+def read_traffic() -> float | None:
+    """DRAM bytes per residual launch from the committed ncu summary, scaled per cell."""
+    if not PROFILE_SUMMARY.exists():
+        return None
+    for line in PROFILE_SUMMARY.read_text().splitlines():
+        if line.startswith("dram_bytes_per_cell:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def run_b200(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from pyeulerale_b200 import _lib, solver
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    _lib.load()
+    B = args.instances
+    X, V, Us = workload(B, seed=1000 + rank)
+    specs = [InstanceSpec(X, FLOW["mach"], FLOW["aoa_deg"], GRID["chord"], FLOW["center"])
+             for _ in range(B)]
+    inst = InstanceSet(specs)
+    cells = inst.n_cells
+    f64 = dict(dtype=torch.float64, device="cuda")
+    hX = torch.from_numpy(inst.pack_vertices()).pin_memory()
+    hV = torch.from_numpy(inst.pack_vertices([V] * B)).pin_memory()
+    hU = torch.from_numpy(inst.pack_cells(Us)).pin_memory()
+    hR = torch.empty(4 * cells, dtype=torch.float64).pin_memory()
+    dX, dV, dU = hX.cuda(), hV.cuda(), hU.cuda()
+    dR = torch.empty(4 * cells, **f64)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def residual():
+        inst.call("eb_compute_odes", dX, dV, dU, dR, stream=sp)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # residual: warm-up, then K timed launches
+    for _ in range(args.warmup):
+        residual()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            residual()
+        ev1.record(stream)
+        barrier()
+    t_res = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    clk = clocks.summary()
+    value = world * cells * args.steps / t_res
+    per_launch = t_res / args.steps
+    achieved = BYTES_PER_CELL_RESIDUAL * cells / per_launch / 1e9
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
+        if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    traffic_cell = read_traffic()
+
+    # end to end through the C ABI with host buffers: H2D of the step's inputs, D2H of R
+    for _ in range(max(1, args.warmup // 2)):
+        dX.copy_(hX, non_blocking=True)
+        dV.copy_(hV, non_blocking=True)
+        dU.copy_(hU, non_blocking=True)
+        residual()
+        hR.copy_(dR, non_blocking=True)
+    barrier()
+    e2e_steps = max(3, args.steps // 5)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        dX.copy_(hX, non_blocking=True)
+        dV.copy_(hV, non_blocking=True)
+        dU.copy_(hU, non_blocking=True)
+        residual()
+        hR.copy_(dR, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    h2d = (hX.numel() + hV.numel() + hU.numel()) * 8
+    d2h = hR.numel() * 8
+    e2e_value = world * cells * e2e_steps / t_e2e
+
+    # VJP set on stored Jacobians (d/dU, d/dX, d/dV, d/dMa) per instance
+    J_u = torch.empty(144 * cells, **f64)
+    J_x = torch.empty(32 * cells, **f64)
+    J_v = torch.empty(32 * cells, **f64)
+    J_m = torch.empty(4 * cells, **f64)
+    inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u, stream=sp)
+    inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, J_x, stream=sp)
+    inst.call("eb_compute_odes_wrt_velocities", dX, dV, dU, J_v, stream=sp)
+    inst.call("eb_compute_odes_wrt_mach", dX, dV, dU, J_m, stream=sp)
+    w = torch.randn(8 * cells, **f64)
+    gU = torch.empty(8 * cells, **f64)
+    gX = torch.empty(4 * inst.n_verts, **f64)
+    gV = torch.empty(4 * inst.n_verts, **f64)
+    gM = torch.empty(2 * B, **f64)
+
+    def vjp():
+        inst.call("eb_apply_odes_wrt_states_rev", J_u, w, gU, stream=sp)
+        inst.call("eb_apply_odes_wrt_vertices_rev", J_x, w, gX, stream=sp)
+        inst.call("eb_apply_odes_wrt_vertices_rev", J_v, w, gV, stream=sp)
+        inst.call("eb_apply_odes_wrt_mach_rev", J_m, w, gM, stream=sp)
+
+    for _ in range(args.warmup):
+        vjp()
+    barrier()
+    v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    vsteps = max(5, args.steps // 2)
+    v0.record(stream)
+    for _ in range(vsteps):
+        vjp()
+    v1.record(stream)
+    barrier()
+    t_vjp = max_over_ranks(v0.elapsed_time(v1) / 1e3)
+    vjp_rate = world * B * vsteps / t_vjp
+    vjp_gbs = BYTES_PER_CELL_VJP * cells * vsteps / t_vjp / 1e9
+    del J_x, J_v, J_m
+
+    # resolvent: ring-block LU factor + refined solve per frequency-response shift
+    single = InstanceSet([specs[0]])
+    J1 = J_u[:144 * single.n_cells]
+    lu = solver.RingLU(single.batch, tol=1e-10)
+    rng = np.random.default_rng(rank)
+    b = torch.from_numpy(rng.standard_normal(8 * single.n_cells)).cuda()
+    shifts = [1j * k * FLOW["mach"] * 1.4**0.5 / (GRID["chord"] / 2)
+              for k in np.logspace(-2, 1, max(args.shifts, 1))]
+    lu.factor(J1, shifts[0])  # warm-up (handles, workspace)
+    lu.solve(b)
+    barrier()
+    t0 = time.perf_counter()
+    rels = []
+    for s in shifts:
+        lu.factor(J1, s)
+        _, rel = lu.solve(b)
+        rels.append(rel)
+    barrier()
+    t_solve = max_over_ranks(time.perf_counter() - t0)
+    solve_rate = world * len(shifts) / t_solve
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, sample = cpu_residual_rate(X, V, Us[:4], 1, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{sample}; single-threaded like the reference; C++ restatement "
+                         "of src/spatial_discretization.f90 in complex arithmetic"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * per_launch, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded NACA-0004 O-grid, perturbed free stream, smooth grid "
+                "velocities)",
+        "config": {"workload": f"residual of {B} instances of the 129x129 NACA-0004 O-grid "
+                               "(128x128 cells each) per GPU, one launch per step",
+                   "instances_per_gpu": B, "cells_per_gpu": cells,
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "traffic": None if traffic_cell is None else traffic_cell * cells,
+                     "algorithmic_bytes_per_launch": BYTES_PER_CELL_RESIDUAL * cells,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "vjp": {"value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
+                "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4},
+        "resolvent": {"value": solve_rate, "unit": "resolvent solves/s (factor + solve)",
+                      "shifts": len(shifts), "max_rel_residual": max(rels),
+                      "method": "ring-block LU, refined to 1e-10"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()
