@@ -201,6 +201,21 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
                    const double* rhs, double* x, const eb_gmres_options* opt, void* workspace,
                    int64_t workspace_bytes, eb_gmres_info* info, void* stream);
 
+/* Scratch-free GMRES: the same solve as eb_gmres_solve (same arguments minus the
+ * workspace), for callers that cannot allocate device memory -- a host program whose device
+ * memory belongs to another runtime's pool, or a loop that may not allocate once running. Its
+ * workspace is a 48 MiB array in the library's device memory, held by every GPU that loads the
+ * library until the process exits; systems needing more (eb_gmres_workspace_bytes) are
+ * rejected with EB_ERR_ARG. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture. All calls share
+ * the array: calls that overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. No counterpart in the reference (its solver allocates on every
+ * call, core.py:512-599). */
+int eb_gmres_solve_noalloc(const eb_batch* b, const eb_instance* host_table, const double* J,
+                           int n_sys, const int32_t* sys_inst, const double* shifts,
+                           int adjoint, const double* rhs, double* x,
+                           const eb_gmres_options* opt, eb_gmres_info* info, void* stream);
+
 /* ---- resolvent: direct ring-block LU ----------------------------------------------------- */
 
 /* Device workspace (bytes) holding the block-LU factors of one M x N instance: 5 M dense

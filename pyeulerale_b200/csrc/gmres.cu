@@ -19,6 +19,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -30,6 +31,7 @@ namespace eb {
 int fail(int code, const char* msg);
 int check_launch(const char* what);
 int validate(const eb_batch* b);
+extern thread_local std::string g_last_error;
 
 namespace gm {
 
@@ -744,3 +746,64 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
 }
 
 }  // extern "C"
+
+// ---- scratch-free variant ----------------------------------------------------------------
+//
+// Some callers cannot allocate device memory themselves: host programs whose device memory is
+// owned by another runtime's pool (a second allocator would break its budget), or solver loops
+// that run under a no-allocation-after-start-up rule. For them eb_gmres_solve_noalloc runs the
+// same solve with its workspace in this fixed device array. Every GPU that loads the library
+// holds the array until the process exits; all calls share it.
+
+namespace eb {
+namespace gm {
+
+constexpr size_t kStaticScratchBytes = (size_t)48 << 20;  // 48 MiB
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mutex;
+void* g_static_ptr[128] = {};
+
+// Device address of the static scratch on the current device, looked up once per device.
+int static_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+    return fail(EB_ERR_CUDA, "gmres_noalloc: no current device");
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p) {
+      g_last_error = std::string("gmres_noalloc: cudaGetSymbolAddress failed: ") +
+                     cudaGetErrorString(e);
+      return EB_ERR_CUDA;
+    }
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return EB_OK;
+}
+
+}  // namespace gm
+}  // namespace eb
+
+extern "C" int eb_gmres_solve_noalloc(const eb_batch* b, const eb_instance* host_table,
+                                      const double* J, int n_sys, const int32_t* sys_inst,
+                                      const double* shifts, int adjoint, const double* rhs,
+                                      double* x, const eb_gmres_options* opt,
+                                      eb_gmres_info* info, void* stream) {
+  if (!b || !opt || n_sys < 1) return fail(EB_ERR_ARG, "gmres_noalloc: null argument");
+  const int64_t need = eb_gmres_workspace_bytes(b, host_table, n_sys, sys_inst, opt->restart);
+  if (need < 0) return fail(EB_ERR_ARG, "gmres_noalloc: invalid systems");
+  if (need > (int64_t)kStaticScratchBytes) {
+    g_last_error = "gmres_noalloc: the systems need " + std::to_string(need) +
+                   " bytes of workspace, more than the 48 MiB static scratch; use "
+                   "eb_gmres_solve with a caller-provided workspace";
+    return EB_ERR_ARG;
+  }
+  void* scratch = nullptr;
+  const int rc = static_scratch(&scratch);
+  if (rc != EB_OK) return rc;
+  return eb_gmres_solve(b, host_table, J, n_sys, sys_inst, shifts, adjoint, rhs, x, opt, scratch,
+                        (int64_t)kStaticScratchBytes, info, stream);
+}

@@ -171,3 +171,43 @@ class RingLU:
             raise _lib.EulerB200Error("eb_ringlu_solve", rc,
                                       self._lib.eb_last_error().decode() + f" (rel {rel.value})")
         return x, rel.value
+
+
+def solve_shifted_noalloc(batch: _lib.Batch, J, rhs, shifts, *, adjoint: bool = False,
+                          tol: float = 1e-10, restart: int = 60, maxiter: int = 3000,
+                          check_every: int = 10, x=None, sys_inst=None, host_table=None):
+    """``solve_shifted`` through ``eb_gmres_solve_noalloc``: no device workspace is allocated.
+
+    For callers that cannot allocate device memory (their memory belongs to another runtime's
+    pool, or their loop may not allocate once running): the solver's workspace is the
+    library's fixed 48 MiB device array. ``x`` may be given to avoid allocating the solution
+    vector too. Calls that overlap on the GPU share that array and race.
+    """
+    import torch
+
+    lib = _lib.load()
+    if not getattr(lib, "_noalloc_bound", False):
+        lib.eb_gmres_solve_noalloc.restype = ctypes.c_int
+        lib.eb_gmres_solve_noalloc.argtypes = [
+            ctypes.POINTER(_lib.Batch), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.POINTER(GmresOptions), ctypes.POINTER(GmresInfo), ctypes.c_void_p]
+        lib._noalloc_bound = True
+    n_sys = len(shifts)
+    sh = np.zeros(2 * n_sys)
+    sh[0::2] = np.real(shifts)
+    sh[1::2] = np.imag(shifts)
+    inst = None if sys_inst is None else np.ascontiguousarray(sys_inst, dtype=np.int32)
+    x = torch.empty_like(rhs) if x is None else x
+    opts = GmresOptions(float(tol), int(restart), int(maxiter), int(check_every), 0)
+    infos = (GmresInfo * n_sys)()
+    rc = lib.eb_gmres_solve_noalloc(
+        ctypes.byref(batch), None if host_table is None else ctypes.addressof(host_table),
+        J.data_ptr(), n_sys, None if inst is None else inst.ctypes.data, sh.ctypes.data,
+        1 if adjoint else 0, rhs.data_ptr(), x.data_ptr(), ctypes.byref(opts), infos,
+        torch.cuda.current_stream().cuda_stream)
+    if rc != _lib.EB_OK:
+        raise _lib.EulerB200Error("eb_gmres_solve_noalloc", rc, lib.eb_last_error().decode())
+    return x, SolveInfo({"iterations": i.iterations, "cycles": i.cycles,
+                         "converged": bool(i.converged), "rel_residual": i.rel_residual}
+                        for i in infos)
