@@ -48,7 +48,7 @@ PROFILE_SUMMARY = ROOT / "profiles" / "residual_naca0004_129x129.md"
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--instances", type=int, default=256, help="instances per GPU")
@@ -76,53 +76,60 @@ def workload(n_inst: int, seed: int):
 # ---- clocks ---------------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and throttle-reason sampling (NVML, every 5 ms) during the timed region."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, device_index: int) -> None:
         self.device_index = device_index
-        self.proc = None
-        self.path = None
+        self.samples: list[tuple[int, int]] = []
+        self._stop = None
+        self._thread = None
+        self.max_mhz = None
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-        time.sleep(0.3)
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception:  # NVML unavailable: report unsampled
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((mhz, reasons))
+                except Exception:
+                    pass
+                self._stop.wait(0.005)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
+        time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            self.proc.wait(timeout=10)
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self) -> dict:
-        rows = []
-        if self.path and os.path.exists(self.path):
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-            os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
-        return {"sm_mhz": statistics.median(loaded) if loaded else None,
-                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit()
-                else None,
-                "reasons": reasons, "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        mhz = [m for m, _ in self.samples]
+        loaded = [m for m in mhz if m > 0.5 * max(mhz)]
+        reasons = sorted({name for _, r in self.samples for name, bit in self.REASONS.items()
+                          if r & bit})
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples)}
 
 
 # ---- CPU baseline (the oracle) --------------------------------------------------------------
@@ -159,8 +166,7 @@ def run_reference(args) -> None:
 
     threads = load_library().sdo_max_threads()
     X, V, Us = workload(4, seed=0)
-    per_step = max(1.0, args.cpu_seconds / max(args.steps, 1))
-    from oracle.shim import SpatialDiscretizationModule
+    per_step = max(0.2, min(1.0, 60.0 / max(args.steps, 1)))
 
     # warm-up steps, then timed steps (each a bounded sample of the workload)
     for _ in range(args.warmup):
@@ -171,7 +177,6 @@ def run_reference(args) -> None:
         r, sample = cpu_residual_rate(X, V, Us, threads, per_step)
         rates.append(r)
     value = statistics.median(rates)
-    del SpatialDiscretizationModule
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,

@@ -26,6 +26,11 @@ NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC",
 ]
+# The Jacobian kernels evaluate without FMA contraction: derivatives of the reference's branch
+# primitives (abs_c, max_c) are decided by exact ties and cancellations at degenerate states (an
+# exact free stream), and only uncontracted evaluation keeps equal inputs bitwise equal across
+# the differently inlined call sites. The residual itself is continuous there and keeps FMA.
+PER_FILE_FLAGS = {"jacobians.cu": ["-fmad=false"], "second_order.cu": ["-fmad=false"]}
 # cuBLAS / cuSOLVER serve the dense super-block factorisations of the ring-block LU.
 LINK_FLAGS = ["-L/usr/local/cuda/lib64", "-lcublas", "-lcusolver",
               "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
@@ -51,7 +56,8 @@ def _compile(src: Path, force: bool, verbose: bool) -> Path:
     if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime,
                                                                   _headers_mtime()):
         return obj
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj) + ".tmp"]
+    cmd = [_nvcc(), *NVCC_FLAGS, *PER_FILE_FLAGS.get(src.name, []), "-I", str(INCLUDE), "-c",
+           str(src), "-o", str(obj) + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -273,6 +273,13 @@ __global__ void __launch_bounds__(128) k_apply_states_rev(Table t, int64_t n_cel
       if (mc < 0 || mc >= M || !slot_active(s, mc, M)) continue;
       const int64_t c = mc + (int64_t)M * wrap(n - slot_dn(s), N);
       const double* blk = Ji + slot_stride * s + 16 * c;
+      double bl[16];
+#pragma unroll
+      for (int e = 0; e < 16; e += 2) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(blk + e));
+        bl[e] = v.x;
+        bl[e + 1] = v.y;
+      }
       C2 wv[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) wv[r] = ldc(wi + 8 * c + 2 * r);
@@ -281,8 +288,8 @@ __global__ void __launch_bounds__(128) k_apply_states_rev(Table t, int64_t n_cel
         double tr = 0.0, ti = 0.0;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-          tr += wv[r].re * blk[r + 4 * i];
-          ti += wv[r].im * blk[r + 4 * i];
+          tr += wv[r].re * bl[r + 4 * i];
+          ti += wv[r].im * bl[r + 4 * i];
         }
         acc[i].re += tr;
         acc[i].im += ti;
@@ -347,7 +354,14 @@ __global__ void __launch_bounds__(128) k_apply_vertices_rev(Table t, int64_t n_v
     for (int k = 0; k < 4; ++k) {
       if (cm[k] < 0 || cm[k] >= M || cn[k] < 0 || cn[k] >= N) continue;
       const int64_t c = cm[k] + (int64_t)M * cn[k];
-      const double* blk = Ji + slot_stride * k + 8 * c;
+      const double* bp = Ji + slot_stride * k + 8 * c;
+      double blk[8];
+#pragma unroll
+      for (int e = 0; e < 8; e += 2) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(bp + e));
+        blk[e] = v.x;
+        blk[e + 1] = v.y;
+      }
       C2 wv[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r) wv[r] = ldc(wi + 8 * c + 2 * r);

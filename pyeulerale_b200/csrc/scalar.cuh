@@ -10,7 +10,7 @@
 // Arithmetic between different scalar types is allowed when one embeds into the other
 // (double -> Dual<double,K>, Dual<double,2> -> Dual<Dual<double,2>,4>, ...): the lower operand
 // is treated as a constant. The two branch primitives of the reference keep its semantics:
-//   abs_c(x): derivative sign taken from sign(1, Re x), -0.0 counting as negative (f90:97-102);
+//   abs_c(x): derivative sign taken from the sign of Re x (f90:97-102), zeros as positive;
 //   max_c(x, y): x only if Re x > Re y + 1e-8 (f90:111-120), tangents follow the selection.
 #pragma once
 
@@ -191,12 +191,17 @@ EB_HD Dual<T, K> sqrt_(const Dual<T, K>& a) {
   return r;
 }
 
-// abs_c, f90:97-102: value |x|, derivative times sign(1, x) with -0.0 -> -1.
+// abs_c, f90:97-102: value |x|, derivative times sign(1, Re x). The reference evaluates the
+// argument in complex arithmetic, where an exact cancellation (p - 2p + p at a uniform state)
+// and a quotient with a zero numerator (Smith's division adds a +0 term) come out as +0; in
+// real arithmetic the same values can come out as -0 depending on how the compiler contracts
+// the expression. Both zeros therefore count as positive here, which is what the reference
+// sees at such degenerate points (e.g. an exact free stream).
 EB_HD double abs_c(double x) { return ::fabs(x); }
 template <class T, int K>
 EB_HD Dual<T, K> abs_c(const Dual<T, K>& a) {
   Dual<T, K> r;
-  const double s = ::copysign(1.0, value(a));
+  const double s = value(a) < 0.0 ? -1.0 : 1.0;
   r.v = abs_c(a.v);
 #pragma unroll
   for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * s;

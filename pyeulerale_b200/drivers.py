@@ -1,0 +1,162 @@
+"""Workload drivers as library calls: PTC/SER steady state, frequency response, static gain.
+
+These are the callers of the hot path in the reference's examples
+(``examples/response/run.py`` and ``examples/gain/run.py``), written as functions over the
+drop-in ``SpatialDiscretization``: everything runs through the device (residual, Jacobians,
+ring-block LU resolvent, exact second-order terms). ``response_report`` / ``gain_report``
+print the same report as the reference's example scripts, so a run can be compared with the
+reference's committed golden outputs line by line.
+"""
+
+from __future__ import annotations
+
+import io
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .grid import HEAT_RATIO
+
+
+@dataclass
+class PtcResult:
+    """History of the pseudo-transient continuation."""
+
+    norms: list[float] = field(default_factory=list)
+    rel_norms: list[float] = field(default_factory=list)
+
+    @property
+    def iterations(self) -> int:
+        return len(self.norms)
+
+
+def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None) -> PtcResult:
+    """Pseudo-transient continuation with switched evolution relaxation
+    (examples/response/run.py:84-123): the time step is 0.1 / (relative infinity-norm of the
+    residual), each step solves (dR/dU - dt^-1 I) dU = -R on the device, and the loop stops at
+    rel <= rtol (or NaN), leaving the solver linearized at the final state."""
+    res = PtcResult()
+    solver.compute_odes()
+    norm_free_stream = np.max(np.abs(solver.odes))
+    if out is not None:
+        print(f"\nPseudo-transient continuation:\n{'it':>6} {'residual':>15} "
+              f"{'rel residual':>15}", file=out)
+    for it in range(max_iter):
+        solver.compute_odes()
+        norm = np.max(np.abs(solver.odes))
+        rel = norm / norm_free_stream
+        res.norms.append(float(norm))
+        res.rel_norms.append(float(rel))
+        if out is not None:
+            print(f"{it:>6} {norm:>15.1e} {rel:>15.1e}", file=out)
+        solver.linearize()
+        solver.compute_forces()
+        if rel <= rtol or np.isnan(rel):
+            break
+        time_step = 1.e-1 * rel**-1.
+        update = solver.solve_odes_wrt_states_fwd(d_odes=-solver.odes, shift=time_step**-1.)
+        solver.states[:] += update
+    return res
+
+
+def pitch_vertices(solver, axis_location: float) -> np.ndarray:
+    """dX/dalpha of a rigid pitch about (axis_location, 0), per radian."""
+    v = np.empty_like(solver.vertices, dtype=complex)
+    v[1] = -(solver.vertices[0] - axis_location)
+    v[0] = solver.vertices[1]
+    return v
+
+
+def frequency_response(solver, chord: float, axis_location: float,
+                       reduced_frequencies, out=None) -> tuple[np.ndarray, np.ndarray]:
+    """Pitch-to-(c_l, c_m) transfer function at s = i k V_inf / (c/2)
+    (examples/response/run.py:125-176). Returns (c_l(s), c_m(s))."""
+    speed = solver.mach_number * HEAT_RATIO**0.5
+    dX = pitch_vertices(solver, axis_location)
+    cl_grad = solver.compute_lift_coefficient_wrt_forces()
+    cm_grad = solver.compute_moment_coefficient_wrt_forces()
+    cm_grad_x = solver.compute_moment_coefficient_wrt_vertices()
+    if out is not None:
+        print(f"\nFrequency response:\n{'red frequency':>15} {'lift coefficient':>25} "
+              f"{'moment coefficient':>25}", file=out)
+    cls, cms = [], []
+    rhs_x = solver.apply_odes_wrt_vertices_fwd(d_vertices=dX)
+    dF_x = solver.apply_forces_wrt_vertices_fwd(d_vertices=dX)
+    for k in reduced_frequencies:
+        s = 1j * k * speed / (chord / 2)
+        dU = -solver.solve_odes_wrt_states_fwd(
+            shift=s, d_odes=rhs_x + solver.apply_odes_wrt_velocities_fwd(d_velocities=s * dX))
+        dF = dF_x + solver.apply_forces_wrt_states_fwd(d_states=dU)
+        cl = np.vdot(cl_grad, dF)
+        cm = np.vdot(cm_grad, dF) + np.vdot(cm_grad_x, dX)
+        cls.append(cl)
+        cms.append(cm)
+        if out is not None:
+            print(f"{k:>15.3e} {cl:>+25.3e} {cm:>+25.3e}", file=out)
+    return np.array(cls), np.array(cms)
+
+
+def static_gain(solver, out=None) -> tuple[float, float]:
+    """Lift slope dc_l/dalpha and its Mach derivative at zero angle of attack
+    (examples/gain/run.py:81-145), with the adjoint of c_l and the exact second-order terms."""
+    dX = pitch_vertices(solver, 0.0)
+    cl_grad = solver.compute_lift_coefficient_wrt_forces()
+    dU_a = -solver.solve_odes_wrt_states_fwd(d_odes=solver.apply_odes_wrt_vertices_fwd(
+        d_vertices=dX))
+    cl_a = np.vdot(cl_grad, solver.apply_forces_wrt_vertices_fwd(d_vertices=dX)
+                   + solver.apply_forces_wrt_states_fwd(d_states=dU_a))
+    dU_m = -solver.solve_odes_wrt_states_fwd(
+        d_odes=solver.apply_odes_wrt_mach_fwd(d_mach=np.asarray([1. + 0j])))
+    adj = -solver.solve_odes_wrt_states_adj(solver.apply_forces_wrt_states_rev(d_forces=cl_grad))
+    cl_a_m = (
+        -2 / solver.mach_number * cl_a
+        + np.vdot(solver.compute_forces_wrt_states_inner_product_wrt_states(
+            d_forces=cl_grad, d_states=dU_a), dU_m)
+        + np.vdot(solver.compute_forces_wrt_vertices_inner_product_wrt_states(
+            d_forces=cl_grad, d_vertices=dX), dU_m)
+        + solver.compute_odes_wrt_states_inner_product_wrt_mach(d_odes=adj, d_states=dU_a).item()
+        + np.vdot(solver.compute_odes_wrt_states_inner_product_wrt_states(
+            d_odes=adj, d_states=dU_m), dU_a)
+        + solver.compute_odes_wrt_vertices_inner_product_wrt_mach(
+            d_odes=adj, d_vertices=dX).item()
+        + np.vdot(solver.compute_odes_wrt_states_inner_product_wrt_vertices(
+            d_odes=adj, d_states=dU_m), dX)
+    )
+    if out is not None:
+        print("\nLift coefficient derivatives:", file=out)
+        print(f"{'wrt pitch angle:':<36} {cl_a.real:.4f} (1/rad)", file=out)
+        print(f"{'wrt pitch angle wrt Mach number:':<36} {cl_a_m.real:.4f} (1/rad)", file=out)
+    return float(cl_a.real), float(cl_a_m.real)
+
+
+def response_report(grid, mesh_name: str, chord: float, mach: float, axis_location: float,
+                    rtol: float = 1e-9, max_iter: int = 100, **solver_kw) -> str:
+    """The report of the response example for one grid (PTC + 11-point frequency response)."""
+    from .core import SpatialDiscretization
+
+    out = io.StringIO()
+    print(f"{'Mesh file:':<25} {mesh_name}", file=out)
+    print(f"{'Chord / L:':<25} {chord}", file=out)
+    print(f"{'Mach number:':<25} {mach}", file=out)
+    print(f"{'Axis location / L:':<25} {axis_location}", file=out)
+    s = SpatialDiscretization(grid, mach_number=mach, angle_of_attack=0., coefficient_length=chord,
+                              coefficient_center=(axis_location, 0.0), **solver_kw)
+    ptc(s, rtol, max_iter, out)
+    frequency_response(s, chord, axis_location, np.logspace(-2, 0, 11), out)
+    return out.getvalue()
+
+
+def gain_report(grid, mesh_name: str, chord: float, mach: float, rtol: float = 1e-9,
+                max_iter: int = 100, **solver_kw) -> str:
+    """The report of the gain example for one grid (PTC + lift slope and its Mach derivative)."""
+    from .core import SpatialDiscretization
+
+    out = io.StringIO()
+    print(f"{'Mesh file:':<25} {mesh_name}", file=out)
+    print(f"{'Chord / L:':<25} {chord}", file=out)
+    print(f"{'Mach number:':<25} {mach}", file=out)
+    s = SpatialDiscretization(grid, mach_number=mach, angle_of_attack=0., coefficient_length=chord,
+                              **solver_kw)
+    ptc(s, rtol, max_iter, out)
+    static_gain(s, out)
+    return out.getvalue()
