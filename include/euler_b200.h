@@ -65,7 +65,7 @@ typedef struct eb_instance {
 typedef struct eb_batch {
   const eb_instance* d_table;
   int32_t n_inst;
-  int32_t reserved;
+  int32_t max_dim;      /* largest M or N over the instances (0: only `single` is used) */
   int64_t n_cells;      /* total cells over all instances */
   int64_t n_verts;      /* total vertices over all instances */
   int64_t n_wall;       /* total wall faces (sum of N) over all instances */
@@ -85,6 +85,11 @@ int eb_set_free_stream_state(const eb_batch* b, double* U, void* stream);
 /* compute_odes, f90:496-537: R = R(Ma, U, X, V). V may be NULL (static grid). */
 int eb_compute_odes(const eb_batch* b, const double* X, const double* V, const double* U,
                     double* R, void* stream);
+
+/* The same residual by the plain one-thread-per-cell kernel (every stencil state read from
+ * global memory, the reference's per-face recomputation); a baseline for the tiled kernel. */
+int eb_compute_odes_untiled(const eb_batch* b, const double* X, const double* V,
+                            const double* U, double* R, void* stream);
 
 /* compute_forces, f90:1156-1174: F(:, n) = p(U(:, 1, n)) * normal(X(:, 1, n), X(:, 1, n+1)).
  * F is real (2, N) per instance at 2*wall_offset. coef (optional, may be NULL) receives per

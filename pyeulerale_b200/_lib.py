@@ -49,7 +49,7 @@ class Batch(ctypes.Structure):
     """``eb_batch``: a set of instances (single instance passed by value)."""
 
     _fields_ = [
-        ("d_table", ctypes.c_void_p), ("n_inst", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("d_table", ctypes.c_void_p), ("n_inst", ctypes.c_int32), ("max_dim", ctypes.c_int32),
         ("n_cells", ctypes.c_int64), ("n_verts", ctypes.c_int64), ("n_wall", ctypes.c_int64),
         ("single", Instance),
     ]
@@ -73,6 +73,7 @@ def single_batch(inst: Instance) -> Batch:
     b = Batch()
     b.d_table = None
     b.n_inst = 1
+    b.max_dim = max(inst.M, inst.N)
     b.n_cells = inst.M * inst.N
     b.n_verts = (inst.M + 1) * (inst.N + 1)
     b.n_wall = inst.N
@@ -83,6 +84,7 @@ def single_batch(inst: Instance) -> Batch:
 _SIGNATURES: dict[str, list] = {
     "eb_set_free_stream_state": ["b", "p", "s"],
     "eb_compute_odes": ["b", "p", "p", "p", "p", "s"],
+    "eb_compute_odes_untiled": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_forces": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_odes_wrt_mach": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_odes_wrt_states": ["b", "p", "p", "p", "p", "s"],

@@ -70,6 +70,7 @@ class InstanceSet:
         else:
             b.d_table = self.device_table.data_ptr()
         b.n_inst = n
+        b.max_dim = max(max(s.M, s.N) for s in specs)
         b.n_cells, b.n_verts, b.n_wall = c, v, w
         self.batch = b
 

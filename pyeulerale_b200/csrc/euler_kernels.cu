@@ -16,9 +16,15 @@
 #include <cstring>
 #include <string>
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace eb {
+
+int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
+                          double* R, cudaStream_t stream, int max_tiles);
+int residual_tiles(int M, int N);
 
 thread_local std::string g_last_error;
 
@@ -647,9 +653,21 @@ int eb_compute_odes(const eb_batch* b, const double* X, const double* V, const d
                     double* R, void* stream) {
   EB_VALIDATE(b);
   if (!X || !U || !R) return fail(EB_ERR_ARG, "null array");
+  int dim = b->max_dim;
+  if (b->n_inst == 1 && b->d_table == nullptr) dim = std::max(b->single.M, b->single.N);
+  if (dim < 5) return fail(EB_ERR_ARG, "batch max_dim must be the largest M or N");
+  return launch_residual_tiled(b, X, V, U, R, EB_STREAM(stream), residual_tiles(dim, dim));
+}
+
+// The untiled per-cell residual (one thread per cell, every stencil state from global memory).
+// Kept as the plain variant for comparison; the tiled kernel serves eb_compute_odes.
+int eb_compute_odes_untiled(const eb_batch* b, const double* X, const double* V, const double* U,
+                            double* R, void* stream) {
+  EB_VALIDATE(b);
+  if (!X || !U || !R) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_residual<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U, R);
-  return check_launch("compute_odes");
+  return check_launch("compute_odes_untiled");
 }
 
 int eb_compute_forces(const eb_batch* b, const double* X, const double* U, double* F,

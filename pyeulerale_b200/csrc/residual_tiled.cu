@@ -1,0 +1,296 @@
+// Tiled FP64 residual kernel: R(Ma, U, X, V) for packed instances (eb_compute_odes).
+//
+// One CTA computes a tile of kTM x kTN cells (radial x angular) of one instance:
+//  1. it stages the tile's states with a two-cell halo (the reach of the nine-point cross
+//     stencil, periodic in the angular index) and the tile's vertices and vertex velocities in
+//     shared memory, with coalesced 16-byte loads (consecutive threads = consecutive radial
+//     cells = consecutive 32-byte states);
+//  2. per staged state it computes once what every face needs: 1/rho, the pressure and the
+//     speed of sound (the reference recomputes these for each use, f90:128-171);
+//  3. per state it computes the two pressure sensors |p_a - 2 p_b + p_c| / (p_a + 2 p_b + p_c)
+//     centred on the state along the angular and the radial direction (each face's JST sensor
+//     is the max_c of the sensors centred on its two cells, f90:208-211; the wall and
+//     far-field rows use their ghost states as the missing neighbour);
+//  4. each thread evaluates the four faces of its cell in the cell's own orientation (the
+//     asymmetric max_c of the reference decides per cell, f90:111-120) and writes
+//     -(F_b + F_f + F_i + F_o) / area (f90:370-436).
+// Results agree with the reference to the rounding of the reordered arithmetic (<= 1e-12
+// relative); every branch (boundary cases, max_c tolerance) follows the reference.
+
+#include "common.cuh"
+
+namespace eb {
+
+constexpr int kTM = 32;                       // radial cells per tile (warp-contiguous)
+constexpr int kTN = 8;                        // angular cells per tile
+constexpr int kThreads = kTM * kTN;           // one thread per cell
+constexpr int kSR = kTM + 4;                  // staged rows (radial halo 2)
+constexpr int kSC = kTN + 4;                  // staged columns (angular halo 2)
+constexpr int kStaged = kSR * kSC;
+constexpr int kVR = kTM + 1, kVC = kTN + 1;   // staged vertices
+constexpr int kVerts = kVR * kVC;
+
+struct TileSmem {
+  double rho[kStaged], j1[kStaged], j2[kStaged], e[kStaged];
+  double p[kStaged], ir[kStaged], cs[kStaged];
+  double s_ang[kTM * (kTN + 2)];   // angular sensor centred on (r, c), c in [-1, kTN]
+  double s_rad[(kTM + 2) * kTN];   // radial sensor centred on (r, c), r in [-1, kTM]
+  double x[kVerts], z[kVerts], vx[kVerts], vz[kVerts];
+};
+
+__device__ __forceinline__ int sidx(int r, int c) { return (c + 2) * kSR + (r + 2); }
+__device__ __forceinline__ int vidx(int r, int c) { return c * kVR + r; }
+
+struct St {  // a state with its derived quantities
+  double rho, j1, j2, e, p, ir, cs;
+};
+
+__device__ __forceinline__ St derive(double rho, double j1, double j2, double e) {
+  St s;
+  s.rho = rho;
+  s.j1 = j1;
+  s.j2 = j2;
+  s.e = e;
+  s.ir = 1.0 / rho;
+  s.p = kGm1 * (e - (j1 * j1 + j2 * j2) * s.ir * 0.5);
+  s.cs = sqrt(kGamma * s.p * s.ir);
+  return s;
+}
+
+__device__ __forceinline__ St staged(const TileSmem& S, int i) {
+  return St{S.rho[i], S.j1[i], S.j2[i], S.e[i], S.p[i], S.ir[i], S.cs[i]};
+}
+
+__device__ __forceinline__ double sensor(double pa, double pb, double pc) {
+  return fabs(pa - 2.0 * pb + pc) / (pa + 2.0 * pb + pc);
+}
+
+__device__ __forceinline__ double max_cd(double x, double y) {
+  return (x > y + 1e-8) ? x : y;
+}
+
+// Wall ghost (make_wall_ghost_state, f90:231-240) of state s for face normal n, grid velocity g.
+__device__ __forceinline__ St wall_ghost_st(const St& s, double nx, double nz, double gx,
+                                            double gz) {
+  const double proj = nx * (s.j1 - gx * s.rho) + nz * (s.j2 - gz * s.rho);
+  const double nn = nx * nx + nz * nz;
+  return derive(s.rho, s.j1 - 2.0 * nx * proj / nn, s.j2 - 2.0 * nz * proj / nn, s.e);
+}
+
+// Far-field ghost (make_farfield_ghost_state, f90:269-274): 2 U_inf - U.
+__device__ __forceinline__ St farfield_ghost_st(const St& s, const Instance& in) {
+  const double speed = in.mach * sqrt(kGamma);
+  const double f1 = speed * in.cos_aoa, f2 = speed * in.sin_aoa;
+  const double fe = 1.0 / kGm1 + speed * speed / 2.0;
+  return derive(2.0 - s.rho, 2.0 * f1 - s.j1, 2.0 * f2 - s.j2, 2.0 * fe - s.e);
+}
+
+struct Flux {
+  double f[4];
+};
+
+// Central part + ALE term of make_face_flux (f90:197, 219) for l, r through normal (nx, nz)
+// with grid-velocity flux vn = g.n.
+__device__ __forceinline__ Flux central(const St& l, const St& r, double nx, double nz,
+                                       double vn) {
+  const double vl = (nx * l.j1 + nz * l.j2) * l.ir;
+  const double vr = (nx * r.j1 + nz * r.j2) * r.ir;
+  Flux F;
+  F.f[0] = (l.rho * vl + r.rho * vr) / 2.0 - (l.rho + r.rho) / 2.0 * vn;
+  F.f[1] = ((l.j1 * vl + nx * l.p) + (r.j1 * vr + nx * r.p)) / 2.0 - (l.j1 + r.j1) / 2.0 * vn;
+  F.f[2] = ((l.j2 * vl + nz * l.p) + (r.j2 * vr + nz * r.p)) / 2.0 - (l.j2 + r.j2) / 2.0 * vn;
+  F.f[3] = ((l.e + l.p) * vl + (r.e + r.p) * vr) / 2.0 - (l.e + r.e) / 2.0 * vn;
+  return F;
+}
+
+// make_face_flux with JST dissipation (f90:189-220); s1, s2 are the sensors centred on l and r.
+__device__ __forceinline__ Flux jst(const St& ll, const St& l, const St& r, const St& rr,
+                                   double nx, double nz, double len, double vn, double s1,
+                                   double s2, const Instance& in) {
+  const double vl = (nx * l.j1 + nz * l.j2) * l.ir;
+  const double vr = (nx * r.j1 + nz * r.j2) * r.ir;
+  const double lam = max_cd(fabs(vl) + l.cs * len, fabs(vr) + r.cs * len);
+  const double coef2 = in.k2 * max_cd(s1, s2) * lam;
+  const double c4 = in.k4 * lam - in.c4 * coef2;
+  const double coef4 = (0.0 > c4 + 1e-8) ? 0.0 : c4;
+  Flux F;
+  const double lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
+  const double llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
+  const double fl[4] = {l.rho * vl, l.j1 * vl + nx * l.p, l.j2 * vl + nz * l.p, (l.e + l.p) * vl};
+  const double fr[4] = {r.rho * vr, r.j1 * vr + nx * r.p, r.j2 * vr + nz * r.p, (r.e + r.p) * vr};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double c = (fl[k] + fr[k]) / 2.0;
+    c = c - (coef2 * (rv[k] - lv[k]) - coef4 * (rrv[k] - 3.0 * rv[k] + 3.0 * lv[k] - llv[k]));
+    F.f[k] = c - (lv[k] + rv[k]) / 2.0 * vn;
+  }
+  return F;
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_residual_tiled(Table t, const double* X, const double* V, const double* U, double* R) {
+  __shared__ TileSmem S;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;
+  const int M = in.M, N = in.N;
+  const int tiles_m = (M + kTM - 1) / kTM;
+  const int tiles = tiles_m * ((N + kTN - 1) / kTN);
+  if ((int)blockIdx.x >= tiles) return;
+  const int m0 = (blockIdx.x % tiles_m) * kTM, n0 = (blockIdx.x / tiles_m) * kTN;
+  const double* Ui = U + 4 * in.cell_offset;
+  const double* Xi = X + 2 * in.vert_offset;
+  const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
+  const int tid = threadIdx.x;
+
+  // 1. stage states (cross-shaped halo) and derived quantities
+  for (int e = tid; e < kStaged; e += kThreads) {
+    const int r = e % kSR - 2, c = e / kSR - 2;
+    const bool corner = (r < 0 || r >= kTM) && (c < 0 || c >= kTN);
+    const int m = m0 + r;
+    if (corner || m < 0 || m >= M) {
+      S.rho[e] = 1.0; S.j1[e] = 0.0; S.j2[e] = 0.0; S.e[e] = 1.0;
+      S.p[e] = 1.0; S.ir[e] = 1.0; S.cs[e] = 1.0;
+      continue;
+    }
+    const int n = wrap(n0 + c, N);
+    const double* q = Ui + 4 * (m + (int64_t)M * n);
+    const double2 a = __ldg(reinterpret_cast<const double2*>(q));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(q + 2));
+    const St s = derive(a.x, a.y, b.x, b.y);
+    S.rho[e] = s.rho; S.j1[e] = s.j1; S.j2[e] = s.j2; S.e[e] = s.e;
+    S.p[e] = s.p; S.ir[e] = s.ir; S.cs[e] = s.cs;
+  }
+  for (int e = tid; e < kVerts; e += kThreads) {
+    const int r = e % kVR, c = e / kVR;
+    const int m = min(m0 + r, M), n = min(n0 + c, N);
+    const int64_t v = m + (int64_t)(M + 1) * n;
+    const double2 xv = __ldg(reinterpret_cast<const double2*>(Xi + 2 * v));
+    S.x[e] = xv.x;
+    S.z[e] = xv.y;
+    if (Vi) {
+      const double2 vv = __ldg(reinterpret_cast<const double2*>(Vi + 2 * v));
+      S.vx[e] = vv.x;
+      S.vz[e] = vv.y;
+    } else {
+      S.vx[e] = 0.0;
+      S.vz[e] = 0.0;
+    }
+  }
+  __syncthreads();
+
+  // 2. sensors centred on each needed state
+  for (int e = tid; e < kTM * (kTN + 2); e += kThreads) {
+    const int r = e % kTM, c = e / kTM - 1;
+    S.s_ang[e] = sensor(S.p[sidx(r, c - 1)], S.p[sidx(r, c)], S.p[sidx(r, c + 1)]);
+  }
+  for (int e = tid; e < (kTM + 2) * kTN; e += kThreads) {
+    const int r = e % (kTM + 2) - 1, c = e / (kTM + 2);
+    const int m = m0 + r;
+    double s = 0.0;
+    if (m == 0) {  // inner neighbour: the wall ghost of this wall cell (face o, flag 1)
+      const double nx = S.z[vidx(r, c + 1)] - S.z[vidx(r, c)];
+      const double nz = S.x[vidx(r, c)] - S.x[vidx(r, c + 1)];
+      const double gx = (S.vx[vidx(r, c)] + S.vx[vidx(r, c + 1)]) / 2.0;
+      const double gz = (S.vz[vidx(r, c)] + S.vz[vidx(r, c + 1)]) / 2.0;
+      const St gh = wall_ghost_st(staged(S, sidx(r, c)), nx, nz, gx, gz);
+      s = sensor(gh.p, S.p[sidx(r, c)], S.p[sidx(r + 1, c)]);
+    } else if (m == M - 1) {  // outer neighbour: the far-field ghost (face i, flag 5)
+      const St gh = farfield_ghost_st(staged(S, sidx(r, c)), in);
+      s = sensor(gh.p, S.p[sidx(r, c)], S.p[sidx(r - 1, c)]);
+    } else if (m > 0 && m < M - 1) {
+      s = sensor(S.p[sidx(r - 1, c)], S.p[sidx(r, c)], S.p[sidx(r + 1, c)]);
+    }
+    S.s_rad[e] = s;
+  }
+  __syncthreads();
+
+  // 3. the cell's four faces
+  const int r = tid % kTM, c = tid / kTM;
+  const int m = m0 + r, n = n0 + c;
+  if (m >= M || n >= N) return;
+  const int flag = boundary_flag(M, m);
+  const double bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
+  const double fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
+  const double fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
+  const double box = S.x[vidx(r + 1, c)], boz = S.z[vidx(r + 1, c)];
+  const double gbix = S.vx[vidx(r, c)], gbiz = S.vz[vidx(r, c)];
+  const double gfix = S.vx[vidx(r, c + 1)], gfiz = S.vz[vidx(r, c + 1)];
+  const double gfox = S.vx[vidx(r + 1, c + 1)], gfoz = S.vz[vidx(r + 1, c + 1)];
+  const double gbox = S.vx[vidx(r + 1, c)], gboz = S.vz[vidx(r + 1, c)];
+  const double area = fabs((fox - bix) * (boz - fiz) - (foz - biz) * (box - fix)) / 2.0;
+  // normals (make_normal, f90:306-311) and grid velocities (make_grid_velo, f90:320-324)
+  const double nix = fiz - biz, niz = bix - fix;
+  const double nfx = foz - fiz, nfz = fix - fox;
+  const double nox = boz - foz, noz = fox - box;
+  const double nbx = biz - boz, nbz = box - bix;
+  const double vni = (gbix + gfix) / 2.0 * nix + (gbiz + gfiz) / 2.0 * niz;
+  const double vnf = (gfix + gfox) / 2.0 * nfx + (gfiz + gfoz) / 2.0 * nfz;
+  const double vno = (gfox + gbox) / 2.0 * nox + (gfoz + gboz) / 2.0 * noz;
+  const double vnb = (gbox + gbix) / 2.0 * nbx + (gboz + gbiz) / 2.0 * nbz;
+  const St C = staged(S, sidx(r, c));
+  const double sac = S.s_ang[c * kTM + r + kTM];          // angular sensor centred on c
+  const double src = S.s_rad[c * (kTM + 2) + r + 1];      // radial sensor centred on c
+  // face b (l = c, r = b, ll = f, rr = bb)
+  const Flux Fb = jst(staged(S, sidx(r, c + 1)), C, staged(S, sidx(r, c - 1)),
+                      staged(S, sidx(r, c - 2)), nbx, nbz, sqrt(nbx * nbx + nbz * nbz), vnb,
+                      sac, S.s_ang[(c - 1) * kTM + r + kTM], in);
+  // face f (l = c, r = f, ll = b, rr = ff)
+  const Flux Ff = jst(staged(S, sidx(r, c - 1)), C, staged(S, sidx(r, c + 1)),
+                      staged(S, sidx(r, c + 2)), nfx, nfz, sqrt(nfx * nfx + nfz * nfz), vnf,
+                      sac, S.s_ang[(c + 1) * kTM + r + kTM], in);
+  Flux Fi, Fo;
+  const double leni = sqrt(nix * nix + niz * niz), leno = sqrt(nox * nox + noz * noz);
+  switch (flag) {
+    case 1: {
+      const St G = wall_ghost_st(C, nix, niz, (gbix + gfix) / 2.0, (gbiz + gfiz) / 2.0);
+      Fi = central(C, G, nix, niz, vni);
+      Fo = jst(G, C, staged(S, sidx(r + 1, c)), staged(S, sidx(r + 2, c)), nox, noz, leno, vno,
+               src, S.s_rad[c * (kTM + 2) + r + 2], in);
+      break;
+    }
+    case 2:
+      Fi = central(C, staged(S, sidx(r - 1, c)), nix, niz, vni);
+      Fo = jst(staged(S, sidx(r - 1, c)), C, staged(S, sidx(r + 1, c)),
+               staged(S, sidx(r + 2, c)), nox, noz, leno, vno, src,
+               S.s_rad[c * (kTM + 2) + r + 2], in);
+      break;
+    case 5: {
+      const St G = farfield_ghost_st(C, in);
+      Fi = jst(G, C, staged(S, sidx(r - 1, c)), staged(S, sidx(r - 2, c)), nix, niz, leni, vni,
+               src, S.s_rad[c * (kTM + 2) + r], in);
+      Fo = central(C, G, nox, noz, vno);
+      break;
+    }
+    default:
+      Fi = jst(staged(S, sidx(r + 1, c)), C, staged(S, sidx(r - 1, c)),
+               staged(S, sidx(r - 2, c)), nix, niz, leni, vni, src,
+               S.s_rad[c * (kTM + 2) + r], in);
+      if (flag == 4) {
+        Fo = central(C, staged(S, sidx(r + 1, c)), nox, noz, vno);
+      } else {
+        Fo = jst(staged(S, sidx(r - 1, c)), C, staged(S, sidx(r + 1, c)),
+                 staged(S, sidx(r + 2, c)), nox, noz, leno, vno, src,
+                 S.s_rad[c * (kTM + 2) + r + 2], in);
+      }
+      break;
+  }
+  const double ia = 1.0 / area;
+  double* out = R + 4 * (in.cell_offset + m + (int64_t)M * n);
+  const double r0 = -(((Fb.f[0] + Ff.f[0]) + Fi.f[0]) + Fo.f[0]) * ia;
+  const double r1 = -(((Fb.f[1] + Ff.f[1]) + Fi.f[1]) + Fo.f[1]) * ia;
+  const double r2 = -(((Fb.f[2] + Ff.f[2]) + Fi.f[2]) + Fo.f[2]) * ia;
+  const double r3 = -(((Fb.f[3] + Ff.f[3]) + Fi.f[3]) + Fo.f[3]) * ia;
+  reinterpret_cast<double2*>(out)[0] = make_double2(r0, r1);
+  reinterpret_cast<double2*>(out)[1] = make_double2(r2, r3);
+}
+
+int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
+                          double* R, cudaStream_t stream, int max_tiles) {
+  const Table t = make_table(b);
+  dim3 grid(max_tiles, b->n_inst);
+  k_residual_tiled<<<grid, kThreads, 0, stream>>>(t, X, V, U, R);
+  return check_launch("compute_odes");
+}
+
+int residual_tiles(int M, int N) { return ((M + kTM - 1) / kTM) * ((N + kTN - 1) / kTN); }
+
+}  // namespace eb

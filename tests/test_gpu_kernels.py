@@ -152,3 +152,28 @@ def test_bsr_shifted_spmv(evaluated, oracle):
     oracle.apply_odes_wrt_states_fwd(g["J_u"], x, ref)
     ref = ref - shift * x
     assert rel_err(got, ref) <= TOL_APPLY, name
+
+
+@pytest.mark.parametrize("entry", ["eb_compute_odes", "eb_compute_odes_untiled"])
+def test_residual_uneven_batch(cuda, oracle, golden_grids, entry):
+    """One launch over instances of uneven sizes (partial tiles) and different flows."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    rng = np.random.default_rng(17)
+    grids = [G.naca_ogrid(33, 41, 0.12, 1.0, 20.0, 0.01), G.naca_ogrid(20, 13, 0.06, 2.0, 30.0, 0.05),
+             golden_grids["naca0004_129x129"], G.naca_ogrid(70, 37, 0.10, 1.0, 15.0, 0.02)]
+    flows = [(0.5, 1.25), (0.3, -2.0), (0.6, 3.0), (0.45, 0.0)]
+    specs = [InstanceSpec(X, ma, a) for X, (ma, a) in zip(grids, flows)]
+    states = [G.perturbed_states(s.M, s.N, s.mach, s.aoa_deg, 0.01, rng) for s in specs]
+    vels = [G.smooth_velocities(X, rng) for X in grids]
+    inst = InstanceSet(specs)
+    dX = cuda.from_numpy(inst.pack_vertices()).cuda()
+    dV = cuda.from_numpy(inst.pack_vertices(vels)).cuda()
+    dU = cuda.from_numpy(inst.pack_cells(states)).cuda()
+    dR = cuda.zeros(4 * inst.n_cells, dtype=cuda.float64, device="cuda")
+    inst.call(entry, dX, dV, dU, dR)
+    got = inst.unpack_cells(dR.cpu().numpy())
+    for k, (s, X, V, U) in enumerate(zip(specs, grids, vels, states)):
+        ref = oracle_eval(oracle, dict(X=X, V=V, U=U, mach=s.mach, aoa=s.aoa_deg))["R"]
+        assert rel_err(got[k], ref) <= TOL_R, (entry, k, rel_err(got[k], ref))
