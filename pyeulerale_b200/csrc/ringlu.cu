@@ -24,6 +24,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -44,12 +45,15 @@ struct Handles {
   cusolverDnHandle_t solver = nullptr;
 };
 
-thread_local Handles g_handles;
+// One cuBLAS / cuSOLVER handle pair per concurrent stream slot (a handle's internal workspace
+// must not be shared by work that overlaps on the device). A deque keeps the pointers stable.
+thread_local std::deque<Handles> g_handles;
 
-int handles(cudaStream_t st, Handles*& h) {
+int handles(int slot, cudaStream_t st, Handles*& h) {
   int dev = 0;
   cudaGetDevice(&dev);
-  h = &g_handles;
+  while ((int)g_handles.size() <= slot) g_handles.emplace_back();
+  h = &g_handles[slot];
   if (h->device != dev) {
     if (h->blas) cublasDestroy(h->blas);
     if (h->solver) cusolverDnDestroy(h->solver);
@@ -140,19 +144,47 @@ __global__ void k_assemble(int M, int N, const double* J, double sr, double si,
   }
 }
 
-// X <- X P^T for the row pivots of getrf (column interchanges in reverse order), one thread
-// per row of X.
-__global__ void k_col_pivots(int K, const int* ipiv, cuDoubleComplex* X) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= K) return;
-  for (int k = K - 1; k >= 0; --k) {
-    const int p = ipiv[k] - 1;
-    if (p != k) {
-      const cuDoubleComplex t = X[(int64_t)k * K + row];
-      X[(int64_t)k * K + row] = X[(int64_t)p * K + row];
-      X[(int64_t)p * K + row] = t;
+// X <- X P^T for the row pivots of getrf (the column interchanges applied in reverse order).
+// Each CTA first composes the interchanges into one permutation in shared memory, then moves
+// a tile of `rows` rows of X through shared memory in permuted column order.
+__global__ void k_col_pivots(int K, int rows, const int* ipiv, cuDoubleComplex* X) {
+  extern __shared__ __align__(16) unsigned char pv_smem[];
+  cuDoubleComplex* tile = reinterpret_cast<cuDoubleComplex*>(pv_smem);
+  int* idx = reinterpret_cast<int*>(tile + (size_t)rows * K);
+  for (int j = threadIdx.x; j < K; j += blockDim.x) idx[j] = j;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = K - 1; k >= 0; --k) {
+      const int p = ipiv[k] - 1;
+      if (p != k) {
+        const int t = idx[k];
+        idx[k] = idx[p];
+        idx[p] = t;
+      }
     }
   }
+  const int r0 = blockIdx.x * rows;
+  const int nr = min(rows, K - r0);
+  for (int e = threadIdx.x; e < nr * K; e += blockDim.x) {
+    const int rr = e % nr, col = e / nr;
+    tile[(size_t)rr * K + col] = X[(int64_t)col * K + r0 + rr];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nr * K; e += blockDim.x) {
+    const int rr = e % nr, col = e / nr;
+    X[(int64_t)col * K + r0 + rr] = tile[(size_t)rr * K + idx[col]];
+  }
+}
+
+// Rows per CTA of k_col_pivots: up to 8, within 200 KB of shared memory.
+inline int pivot_rows(int K) {
+  const size_t budget = 200 * 1024 - sizeof(int) * (size_t)K;
+  const size_t per_row = sizeof(cuDoubleComplex) * (size_t)K;
+  const int r = per_row > budget ? 0 : (int)(budget / per_row);
+  return r > 8 ? 8 : r;
+}
+inline size_t pivot_smem(int K, int rows) {
+  return (size_t)rows * K * sizeof(cuDoubleComplex) + sizeof(int) * (size_t)K;
 }
 
 // Reference layout (4, M, N) <-> ring layout [m][n][v].
@@ -306,9 +338,9 @@ using namespace eb::rl;
 extern "C" {
 
 int64_t eb_ringlu_workspace_bytes(int M, int N) {
-  if (M < 4 || N < 5) return -1;
+  if (M < 4 || N < 5 || pivot_rows(4 * N) < 1) return -1;
   Handles* h = nullptr;
-  if (handles(nullptr, h) != EB_OK) return -1;
+  if (handles(0, nullptr, h) != EB_OK) return -1;
   const int K = 4 * N;
   int lwork = 0;
   if (cusolverDnZgetrf_bufferSize(h->solver, K, K, nullptr, K, &lwork) != CUSOLVER_STATUS_SUCCESS)
@@ -316,60 +348,53 @@ int64_t eb_ringlu_workspace_bytes(int M, int N) {
   return (int64_t)plan(M, N, lwork).total;
 }
 
-int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double shift_im,
-                     void* workspace, int64_t workspace_bytes, void* stream) {
-  int rc = validate(b);
-  if (rc != EB_OK) return rc;
-  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
-  if (!J || !workspace) return fail(EB_ERR_ARG, "ringlu: null argument");
-  const int M = b->single.M, N = b->single.N, K = 4 * N;
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  Handles* h = nullptr;
-  if ((rc = handles(st, h)) != EB_OK) return rc;
-  int lwork = 0;
-  cusolverDnZgetrf_bufferSize(h->solver, K, K, nullptr, K, &lwork);
-  const Layout L = plan(M, N, lwork);
-  if ((int64_t)L.total > workspace_bytes) return fail(EB_ERR_ARG, "ringlu: workspace too small");
-  Factor F{L, static_cast<char*>(workspace)};
-  cudaMemsetAsync(F.base, 0, L.off_piv, st);  // the five block arrays
-  k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
-      M, N, J, shift_re, shift_im, F.blk(L.off_D, 0), F.blk(L.off_L1, 0), F.blk(L.off_L2, 0),
-      F.blk(L.off_C1, 0), F.blk(L.off_C2, 0));
-  if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
+}  // extern "C"
+
+namespace eb {
+namespace rl {
+
+// One ring of the block elimination for one factorisation (all work on stream st).
+int factor_ring(Handles* h, const Factor& f, int m, cudaStream_t st) {
+  const Layout& L = f.L;
+  const int M = L.M, K = L.K;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
   const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
-  int* info = reinterpret_cast<int*>(F.base + L.off_info);
-  cuDoubleComplex* work = reinterpret_cast<cuDoubleComplex*>(F.base + L.off_work);
-  for (int m = 0; m < M; ++m) {
-    cuDoubleComplex* D = F.blk(L.off_D, m);
-    if (cusolverDnZgetrf(h->solver, K, K, D, K, work, F.piv(m), info + m) != CUSOLVER_STATUS_SUCCESS)
-      return fail(EB_ERR_CUDA, "ringlu: getrf failed");
-    // L_a[m+a] = B_a[m+a] D_m^-1 = B U^-1 L^-1 P^T
-    for (int a = 1; a <= 2; ++a) {
-      if (m + a >= M) continue;
-      cuDoubleComplex* X = F.blk(a == 1 ? L.off_L1 : L.off_L2, m + a);
-      cublasZtrsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                  CUBLAS_DIAG_NON_UNIT, K, K, &one, D, K, X, K);
-      cublasZtrsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                  CUBLAS_DIAG_UNIT, K, K, &one, D, K, X, K);
-      k_col_pivots<<<(K + 127) / 128, 128, 0, st>>>(K, F.piv(m), X);
-    }
-    // Schur complements of the next two rings
-    if (m + 1 < M)
-      cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, F.blk(L.off_L1, m + 1), K,
-                  F.blk(L.off_C1, m), K, &one, F.blk(L.off_D, m + 1), K);
-    if (m + 2 < M) {
-      cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, F.blk(L.off_L2, m + 2), K,
-                  F.blk(L.off_C2, m), K, &one, F.blk(L.off_D, m + 2), K);
-      cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, F.blk(L.off_L2, m + 2), K,
-                  F.blk(L.off_C1, m), K, &one, F.blk(L.off_L1, m + 2), K);
-      cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, F.blk(L.off_L1, m + 1), K,
-                  F.blk(L.off_C2, m), K, &one, F.blk(L.off_C1, m + 1), K);
-    }
+  int* info = reinterpret_cast<int*>(f.base + L.off_info);
+  cuDoubleComplex* work = reinterpret_cast<cuDoubleComplex*>(f.base + L.off_work);
+  cuDoubleComplex* D = f.blk(L.off_D, m);
+  if (cusolverDnZgetrf(h->solver, K, K, D, K, work, f.piv(m), info + m) != CUSOLVER_STATUS_SUCCESS)
+    return fail(EB_ERR_CUDA, "ringlu: getrf failed");
+  // L_a[m+a] = B_a[m+a] D_m^-1 = B U^-1 L^-1 P^T
+  for (int a = 1; a <= 2; ++a) {
+    if (m + a >= M) continue;
+    cuDoubleComplex* X = f.blk(a == 1 ? L.off_L1 : L.off_L2, m + a);
+    cublasZtrsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                CUBLAS_DIAG_NON_UNIT, K, K, &one, D, K, X, K);
+    cublasZtrsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                CUBLAS_DIAG_UNIT, K, K, &one, D, K, X, K);
+    const int rows = pivot_rows(K);
+    k_col_pivots<<<(K + rows - 1) / rows, 256, pivot_smem(K, rows), st>>>(K, rows, f.piv(m), X);
   }
-  if ((rc = check_launch("ringlu factor")) != EB_OK) return rc;
+  // Schur complements of the next two rings
+  if (m + 1 < M)
+    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L1, m + 1), K,
+                f.blk(L.off_C1, m), K, &one, f.blk(L.off_D, m + 1), K);
+  if (m + 2 < M) {
+    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L2, m + 2), K,
+                f.blk(L.off_C2, m), K, &one, f.blk(L.off_D, m + 2), K);
+    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L2, m + 2), K,
+                f.blk(L.off_C1, m), K, &one, f.blk(L.off_L1, m + 2), K);
+    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L1, m + 1), K,
+                f.blk(L.off_C2, m), K, &one, f.blk(L.off_C1, m + 1), K);
+  }
+  return EB_OK;
+}
+
+int check_info(const Factor& f, cudaStream_t st) {
+  const int M = f.L.M;
   std::vector<int> hinfo(M);
-  if (cudaMemcpyAsync(hinfo.data(), info, sizeof(int) * M, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+  if (cudaMemcpyAsync(hinfo.data(), f.base + f.L.off_info, sizeof(int) * M,
+                      cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return check_launch("ringlu info");
   for (int m = 0; m < M; ++m)
@@ -377,52 +402,144 @@ int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double
   return EB_OK;
 }
 
+}  // namespace rl
+}  // namespace eb
+
+extern "C" {
+
+int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts,
+                          const double* shifts, void* const* workspaces, int64_t workspace_bytes,
+                          void* const* streams) {
+  int rc = validate(b);
+  if (rc != EB_OK) return rc;
+  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
+  if (!J || !workspaces || !shifts || n_shifts < 1) return fail(EB_ERR_ARG, "ringlu: null argument");
+  const int M = b->single.M, N = b->single.N, K = 4 * N;
+  auto stream_of = [&](int s) {
+    return streams ? reinterpret_cast<cudaStream_t>(streams[s]) : (cudaStream_t) nullptr;
+  };
+  std::vector<Handles*> h(n_shifts);
+  for (int s = 0; s < n_shifts; ++s)
+    if ((rc = handles(s, stream_of(s), h[s])) != EB_OK) return rc;
+  int lwork = 0;
+  cusolverDnZgetrf_bufferSize(h[0]->solver, K, K, nullptr, K, &lwork);
+  const Layout L = plan(M, N, lwork);
+  if ((int64_t)L.total > workspace_bytes) return fail(EB_ERR_ARG, "ringlu: workspace too small");
+  if (cudaFuncSetAttribute(k_col_pivots, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)pivot_smem(K, pivot_rows(K))) != cudaSuccess)
+    return check_launch("ringlu pivot attribute");
+  std::vector<Factor> F(n_shifts);
+  for (int s = 0; s < n_shifts; ++s) {
+    if (!workspaces[s]) return fail(EB_ERR_ARG, "ringlu: null workspace");
+    F[s] = Factor{L, static_cast<char*>(workspaces[s])};
+    cudaStream_t st = stream_of(s);
+    cudaMemsetAsync(F[s].base, 0, L.off_piv, st);  // the five block arrays
+    k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
+        M, N, J, shifts[2 * s], shifts[2 * s + 1], F[s].blk(L.off_D, 0), F[s].blk(L.off_L1, 0),
+        F[s].blk(L.off_L2, 0), F[s].blk(L.off_C1, 0), F[s].blk(L.off_C2, 0));
+  }
+  if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
+  // Ring by ring; within a ring every shift's independent work goes to its own stream, so
+  // the latency-bound dense steps of different shifts overlap on the GPU.
+  for (int m = 0; m < M; ++m)
+    for (int s = 0; s < n_shifts; ++s)
+      if ((rc = factor_ring(h[s], F[s], m, stream_of(s))) != EB_OK) return rc;
+  if ((rc = check_launch("ringlu factor")) != EB_OK) return rc;
+  for (int s = 0; s < n_shifts; ++s)
+    if ((rc = check_info(F[s], stream_of(s))) != EB_OK) return rc;
+  return EB_OK;
+}
+
+int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double shift_im,
+                     void* workspace, int64_t workspace_bytes, void* stream) {
+  const double shift[2] = {shift_re, shift_im};
+  void* ws[1] = {workspace};
+  void* st[1] = {stream};
+  return eb_ringlu_factor_many(b, J, 1, shift, ws, workspace_bytes, st);
+}
+
+int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
+                         int adjoint, void* const* workspaces, int64_t workspace_bytes,
+                         const double* const* rhs, double* const* x, double tol, int max_refine,
+                         double* rel_residuals, void* const* streams) {
+  int rc = validate(b);
+  if (rc != EB_OK) return rc;
+  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
+  if (!J || !workspaces || !shifts || !rhs || !x || n_shifts < 1)
+    return fail(EB_ERR_ARG, "ringlu: null argument");
+  for (int s = 0; s < n_shifts; ++s)
+    if (!workspaces[s] || !rhs[s] || !x[s]) return fail(EB_ERR_ARG, "ringlu: null argument");
+  const int M = b->single.M, N = b->single.N, K = 4 * N;
+  auto stream_of = [&](int s) {
+    return streams ? reinterpret_cast<cudaStream_t>(streams[s]) : (cudaStream_t) nullptr;
+  };
+  std::vector<Handles*> h(n_shifts);
+  for (int s = 0; s < n_shifts; ++s)
+    if ((rc = handles(s, stream_of(s), h[s])) != EB_OK) return rc;
+  int lwork = 0;
+  cusolverDnZgetrf_bufferSize(h[0]->solver, K, K, nullptr, K, &lwork);
+  const Layout L = plan(M, N, lwork);
+  if ((int64_t)L.total > workspace_bytes) return fail(EB_ERR_ARG, "ringlu: workspace too small");
+  const int gc = grid_for((int64_t)M * N, 128);
+  std::vector<Factor> F(n_shifts);
+  std::vector<double> rel(n_shifts, INFINITY);
+  std::vector<char> active(n_shifts, 1);
+  for (int s = 0; s < n_shifts; ++s) F[s] = Factor{L, static_cast<char*>(workspaces[s])};
+  auto y_of = [&](int s) { return reinterpret_cast<cuDoubleComplex*>(F[s].base + L.off_y); };
+  auto r_of = [&](int s) { return reinterpret_cast<double*>(F[s].base + L.off_r); };
+  // two doubles of scratch for the norms (the x ring vector is not used by the solve)
+  auto acc_of = [&](int s) { return reinterpret_cast<double*>(F[s].base + L.off_x); };
+  // x = A^-1 b, then refine x += A^-1 (b - A x) until the relative residual reaches tol. Every
+  // pass issues the work of all unfinished shifts on their streams before reading any norm.
+  for (int it = 0;; ++it) {
+    int n_active = 0;
+    for (int s = 0; s < n_shifts; ++s) {
+      if (!active[s]) continue;
+      ++n_active;
+      cudaStream_t st = stream_of(s);
+      k_to_rings<<<gc, 128, 0, st>>>(M, N, it == 0 ? rhs[s] : r_of(s), y_of(s));
+      if ((rc = ring_solve(h[s], F[s], y_of(s), adjoint != 0)) != EB_OK) return rc;
+      k_from_rings<<<gc, 128, 0, st>>>(M, N, y_of(s), x[s], it == 0 ? 0 : 1);
+      cudaMemsetAsync(acc_of(s), 0, 2 * sizeof(double), st);
+      k_residual_op<<<gc, 128, 0, st>>>(M, N, J, shifts[2 * s], shifts[2 * s + 1], adjoint, x[s],
+                                        rhs[s], r_of(s), acc_of(s));
+    }
+    if (n_active == 0) break;
+    if ((rc = check_launch("ringlu solve")) != EB_OK) return rc;
+    for (int s = 0; s < n_shifts; ++s) {
+      if (!active[s]) continue;
+      double hacc[2];
+      if (cudaMemcpyAsync(hacc, acc_of(s), sizeof(hacc), cudaMemcpyDeviceToHost, stream_of(s)) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(stream_of(s)) != cudaSuccess)
+        return check_launch("ringlu residual");
+      rel[s] = hacc[1] > 0 ? std::sqrt(hacc[0] / hacc[1]) : std::sqrt(hacc[0]);
+      if (!std::isfinite(rel[s])) {
+        if (rel_residuals)
+          for (int q = 0; q < n_shifts; ++q) rel_residuals[q] = rel[q];
+        return fail(EB_ERR_NAN, "ringlu: non-finite residual");
+      }
+      if (rel[s] <= tol || it >= max_refine) active[s] = 0;
+    }
+  }
+  if (rel_residuals)
+    for (int s = 0; s < n_shifts; ++s) rel_residuals[s] = rel[s];
+  for (int s = 0; s < n_shifts; ++s)
+    if (rel[s] > tol) return fail(EB_ERR_NOCONV, "ringlu: refinement did not reach the tolerance");
+  return EB_OK;
+}
+
 int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double shift_im,
                     int adjoint, const void* workspace, int64_t workspace_bytes,
                     const double* rhs, double* x, double tol, int max_refine,
                     double* rel_residual, void* stream) {
-  int rc = validate(b);
-  if (rc != EB_OK) return rc;
-  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
-  if (!J || !workspace || !rhs || !x) return fail(EB_ERR_ARG, "ringlu: null argument");
-  const int M = b->single.M, N = b->single.N, K = 4 * N;
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  Handles* h = nullptr;
-  if ((rc = handles(st, h)) != EB_OK) return rc;
-  int lwork = 0;
-  cusolverDnZgetrf_bufferSize(h->solver, K, K, nullptr, K, &lwork);
-  const Layout L = plan(M, N, lwork);
-  if ((int64_t)L.total > workspace_bytes) return fail(EB_ERR_ARG, "ringlu: workspace too small");
-  Factor F{L, static_cast<char*>(const_cast<void*>(workspace))};
-  cuDoubleComplex* y = reinterpret_cast<cuDoubleComplex*>(F.base + L.off_y);
-  double* r = reinterpret_cast<double*>(F.base + L.off_r);
-  double* acc = reinterpret_cast<double*>(F.base + L.off_x);  // two doubles of scratch
-  const int gc = grid_for((int64_t)M * N, 128);
-  // x = A^-1 b, then refine x += A^-1 (b - A x) until the relative residual reaches tol
-  k_to_rings<<<gc, 128, 0, st>>>(M, N, rhs, y);
-  if ((rc = ring_solve(h, F, y, adjoint != 0)) != EB_OK) return rc;
-  k_from_rings<<<gc, 128, 0, st>>>(M, N, y, x, 0);
-  double rel = INFINITY;
-  for (int it = 0;; ++it) {
-    cudaMemsetAsync(acc, 0, 2 * sizeof(double), st);
-    k_residual_op<<<gc, 128, 0, st>>>(M, N, J, shift_re, shift_im, adjoint, x, rhs, r, acc);
-    double hacc[2];
-    if (cudaMemcpyAsync(hacc, acc, sizeof(hacc), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return check_launch("ringlu residual");
-    rel = hacc[1] > 0 ? std::sqrt(hacc[0] / hacc[1]) : std::sqrt(hacc[0]);
-    if (!std::isfinite(rel)) {
-      if (rel_residual) *rel_residual = rel;
-      return fail(EB_ERR_NAN, "ringlu: non-finite residual");
-    }
-    if (rel <= tol || it >= max_refine) break;
-    k_to_rings<<<gc, 128, 0, st>>>(M, N, r, y);
-    if ((rc = ring_solve(h, F, y, adjoint != 0)) != EB_OK) return rc;
-    k_from_rings<<<gc, 128, 0, st>>>(M, N, y, x, 1);
-  }
-  if (rel_residual) *rel_residual = rel;
-  if (rel > tol) return fail(EB_ERR_NOCONV, "ringlu: refinement did not reach the tolerance");
-  return check_launch("ringlu solve");
+  const double shift[2] = {shift_re, shift_im};
+  void* ws[1] = {const_cast<void*>(workspace)};
+  const double* in[1] = {rhs};
+  double* out[1] = {x};
+  void* st[1] = {stream};
+  return eb_ringlu_solve_many(b, J, 1, shift, adjoint, ws, workspace_bytes, in, out, tol,
+                              max_refine, rel_residual, st);
 }
 
 }  // extern "C"

@@ -108,6 +108,36 @@ def solve_shifted(batch: _lib.Batch, J, rhs, shifts, *, adjoint: bool = False,
     return x, info
 
 
+def _bind_ringlu() -> ctypes.CDLL:
+    lib = _lib.load()
+    if not getattr(lib, "_ringlu_bound", False):
+        P = ctypes.c_void_p
+        lib.eb_ringlu_workspace_bytes.restype = ctypes.c_int64
+        lib.eb_ringlu_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+        lib.eb_ringlu_factor.restype = ctypes.c_int
+        lib.eb_ringlu_factor.argtypes = [ctypes.POINTER(_lib.Batch), P, ctypes.c_double,
+                                         ctypes.c_double, P, ctypes.c_int64, P]
+        lib.eb_ringlu_solve.restype = ctypes.c_int
+        lib.eb_ringlu_solve.argtypes = [
+            ctypes.POINTER(_lib.Batch), P, ctypes.c_double, ctypes.c_double, ctypes.c_int, P,
+            ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+            P]
+        lib.eb_ringlu_factor_many.restype = ctypes.c_int
+        lib.eb_ringlu_factor_many.argtypes = [ctypes.POINTER(_lib.Batch), P, ctypes.c_int, P, P,
+                                              ctypes.c_int64, P]
+        lib.eb_ringlu_solve_many.restype = ctypes.c_int
+        lib.eb_ringlu_solve_many.argtypes = [
+            ctypes.POINTER(_lib.Batch), P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int64, P, P,
+            ctypes.c_double, ctypes.c_int, P, P]
+        lib._ringlu_bound = True
+    return lib
+
+
+def ringlu_workspace_bytes(M: int, N: int) -> int:
+    """Device bytes of one ring-LU factorisation of an M x N cell grid (-1: unsupported)."""
+    return int(_bind_ringlu().eb_ringlu_workspace_bytes(int(M), int(N)))
+
+
 class RingLU:
     """Direct resolvent of one instance: ring-block LU factors of ``J - shift I`` on the device.
 
@@ -123,20 +153,7 @@ class RingLU:
         self.batch = batch
         self.tol = tol
         self.max_refine = max_refine
-        lib = _lib.load()
-        if not getattr(lib, "_ringlu_bound", False):
-            lib.eb_ringlu_workspace_bytes.restype = ctypes.c_int64
-            lib.eb_ringlu_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
-            lib.eb_ringlu_factor.restype = ctypes.c_int
-            lib.eb_ringlu_factor.argtypes = [ctypes.POINTER(_lib.Batch), ctypes.c_void_p,
-                                             ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
-                                             ctypes.c_int64, ctypes.c_void_p]
-            lib.eb_ringlu_solve.restype = ctypes.c_int
-            lib.eb_ringlu_solve.argtypes = [
-                ctypes.POINTER(_lib.Batch), ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
-                ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
-                ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
-            lib._ringlu_bound = True
+        lib = _bind_ringlu()
         self._lib = lib
         need = lib.eb_ringlu_workspace_bytes(batch.single.M, batch.single.N)
         if need < 0:
@@ -171,6 +188,98 @@ class RingLU:
             raise _lib.EulerB200Error("eb_ringlu_solve", rc,
                                       self._lib.eb_last_error().decode() + f" (rel {rel.value})")
         return x, rel.value
+
+
+class RingLUMany:
+    """Ring-LU factors of ``J - s I`` for several shifts ``s`` of one instance at once.
+
+    ``factor(J, shifts)`` runs ``eb_ringlu_factor_many``: the shifts' dense ring steps go to one
+    CUDA stream per shift and overlap on the device. ``solve(rhs, adjoint)`` solves one
+    right-hand side per shift through ``eb_ringlu_solve_many`` the same way. ``capacity``
+    fixes the number of workspaces (each ``ringlu_workspace_bytes(M, N)`` bytes).
+    """
+
+    def __init__(self, batch: _lib.Batch, capacity: int, tol: float = 1e-10,
+                 max_refine: int = 4) -> None:
+        import torch
+
+        self._torch = torch
+        self._lib = _bind_ringlu()
+        self.batch, self.tol, self.max_refine = batch, tol, max_refine
+        need = self._lib.eb_ringlu_workspace_bytes(batch.single.M, batch.single.N)
+        if need < 0:
+            raise ValueError("ring LU needs a single instance with M >= 4, N >= 5")
+        self.bytes = int(need)
+        self.workspaces = [torch.empty(self.bytes, dtype=torch.uint8, device="cuda")
+                           for _ in range(int(capacity))]
+        self.streams = [torch.cuda.Stream() for _ in range(int(capacity))]
+        self.J = None
+        self.shifts: list[complex] = []
+
+    @property
+    def capacity(self) -> int:
+        return len(self.workspaces)
+
+    def _ptrs(self, n: int):
+        ws = (ctypes.c_void_p * n)(*[w.data_ptr() for w in self.workspaces[:n]])
+        st = (ctypes.c_void_p * n)(*[s.cuda_stream for s in self.streams[:n]])
+        return ws, st
+
+    def _join(self, n: int) -> None:
+        cur = self._torch.cuda.current_stream()
+        for s in self.streams[:n]:
+            cur.wait_stream(s)
+
+    def _fork(self, n: int) -> None:
+        cur = self._torch.cuda.current_stream()
+        for s in self.streams[:n]:
+            s.wait_stream(cur)
+
+    def factor(self, J, shifts) -> None:
+        shifts = [complex(v) for v in np.atleast_1d(shifts)]
+        n = len(shifts)
+        if not 1 <= n <= self.capacity:
+            raise ValueError(f"{n} shifts for {self.capacity} workspaces")
+        sh = np.zeros(2 * n)
+        sh[0::2] = np.real(shifts)
+        sh[1::2] = np.imag(shifts)
+        ws, st = self._ptrs(n)
+        self._fork(n)
+        rc = self._lib.eb_ringlu_factor_many(ctypes.byref(self.batch), J.data_ptr(), n,
+                                             sh.ctypes.data, ws, self.bytes, st)
+        self._join(n)
+        if rc != _lib.EB_OK:
+            raise _lib.EulerB200Error("eb_ringlu_factor_many", rc,
+                                      self._lib.eb_last_error().decode())
+        self.J, self.shifts = J, shifts
+
+    def solve(self, rhs, adjoint: bool = False, out=None):
+        """Solves system ``s`` for ``rhs[s]`` (a sequence of, or a stacked, device tensor);
+        returns ``(x, rel_residuals)`` with ``x`` stacked like ``rhs``."""
+        if self.J is None:
+            raise RuntimeError("factor() first")
+        n = len(self.shifts)
+        if len(rhs) != n:
+            raise ValueError(f"{len(rhs)} right-hand sides for {n} shifts")
+        torch = self._torch
+        x = (torch.empty_like(rhs) if isinstance(rhs, torch.Tensor)
+             else [torch.empty_like(r) for r in rhs]) if out is None else out
+        sh = np.zeros(2 * n)
+        sh[0::2] = np.real(self.shifts)
+        sh[1::2] = np.imag(self.shifts)
+        ws, st = self._ptrs(n)
+        rp = (ctypes.c_void_p * n)(*[rhs[k].data_ptr() for k in range(n)])
+        xp = (ctypes.c_void_p * n)(*[x[k].data_ptr() for k in range(n)])
+        rel = (ctypes.c_double * n)()
+        self._fork(n)
+        rc = self._lib.eb_ringlu_solve_many(ctypes.byref(self.batch), self.J.data_ptr(), n,
+                                            sh.ctypes.data, 1 if adjoint else 0, ws, self.bytes,
+                                            rp, xp, self.tol, self.max_refine, rel, st)
+        self._join(n)
+        if rc != _lib.EB_OK:
+            raise _lib.EulerB200Error("eb_ringlu_solve_many", rc,
+                                      self._lib.eb_last_error().decode() + f" (rel {list(rel)})")
+        return x, list(rel)
 
 
 def solve_shifted_noalloc(batch: _lib.Batch, J, rhs, shifts, *, adjoint: bool = False,

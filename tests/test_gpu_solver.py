@@ -100,3 +100,50 @@ def test_ringlu_direct_solve(cuda, oracle, golden_grids, name, shift):
         if n <= 20000:
             ref = spla.spsolve(op, bf)
             assert rel_err(got, ref) <= 1e-7, (name, shift, adjoint)
+
+
+def test_ringlu_odd_ring_size(cuda, oracle):
+    """A ring of 4 N unknowns that is not a multiple of the pivot kernel's row tile (N = 13)."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200 import solver
+
+    X = G.naca_ogrid(21, 14, 0.12, 1.0, 20.0, 0.01)
+    rng = np.random.default_rng(6)
+    case = dict(X=X, V=np.zeros_like(X), U=G.perturbed_states(20, 13, 0.5, 1.25, 0.01, rng),
+                mach=0.5, aoa=1.25)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    b = crandn(rng, (4, 20, 13))
+    lu = solver.RingLU(gpu.batch, tol=1e-10)
+    shift = 0.2 + 0.4j
+    lu.factor(g["_dev"]["J_u"], shift)
+    x, rel = lu.solve(gpu.dev(b))
+    A = bsr_matrix(oracle, g["J_u"]).astype(complex)
+    op = (A - shift * sp.eye(A.shape[0])).tocsc()
+    ref = spla.spsolve(op, b.ravel(order="F"))
+    got = gpu.host(x, (4, 20, 13), complex_=True).ravel(order="F")
+    assert rel <= 1e-10 and rel_err(got, ref) <= 1e-8, rel
+
+
+@pytest.mark.parametrize("name", ["naca0012_33", "naca0004_129"])
+def test_ringlu_many_matches_single(cuda, golden_grids, name):
+    """Concurrent multi-shift factor / solve == one factorisation per shift, both directions."""
+    from pyeulerale_b200 import solver
+
+    case = make_case(name, golden_grids, seed=3)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(12)
+    shifts = [1j * k for k in (0.01, 0.3, 4.0)] + [0.0, 2.0 - 0.5j]
+    rhs = [gpu.dev(crandn(rng, (4, M, N))) for _ in shifts]
+    many = solver.RingLUMany(gpu.batch, capacity=len(shifts), tol=1e-10)
+    many.factor(g["_dev"]["J_u"], shifts)
+    one = solver.RingLU(gpu.batch, tol=1e-10)
+    for adjoint in (False, True):
+        xs, rels = many.solve(rhs, adjoint=adjoint)
+        assert max(rels) <= 1e-10, rels
+        for k, s in enumerate(shifts):
+            one.factor(g["_dev"]["J_u"], s)
+            x1, _ = one.solve(rhs[k], adjoint=adjoint)
+            assert rel_err(xs[k].cpu().numpy(), x1.cpu().numpy()) <= 1e-9, (name, k, adjoint)
