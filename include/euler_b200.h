@@ -235,16 +235,15 @@ int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double
                      void* workspace, int64_t workspace_bytes, void* stream);
 
 /* eb_ringlu_factor for n_shifts shifts of the same J at once: shifts[2 s], shifts[2 s + 1] is
- * shift s (real, imaginary), workspaces[s] its workspace (each workspace_bytes large), streams
- * (optional, n_shifts entries) the stream each factorisation runs on. The shifts' dense ring
- * steps are issued ring by ring across the streams so that they overlap on the device; each
- * workspace then serves eb_ringlu_solve for its shift. This batches the reference's per-shift
- * SuperLU factorisations of a frequency sweep (examples/response/run.py:138-144, one
- * solve_odes_wrt_states_fwd per reduced frequency, each factoring J - s I). Synchronises every
- * stream. */
-int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts,
-                          const double* shifts, void* const* workspaces, int64_t workspace_bytes,
-                          void* const* streams);
+ * shift s (real, imaginary; host array), its workspace starts at workspace + s * workspace_stride
+ * (stride >= eb_ringlu_workspace_bytes, a multiple of 256; workspace 256-byte aligned). Each
+ * step of the elimination runs as one launch over all shifts, so a frequency sweep factors its
+ * shifts together instead of one after another (the reference factors J - s I with SuperLU once
+ * per reduced frequency, examples/response/run.py:138-144). Each shift's workspace then serves
+ * eb_ringlu_solve / eb_ringlu_solve_many. Synchronises `stream`; EB_ERR_NAN if a ring block of
+ * any shift is singular. */
+int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
+                          void* workspace, int64_t workspace_stride, void* stream);
 
 /* x = A^-1 rhs (adjoint = 1: x = A^-H rhs) with the factors of eb_ringlu_factor for the same
  * J and shift, then iterative refinement x += A^-1 (rhs - A x) until ||rhs - A x|| / ||rhs||
@@ -256,15 +255,15 @@ int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double 
                     const double* rhs, double* x, double tol, int max_refine,
                     double* rel_residual, void* stream);
 
-/* eb_ringlu_solve for n_shifts factorisations of eb_ringlu_factor_many at once: system s uses
- * shifts[2 s], shifts[2 s + 1], workspaces[s], rhs[s], x[s] and streams[s] (streams optional).
- * Every refinement pass issues the work of all unfinished systems on their streams before it
- * reads any residual norm, so the systems' triangular sweeps overlap on the device.
- * rel_residuals (host, optional, n_shifts entries) receives the final relative residuals. */
+/* eb_ringlu_solve for the n_shifts factorisations of one eb_ringlu_factor_many call: system s
+ * uses shift s, the workspace at workspace + s * workspace_stride, rhs[s] and x[s] (host arrays
+ * of device pointers). The triangular sweeps of all systems run as batched launches; refinement
+ * passes continue until every system reaches tol. rel_residuals (host, optional, n_shifts
+ * entries) receives the final relative residuals. Synchronises `stream`. */
 int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
-                         int adjoint, void* const* workspaces, int64_t workspace_bytes,
+                         int adjoint, const void* workspace, int64_t workspace_stride,
                          const double* const* rhs, double* const* x, double tol, int max_refine,
-                         double* rel_residuals, void* const* streams);
+                         double* rel_residuals, void* stream);
 
 /* ---- second-order building blocks ------------------------------------------------------ */
 /* Directional derivatives of the Jacobians: with a complex direction d on the variable

@@ -31,8 +31,8 @@ NVCC_FLAGS = [
 # exact free stream), and only uncontracted evaluation keeps equal inputs bitwise equal across
 # the differently inlined call sites. The residual itself is continuous there and keeps FMA.
 PER_FILE_FLAGS = {"jacobians.cu": ["-fmad=false"], "second_order.cu": ["-fmad=false"]}
-# cuBLAS / cuSOLVER serve the dense super-block factorisations of the ring-block LU.
-LINK_FLAGS = ["-L/usr/local/cuda/lib64", "-lcublas", "-lcusolver",
+# cuBLAS serves the dense super-block products (strided-batched GEMM / GEMV) of the ring-block LU.
+LINK_FLAGS = ["-L/usr/local/cuda/lib64", "-lcublas",
               "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
 
 

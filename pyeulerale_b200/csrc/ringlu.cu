@@ -1,30 +1,45 @@
-// Direct resolvent: block LU of (dR/dU - shift I) over the grid's rings.
+// Direct resolvent: block LU of (dR/dU - shift I) over the grid's rings, for many shifts at once.
 //
-// A ring is one radial layer m (all N angular cells, 4N unknowns). The nine-point stencil
+// A ring is one radial layer m (all N angular cells, K = 4N unknowns). The nine-point stencil
 // couples ring m only to rings m-2..m+2, so in ring ordering the shifted Jacobian is block
-// pentadiagonal with 4N x 4N super-blocks: the diagonal block is periodic block-pentadiagonal
-// in the angular index (slots c, b, bb, f, ff) and the off-diagonal blocks start block
-// diagonal (slots i, ii, o, oo). Block Gaussian elimination over the rings (pivoting inside
-// each diagonal super-block only) factors it exactly:
-//   A = Lt Ut,  Lt = I + sum L_a[m] (block (m, m-a)),  Ut = blockdiag(D_m) + sum C_b[m] (m, m+b).
-// This replaces the reference's SuperLU factorisation (src/py_euler_ale/core.py:512-599)
-// and is the robust path for shifts near zero, where Krylov methods with local
-// preconditioners stagnate. One factorisation serves both the forward solve and the
-// Hermitian-adjoint solve A^H x = b (the reference's solve_odes_wrt_states_adj solves
-// (J - conj(s) I)^T x = b, which is A^H for A = J - s I).
+// pentadiagonal with K x K super-blocks: the diagonal block D_m is periodic block-pentadiagonal
+// in the angular index (slots c, b, bb, f, ff), the off-diagonal blocks B1_m (slot i), B2_m
+// (slot ii), C1_m (slot o) and C2_m (slot oo) start block diagonal. Block Gaussian elimination
+// over the rings (pivoting inside each diagonal super-block) factors it exactly:
+//   A = Lt Ut,  Lt = I + sum L_a[m] (block (m, m-a)),  Ut = blockdiag(D_m) + sum C_b[m] (m, m+b),
+// with, at ring m,
+//   Dinv_m = D_m^-1                      (Gauss-Jordan inversion with partial pivoting)
+//   L1[m+1] = B1'[m+1] Dinv_m,  L2[m+2] = B2[m+2] Dinv_m
+//   D[m+1] -= L1[m+1] C1'[m],   B1'[m+2] -= L2[m+2] C1'[m]
+//   D[m+2] -= L2[m+2] C2[m],    C1'[m+1] -= L1[m+1] C2[m]
+// (primes: blocks already updated by earlier rings). B2 and C2 are never updated, so they stay
+// block diagonal and the products with them are block-row / block-column scalings instead of
+// dense GEMMs: a ring costs one inversion and three dense complex GEMMs of order K.
+// This replaces the reference's SuperLU factorisation (src/py_euler_ale/core.py:512-599) and is
+// the robust path for shifts near zero, where Krylov methods with local preconditioners
+// stagnate. One factorisation serves both the forward solve and the Hermitian-adjoint solve
+// A^H x = b (the reference's solve_odes_wrt_states_adj solves (J - conj(s) I)^T x = b, which
+// is A^H for A = J - s I).
 //
-// Dense super-block work uses cuSOLVER (getrf / getrs) and cuBLAS (gemm / trsm / gemv); the
-// assembly from the nine-slot Jacobian, the layout permutations, the pivot application and
-// the residual / refinement loop are kernels of this library. All device memory comes from
+// Batching: the shifts of one call share the instance and the Jacobian; shift s has its own
+// workspace at base + s * stride. Every step of the elimination is one launch for all shifts
+// (grid dimension = shift), the dense GEMMs and GEMVs are cuBLAS strided-batched calls, so the
+// launch count per ring does not grow with the number of shifts. All device memory comes from
 // the caller's workspace.
+//
+// Gauss-Jordan inversion (blocked, nb columns per panel, implicit row pivoting): the panel
+// kernel runs the nb elimination steps on the panel columns in shared memory (pivot = largest
+// modulus among the rows not yet chosen; in-place storage of the transformation); the update
+// kernel applies the panel's transformation to all other columns as a rank-nb update
+// A[:, c] += G R[:, c], R = the panel's pivot rows, G = panel columns minus the unit vectors of
+// the pivot rows. After K steps the working array W holds T P (T = product of the elementary
+// transformations), and the inverse is Dinv[j, p_k] = W[p_j, k] (one permuting copy).
 
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
-#include <cusolverDn.h>
 
 #include <cmath>
 #include <cstring>
-#include <deque>
 #include <string>
 #include <vector>
 
@@ -39,46 +54,49 @@ int validate(const eb_batch* b);
 
 namespace rl {
 
-struct Handles {
+struct Handle {
   int device = -1;
   cublasHandle_t blas = nullptr;
-  cusolverDnHandle_t solver = nullptr;
 };
 
-// One cuBLAS / cuSOLVER handle pair per concurrent stream slot (a handle's internal workspace
-// must not be shared by work that overlaps on the device). A deque keeps the pointers stable.
-thread_local std::deque<Handles> g_handles;
+thread_local Handle g_handle;
 
-int handles(int slot, cudaStream_t st, Handles*& h) {
+int blas_handle(cudaStream_t st, cublasHandle_t& out) {
   int dev = 0;
   cudaGetDevice(&dev);
-  while ((int)g_handles.size() <= slot) g_handles.emplace_back();
-  h = &g_handles[slot];
-  if (h->device != dev) {
-    if (h->blas) cublasDestroy(h->blas);
-    if (h->solver) cusolverDnDestroy(h->solver);
-    h->blas = nullptr;
-    h->solver = nullptr;
-    if (cublasCreate(&h->blas) != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "cublasCreate failed");
-    if (cusolverDnCreate(&h->solver) != CUSOLVER_STATUS_SUCCESS)
-      return fail(EB_ERR_CUDA, "cusolverDnCreate failed");
-    h->device = dev;
+  Handle& h = g_handle;
+  if (h.device != dev) {
+    if (h.blas) cublasDestroy(h.blas);
+    h.blas = nullptr;
+    if (cublasCreate(&h.blas) != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "cublasCreate failed");
+    h.device = dev;
   }
-  cublasSetStream(h->blas, st);
-  cusolverDnSetStream(h->solver, st);
+  cublasSetStream(h.blas, st);
+  out = h.blas;
   return EB_OK;
 }
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Panel width of the Gauss-Jordan inversion: the largest of 16, 8, 4 that divides K (= 4N) and
+// keeps a thread's panel rows (K / 512 rounded up, at most 2) within 16 complex registers.
+inline int panel_width(int K) {
+  if (K > 1024) return 0;
+  const int rows = (K + 511) / 512;
+  for (int nb = 16; nb >= 4; nb /= 2)
+    if (K % nb == 0 && rows * nb <= 16) return nb;
+  return 0;
+}
+
 struct Layout {
   int M, N, K;
   size_t blk;  // bytes of one K x K complex block
-  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_piv, off_info, off_y, off_x, off_r, off_work;
+  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_T, off_perm, off_info, off_acc;
+  size_t off_y, off_x, off_r;
   size_t total;
 };
 
-Layout plan(int M, int N, int lwork) {
+Layout plan(int M, int N) {
   Layout L;
   L.M = M;
   L.N = N;
@@ -95,13 +113,14 @@ Layout plan(int M, int N, int lwork) {
   L.off_L2 = take(L.blk * M);
   L.off_C1 = take(L.blk * M);
   L.off_C2 = take(L.blk * M);
-  L.off_piv = take(sizeof(int) * (size_t)L.K * M);
-  L.off_info = take(sizeof(int) * M);
+  L.off_T = take(L.blk);
+  L.off_perm = take(sizeof(int) * (size_t)L.K);
+  L.off_info = take(sizeof(int) * 4);
+  L.off_acc = take(sizeof(double) * 2);
   const size_t vec = sizeof(cuDoubleComplex) * (size_t)L.K * M;
   L.off_y = take(vec);
   L.off_x = take(vec);
   L.off_r = take(vec);
-  L.off_work = take(sizeof(cuDoubleComplex) * (size_t)(lwork > 0 ? lwork : 1));
   L.total = o;
   return L;
 }
@@ -144,47 +163,314 @@ __global__ void k_assemble(int M, int N, const double* J, double sr, double si,
   }
 }
 
-// X <- X P^T for the row pivots of getrf (the column interchanges applied in reverse order).
-// Each CTA first composes the interchanges into one permutation in shared memory, then moves
-// a tile of `rows` rows of X through shared memory in permuted column order.
-__global__ void k_col_pivots(int K, int rows, const int* ipiv, cuDoubleComplex* X) {
-  extern __shared__ __align__(16) unsigned char pv_smem[];
-  cuDoubleComplex* tile = reinterpret_cast<cuDoubleComplex*>(pv_smem);
-  int* idx = reinterpret_cast<int*>(tile + (size_t)rows * K);
-  for (int j = threadIdx.x; j < K; j += blockDim.x) idx[j] = j;
+__device__ __forceinline__ cuDoubleComplex cmul(cuDoubleComplex a, cuDoubleComplex b) {
+  return make_cuDoubleComplex(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// acc + a b
+__device__ __forceinline__ cuDoubleComplex cfma(cuDoubleComplex a, cuDoubleComplex b,
+                                                cuDoubleComplex acc) {
+  return make_cuDoubleComplex(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+}
+// acc - a b
+__device__ __forceinline__ cuDoubleComplex cfms(cuDoubleComplex a, cuDoubleComplex b,
+                                                cuDoubleComplex acc) {
+  return make_cuDoubleComplex(fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y)));
+}
+
+// Per-shift pointer into the workspace.
+template <class T>
+__device__ __forceinline__ T* at(char* ws0, int64_t stride, size_t off) {
+  return reinterpret_cast<T*>(ws0 + stride * blockIdx.y + off);
+}
+
+// Gauss-Jordan panel: elimination steps j0 .. j0+NB-1 on the panel columns of the K x K block
+// `in` (byte offset off_in of each shift's workspace), result written to the same columns of
+// `out` (grid: 1 x n_shifts, 512 threads). Thread t keeps rows t + 512 r (r < ROWS) of the panel
+// in registers. A step: every warp finds its best row among the rows not chosen yet (largest
+// modulus, ties to the smaller row) and stages it in shared memory; after one barrier every
+// warp reduces the warp candidates itself, so all threads know the pivot row p and its values,
+// and eliminate the pivot column from their rows (row p: scaled by the pivot's inverse), which
+// also yields their candidates for the next step. The staging buffers alternate between steps,
+// so one barrier per step suffices. Records the pivot row of each step in perm and flags a zero
+// or non-finite pivot in info[0].
+constexpr int kPanelThreads = 512;
+constexpr int kMaxK = 1024;
+template <int NB, int ROWS>
+__global__ void __launch_bounds__(kPanelThreads, 1)
+    k_gj_panel(int K, int j0, char* ws0, int64_t stride, size_t off_in, size_t off_out,
+               size_t off_perm, size_t off_info) {
+  constexpr int kWarps = kPanelThreads / 32;
+  __shared__ cuDoubleComplex cand[2][kWarps][NB];
+  __shared__ double cand_v[2][kWarps];
+  __shared__ int cand_i[2][kWarps];
+  __shared__ unsigned char chosen[kMaxK];
+  const cuDoubleComplex* in = at<cuDoubleComplex>(ws0, stride, off_in);
+  cuDoubleComplex* out = at<cuDoubleComplex>(ws0, stride, off_out);
+  int* perm = at<int>(ws0, stride, off_perm);
+  int* info = at<int>(ws0, stride, off_info);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (*info != 0) return;  // an earlier panel met a singular pivot
+  for (int i = tid; i < K; i += kPanelThreads) chosen[i] = 0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = K - 1; k >= 0; --k) {
-      const int p = ipiv[k] - 1;
-      if (p != k) {
-        const int t = idx[k];
-        idx[k] = idx[p];
-        idx[p] = t;
+  for (int j = tid; j < j0; j += kPanelThreads) {
+    const int pj = perm[j];
+    if (pj >= 0 && pj < K) chosen[pj] = 1;
+  }
+  cuDoubleComplex a[ROWS][NB];
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) {
+    const int i = tid + r * kPanelThreads;
+#pragma unroll
+    for (int k = 0; k < NB; ++k)
+      a[r][k] = i < K ? in[(size_t)K * (j0 + k) + i] : make_cuDoubleComplex(0.0, 0.0);
+  }
+  __syncthreads();
+  double best = -1.0;
+  int bi = kMaxK;
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) {
+    const int i = tid + r * kPanelThreads;
+    if (i < K && !chosen[i]) {
+      const double v = a[r][0].x * a[r][0].x + a[r][0].y * a[r][0].y;
+      if (v > best) {
+        best = v;
+        bi = i;
       }
     }
   }
-  const int r0 = blockIdx.x * rows;
-  const int nr = min(rows, K - r0);
-  for (int e = threadIdx.x; e < nr * K; e += blockDim.x) {
-    const int rr = e % nr, col = e / nr;
-    tile[(size_t)rr * K + col] = X[(int64_t)col * K + r0 + rr];
+#pragma unroll 1
+  for (int jj = 0; jj < NB; ++jj) {
+    const int par = jj & 1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+      if (bi == tid + r * kPanelThreads) {
+#pragma unroll
+        for (int k = 0; k < NB; ++k) cand[par][warp][k] = a[r][k];
+      }
+    if (lane == 0) {
+      cand_v[par][warp] = best;
+      cand_i[par][warp] = bi;
+    }
+    __syncthreads();
+    double v = lane < kWarps ? cand_v[par][lane] : -1.0;
+    int p = lane < kWarps ? cand_i[par][lane] : kMaxK;
+    int w = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, p, o);
+      const int ow = __shfl_xor_sync(0xffffffffu, w, o);
+      if (ov > v || (ov == v && oi < p)) {
+        v = ov;
+        p = oi;
+        w = ow;
+      }
+    }
+    if (!(v > 0.0 && v <= 1.7e308 && p < K)) {  // the same decision in every thread
+      if (tid == 0) atomicExch(info, 1);
+      return;
+    }
+    if (tid == 0) {
+      perm[j0 + jj] = p;
+      chosen[p] = 1;
+    }
+    const cuDoubleComplex* prow = cand[par][w];
+    const cuDoubleComplex ap = prow[jj];
+    const double d = 1.0 / (ap.x * ap.x + ap.y * ap.y);
+    const cuDoubleComplex inv = make_cuDoubleComplex(ap.x * d, -ap.y * d);
+    best = -1.0;
+    bi = kMaxK;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+      const int i = tid + r * kPanelThreads;
+      cuDoubleComplex f = a[r][0];
+#pragma unroll
+      for (int k = 1; k < NB; ++k)
+        if (k == jj) f = a[r][k];
+      if (i == p) {
+#pragma unroll
+        for (int k = 0; k < NB; ++k) a[r][k] = k == jj ? inv : cmul(a[r][k], inv);
+      } else {
+        const cuDoubleComplex fi = cmul(f, inv);
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+          a[r][k] = k == jj ? make_cuDoubleComplex(-fi.x, -fi.y) : cfms(fi, prow[k], a[r][k]);
+      }
+      if (jj + 1 < NB && i < K && i != p && !chosen[i]) {
+        cuDoubleComplex c = a[r][0];
+#pragma unroll
+        for (int k = 1; k < NB; ++k)
+          if (k == jj + 1) c = a[r][k];
+        const double cv = c.x * c.x + c.y * c.y;
+        if (cv > best) {
+          best = cv;
+          bi = i;
+        }
+      }
+    }
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nr * K; e += blockDim.x) {
-    const int rr = e % nr, col = e / nr;
-    X[(int64_t)col * K + r0 + rr] = tile[(size_t)rr * K + idx[col]];
+#pragma unroll
+  for (int r = 0; r < ROWS; ++r) {
+    const int i = tid + r * kPanelThreads;
+    if (i < K) {
+#pragma unroll
+      for (int k = 0; k < NB; ++k) out[(size_t)K * (j0 + k) + i] = a[r][k];
+    }
   }
 }
 
-// Rows per CTA of k_col_pivots: up to 8, within 200 KB of shared memory.
-inline int pivot_rows(int K) {
-  const size_t budget = 200 * 1024 - sizeof(int) * (size_t)K;
-  const size_t per_row = sizeof(cuDoubleComplex) * (size_t)K;
-  const int r = per_row > budget ? 0 : (int)(budget / per_row);
-  return r > 8 ? 8 : r;
+// Gauss-Jordan update, out of place: out[:, c] = in[:, c] + G R[:, c] for every column c
+// outside the panel, where R[k, c] = in[perm[j0 + k], c] and G[:, k] = out[:, j0 + k] -
+// e_{perm[j0 + k]} (the panel columns that k_gj_panel wrote). One CTA per 64-row x 32-column
+// tile; a thread prefetches its 8 inputs before the rank-NB products. Grid: tiles x shifts.
+constexpr int kUpdRowsT = 64;
+constexpr int kUpdColsT = 32;
+template <int NB>
+__global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int64_t stride,
+                                                   size_t off_in, size_t off_out, size_t off_perm,
+                                                   size_t off_info) {
+  constexpr int kPer = kUpdRowsT * kUpdColsT / 256;  // outputs per thread
+  __shared__ cuDoubleComplex G[NB][kUpdRowsT];
+  __shared__ cuDoubleComplex R[NB][kUpdColsT];
+  __shared__ int pv[NB];
+  __shared__ int bad;
+  const int ctiles = (K + kUpdColsT - 1) / kUpdColsT;
+  const int c0 = (blockIdx.x % ctiles) * kUpdColsT, r0 = (blockIdx.x / ctiles) * kUpdRowsT;
+  const cuDoubleComplex* in = at<cuDoubleComplex>(ws0, stride, off_in);
+  cuDoubleComplex* out = at<cuDoubleComplex>(ws0, stride, off_out);
+  const int* perm = at<int>(ws0, stride, off_perm);
+  const int tid = threadIdx.x;
+  const int r = tid % kUpdRowsT, row = r0 + r, cb = tid / kUpdRowsT;
+  // prefetch this thread's inputs (columns cb, cb + 4, ...)
+  cuDoubleComplex acc[kPer];
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) {
+    const int col = c0 + cb + 4 * q;
+    acc[q] = row < K && col < K ? in[(size_t)K * col + row] : make_cuDoubleComplex(0.0, 0.0);
+  }
+  if (tid == 0) bad = *at<int>(ws0, stride, off_info);
+  __syncthreads();
+  if (tid < NB) {
+    pv[tid] = perm[j0 + tid];
+    if (pv[tid] < 0 || pv[tid] >= K) atomicExch(&bad, 1);
+  }
+  __syncthreads();
+  if (bad) return;  // singular block: pivots incomplete, the caller fails
+  for (int e = tid; e < NB * kUpdRowsT; e += 256) {
+    const int k = e / kUpdRowsT, x = e % kUpdRowsT, rr = r0 + x;
+    cuDoubleComplex g = rr < K ? out[(size_t)K * (j0 + k) + rr] : make_cuDoubleComplex(0.0, 0.0);
+    if (rr == pv[k]) g.x -= 1.0;
+    G[k][x] = g;
+  }
+  for (int e = tid; e < NB * kUpdColsT; e += 256) {
+    const int k = e / kUpdColsT, x = e % kUpdColsT, col = c0 + x;
+    R[k][x] = col < K ? in[(size_t)K * col + pv[k]] : make_cuDoubleComplex(0.0, 0.0);
+  }
+  __syncthreads();
+  if (row >= K) return;
+  cuDoubleComplex g[NB];
+#pragma unroll
+  for (int k = 0; k < NB; ++k) g[k] = G[k][r];
+#pragma unroll
+  for (int q = 0; q < kPer; ++q) {
+    const int c = cb + 4 * q, col = c0 + c;
+    if (col >= K || (col >= j0 && col < j0 + NB)) continue;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) acc[q] = cfma(g[k], R[k][c], acc[q]);
+    out[(size_t)K * col + row] = acc[q];
+  }
 }
-inline size_t pivot_smem(int K, int rows) {
-  return (size_t)rows * K * sizeof(cuDoubleComplex) + sizeof(int) * (size_t)K;
+
+// Dinv[j, perm[k]] = W[perm[j], k]: the inverse from the Gauss-Jordan working array (W at
+// off_W, result at off_out; grid: column groups x shifts).
+__global__ void __launch_bounds__(256) k_gj_permute(int K, char* ws0, int64_t stride, size_t off_W,
+                                                    size_t off_out, size_t off_perm, size_t off_info) {
+  extern __shared__ int pm[];
+  __shared__ int bad;
+  const cuDoubleComplex* W = at<cuDoubleComplex>(ws0, stride, off_W);
+  cuDoubleComplex* out = at<cuDoubleComplex>(ws0, stride, off_out);
+  const int* perm = at<int>(ws0, stride, off_perm);
+  if (threadIdx.x == 0) bad = *at<int>(ws0, stride, off_info);
+  __syncthreads();
+  for (int i = threadIdx.x; i < K; i += blockDim.x) {
+    pm[i] = perm[i];
+    if (pm[i] < 0 || pm[i] >= K) atomicExch(&bad, 1);
+  }
+  __syncthreads();
+  if (bad) return;  // singular block: pivots incomplete, the caller fails
+  for (int k = blockIdx.x; k < K; k += gridDim.x) {
+    const cuDoubleComplex* w = W + (size_t)K * k;
+    cuDoubleComplex* o = out + (size_t)K * pm[k];
+    for (int j = threadIdx.x; j < K; j += blockDim.x) o[j] = w[pm[j]];
+  }
+}
+
+// Block-diagonal left product in place: X <- Bd X, where X (at off_X) holds the block-diagonal
+// Bd in its 4 x 4 diagonal blocks on entry and Y = Bd Src is written over it (Src at off_S).
+// Grid: N row blocks x shifts.
+__global__ void __launch_bounds__(256) k_bd_left(int K, char* ws0, int64_t stride, size_t off_X,
+                                                 size_t off_S) {
+  __shared__ cuDoubleComplex bd[4][4];
+  cuDoubleComplex* X = at<cuDoubleComplex>(ws0, stride, off_X);
+  const cuDoubleComplex* S = at<cuDoubleComplex>(ws0, stride, off_S);
+  const int n = blockIdx.x;
+  if (threadIdx.x < 16) {
+    const int r = threadIdx.x & 3, q = threadIdx.x >> 2;
+    bd[r][q] = X[(size_t)K * (4 * n + q) + 4 * n + r];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < K; c += blockDim.x) {
+    const cuDoubleComplex* s = S + (size_t)K * c + 4 * n;
+    const cuDoubleComplex s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
+    cuDoubleComplex* x = X + (size_t)K * c + 4 * n;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      cuDoubleComplex acc = cmul(bd[r][0], s0);
+      acc = cfma(bd[r][1], s1, acc);
+      acc = cfma(bd[r][2], s2, acc);
+      acc = cfma(bd[r][3], s3, acc);
+      x[r] = acc;
+    }
+  }
+}
+
+// Block-diagonal right products: Y -= X Bd for two (X, Y) pairs selected by blockIdx.z, Bd the
+// 4 x 4 diagonal blocks stored in the K x K block at off_B. Grid: N column blocks x shifts x 2.
+__global__ void __launch_bounds__(256) k_bd_right(int K, char* ws0, int64_t stride, size_t off_B,
+                                                  size_t off_X0, size_t off_Y0, size_t off_X1,
+                                                  size_t off_Y1) {
+  __shared__ cuDoubleComplex bd[4][4];
+  const cuDoubleComplex* B = at<cuDoubleComplex>(ws0, stride, off_B);
+  const cuDoubleComplex* X = at<cuDoubleComplex>(ws0, stride, blockIdx.z ? off_X1 : off_X0);
+  cuDoubleComplex* Y = at<cuDoubleComplex>(ws0, stride, blockIdx.z ? off_Y1 : off_Y0);
+  const int n = blockIdx.x;
+  if (threadIdx.x < 16) {
+    const int q = threadIdx.x & 3, c = threadIdx.x >> 2;
+    bd[q][c] = B[(size_t)K * (4 * n + c) + 4 * n + q];
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < K; r += blockDim.x) {
+    cuDoubleComplex x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) x[q] = X[(size_t)K * (4 * n + q) + r];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      cuDoubleComplex* y = Y + (size_t)K * (4 * n + c) + r;
+      cuDoubleComplex acc = *y;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc = cfms(x[q], bd[q][c], acc);
+      *y = acc;
+    }
+  }
 }
 
 // Reference layout (4, M, N) <-> ring layout [m][n][v].
@@ -276,57 +562,168 @@ __global__ void __launch_bounds__(128) k_residual_op(int M, int N, const double*
   }
 }
 
-struct Factor {
-  Layout L;
-  char* base;
-  cuDoubleComplex* blk(size_t off, int m) const {
-    return reinterpret_cast<cuDoubleComplex*>(base + off + L.blk * (size_t)m);
-  }
-  int* piv(int m) const { return reinterpret_cast<int*>(base + L.off_piv) + (size_t)L.K * m; }
-};
-
-// Ring-ordered triangular solves with the stored factors, in place on ring vector y.
-int ring_solve(Handles* h, const Factor& F, cuDoubleComplex* y, bool adjoint) {
-  const int M = F.L.M, K = F.L.K;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
-  int* info = reinterpret_cast<int*>(F.base + F.L.off_info);
-  auto vec = [&](int m) { return y + (size_t)K * m; };
-  if (!adjoint) {
-    for (int m = 1; m < M; ++m) {  // Lt z = b
-      cublasZgemv(h->blas, CUBLAS_OP_N, K, K, &mone, F.blk(F.L.off_L1, m), K, vec(m - 1), 1, &one, vec(m), 1);
-      if (m >= 2)
-        cublasZgemv(h->blas, CUBLAS_OP_N, K, K, &mone, F.blk(F.L.off_L2, m), K, vec(m - 2), 1, &one, vec(m), 1);
-    }
-    for (int m = M - 1; m >= 0; --m) {  // Ut x = z
-      if (m + 1 < M)
-        cublasZgemv(h->blas, CUBLAS_OP_N, K, K, &mone, F.blk(F.L.off_C1, m), K, vec(m + 1), 1, &one, vec(m), 1);
-      if (m + 2 < M)
-        cublasZgemv(h->blas, CUBLAS_OP_N, K, K, &mone, F.blk(F.L.off_C2, m), K, vec(m + 2), 1, &one, vec(m), 1);
-      cusolverDnZgetrs(h->solver, CUBLAS_OP_N, K, 1, F.blk(F.L.off_D, m), K, F.piv(m), vec(m), K, info + m);
-    }
-  } else {
-    for (int m = 0; m < M; ++m) {  // Ut^H z = b
-      if (m >= 1)
-        cublasZgemv(h->blas, CUBLAS_OP_C, K, K, &mone, F.blk(F.L.off_C1, m - 1), K, vec(m - 1), 1, &one, vec(m), 1);
-      if (m >= 2)
-        cublasZgemv(h->blas, CUBLAS_OP_C, K, K, &mone, F.blk(F.L.off_C2, m - 2), K, vec(m - 2), 1, &one, vec(m), 1);
-      cusolverDnZgetrs(h->solver, CUBLAS_OP_C, K, 1, F.blk(F.L.off_D, m), K, F.piv(m), vec(m), K, info + m);
-    }
-    for (int m = M - 1; m >= 0; --m) {  // Lt^H x = z
-      if (m + 1 < M)
-        cublasZgemv(h->blas, CUBLAS_OP_C, K, K, &mone, F.blk(F.L.off_L1, m + 1), K, vec(m + 1), 1, &one, vec(m), 1);
-      if (m + 2 < M)
-        cublasZgemv(h->blas, CUBLAS_OP_C, K, K, &mone, F.blk(F.L.off_L2, m + 2), K, vec(m + 2), 1, &one, vec(m), 1);
-    }
-  }
-  return check_launch("ring solve");
-}
-
 inline int grid_for(int64_t n, int threads) {
   int64_t blocks = (n + threads - 1) / threads;
   if (blocks > 148 * 16) blocks = 148 * 16;
   return (int)(blocks < 1 ? 1 : blocks);
+}
+
+// The shifts of one call: workspace of shift s at base + s * stride.
+struct Group {
+  Layout L;
+  char* base;
+  int64_t stride;  // bytes
+  int S;
+  int64_t es() const { return stride / (int64_t)sizeof(cuDoubleComplex); }
+  cuDoubleComplex* blk(size_t off, int m) const {
+    return reinterpret_cast<cuDoubleComplex*>(base + off + L.blk * (size_t)m);
+  }
+  size_t boff(size_t off, int m) const { return off + L.blk * (size_t)m; }
+};
+
+int check_group(const eb_batch* b, int n_shifts, const void* ws, int64_t stride, Layout& L) {
+  int rc = validate(b);
+  if (rc != EB_OK) return rc;
+  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
+  if (n_shifts < 1 || n_shifts > 65535 || !ws) return fail(EB_ERR_ARG, "ringlu: bad shifts or workspace");
+  const int M = b->single.M, N = b->single.N;
+  if (M < 4 || N < 5 || panel_width(4 * N) == 0) return fail(EB_ERR_ARG, "ringlu: unsupported grid size");
+  L = plan(M, N);
+  if (stride < (int64_t)L.total || stride % 256 != 0)
+    return fail(EB_ERR_ARG, "ringlu: workspace stride too small or not a multiple of 256");
+  if (reinterpret_cast<uintptr_t>(ws) % 256 != 0) return fail(EB_ERR_ARG, "ringlu: workspace not 256-byte aligned");
+  return EB_OK;
+}
+
+int blas_ok(cublasStatus_t st, const char* what) {
+  return st == CUBLAS_STATUS_SUCCESS ? EB_OK : fail(EB_ERR_CUDA, what);
+}
+
+template <int NB, int ROWS>
+void gj_pass(const Group& g, int j0, size_t off_in, size_t off_out, cudaStream_t st) {
+  const int K = g.L.K;
+  const int tiles = ((K + kUpdColsT - 1) / kUpdColsT) * ((K + kUpdRowsT - 1) / kUpdRowsT);
+  k_gj_panel<NB, ROWS><<<dim3(1, g.S), kPanelThreads, 0, st>>>(K, j0, g.base, g.stride, off_in, off_out,
+                                                               g.L.off_perm, g.L.off_info);
+  k_gj_update<NB><<<dim3(tiles, g.S), 256, 0, st>>>(K, j0, g.base, g.stride, off_in, off_out,
+                                                           g.L.off_perm, g.L.off_info);
+}
+
+// D_m <- D_m^-1 for every shift (Gauss-Jordan, ping-pong between D_m and the scratch block T).
+int invert_ring(const Group& g, int m, cudaStream_t st) {
+  const Layout& L = g.L;
+  const int K = L.K, nb = panel_width(K), rows = (K + kPanelThreads - 1) / kPanelThreads;
+  const size_t buf[2] = {g.boff(L.off_D, m), L.off_T};
+  const int passes = K / nb;
+  for (int p = 0; p < passes; ++p) {
+    const size_t in = buf[p & 1], out = buf[(p + 1) & 1];
+    const int j0 = p * nb;
+    if (rows == 1) {
+      if (nb == 16) gj_pass<16, 1>(g, j0, in, out, st);
+      else if (nb == 8) gj_pass<8, 1>(g, j0, in, out, st);
+      else gj_pass<4, 1>(g, j0, in, out, st);
+    } else {
+      if (nb == 8) gj_pass<8, 2>(g, j0, in, out, st);
+      else gj_pass<4, 2>(g, j0, in, out, st);
+    }
+  }
+  const size_t W = buf[passes & 1], other = buf[(passes + 1) & 1];
+  k_gj_permute<<<dim3(std::min(K, 1024), g.S), 256, sizeof(int) * K, st>>>(K, g.base, g.stride, W, other,
+                                                                          L.off_perm, L.off_info);
+  if (other != buf[0] &&
+      cudaMemcpy2DAsync(g.base + buf[0], g.stride, g.base + other, g.stride, L.blk, g.S,
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return check_launch("ringlu inverse copy");
+  return EB_OK;
+}
+
+// One ring of the block elimination for every shift of the group.
+int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
+  const Layout& L = g.L;
+  const int M = L.M, K = L.K, N = L.N;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
+  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
+  const int64_t es = g.es();
+  int rc = invert_ring(g, m, st);
+  if (rc != EB_OK) return rc;
+  if (m + 1 < M) {
+    // T = L1[m+1] = B1'[m+1] Dinv_m;  D[m+1] -= T C1'[m]
+    if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &one,
+                                                g.blk(L.off_L1, m + 1), K, es, g.blk(L.off_D, m), K, es,
+                                                &zero, g.blk(L.off_T, 0), K, es, g.S),
+                      "ringlu: gemm L1")) != EB_OK)
+      return rc;
+    if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone,
+                                                g.blk(L.off_T, 0), K, es, g.blk(L.off_C1, m), K, es,
+                                                &one, g.blk(L.off_D, m + 1), K, es, g.S),
+                      "ringlu: gemm D1")) != EB_OK)
+      return rc;
+  }
+  if (m + 2 < M) {
+    // L2[m+2] = B2[m+2] Dinv_m;  B1'[m+2] -= L2[m+2] C1'[m]
+    k_bd_left<<<dim3(N, g.S), 256, 0, st>>>(K, g.base, g.stride, g.boff(L.off_L2, m + 2), g.boff(L.off_D, m));
+    if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone,
+                                                g.blk(L.off_L2, m + 2), K, es, g.blk(L.off_C1, m), K, es,
+                                                &one, g.blk(L.off_L1, m + 2), K, es, g.S),
+                      "ringlu: gemm L1 update")) != EB_OK)
+      return rc;
+    // D[m+2] -= L2[m+2] C2[m];  C1'[m+1] -= L1[m+1] C2[m]
+    k_bd_right<<<dim3(N, g.S, 2), 256, 0, st>>>(K, g.base, g.stride, g.boff(L.off_C2, m),
+                                                g.boff(L.off_L2, m + 2), g.boff(L.off_D, m + 2),
+                                                L.off_T, g.boff(L.off_C1, m + 1));
+  }
+  if (m + 1 < M &&
+      cudaMemcpy2DAsync(g.blk(L.off_L1, m + 1), g.stride, g.blk(L.off_T, 0), g.stride, L.blk, g.S,
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return check_launch("ringlu L1 copy");
+  return EB_OK;
+}
+
+// Ring-ordered triangular solves with the stored factors for every shift: y (ring layout)
+// holds the right-hand sides on entry; the solutions are left in x.
+int ring_solve(const Group& g, cublasHandle_t h, bool adjoint) {
+  const Layout& L = g.L;
+  const int M = L.M, K = L.K;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
+  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
+  const int64_t es = g.es();
+  cuDoubleComplex* y = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_y);
+  cuDoubleComplex* x = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_x);
+  auto yv = [&](int m) { return y + (size_t)K * m; };
+  auto xv = [&](int m) { return x + (size_t)K * m; };
+  auto gemv = [&](cublasOperation_t op, const cuDoubleComplex* alpha, const cuDoubleComplex* A,
+                  const cuDoubleComplex* v, const cuDoubleComplex* beta, cuDoubleComplex* out) {
+    return cublasZgemvStridedBatched(h, op, K, K, alpha, A, K, es, v, 1, es, beta, out, 1, es, g.S);
+  };
+  cublasStatus_t st = CUBLAS_STATUS_SUCCESS;
+  auto run = [&](cublasStatus_t s) {
+    if (s != CUBLAS_STATUS_SUCCESS) st = s;
+  };
+  if (!adjoint) {
+    for (int m = 1; m < M; ++m) {  // Lt z = b (in y)
+      run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_L1, m), yv(m - 1), &one, yv(m)));
+      if (m >= 2) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_L2, m), yv(m - 2), &one, yv(m)));
+    }
+    for (int m = M - 1; m >= 0; --m) {  // Ut x = z
+      if (m + 1 < M) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_C1, m), xv(m + 1), &one, yv(m)));
+      if (m + 2 < M) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_C2, m), xv(m + 2), &one, yv(m)));
+      run(gemv(CUBLAS_OP_N, &one, g.blk(L.off_D, m), yv(m), &zero, xv(m)));
+    }
+  } else {
+    for (int m = 0; m < M; ++m) {  // Ut^H z = b (z in x)
+      if (m >= 1) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_C1, m - 1), xv(m - 1), &one, yv(m)));
+      if (m >= 2) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_C2, m - 2), xv(m - 2), &one, yv(m)));
+      run(gemv(CUBLAS_OP_C, &one, g.blk(L.off_D, m), yv(m), &zero, xv(m)));
+    }
+    for (int m = M - 1; m >= 0; --m) {  // Lt^H x = z
+      if (m + 1 < M) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_L1, m + 1), xv(m + 1), &one, xv(m)));
+      if (m + 2 < M) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_L2, m + 2), xv(m + 2), &one, xv(m)));
+    }
+  }
+  if (st != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "ringlu: gemv failed");
+  return check_launch("ring solve");
 }
 
 }  // namespace rl
@@ -338,195 +735,105 @@ using namespace eb::rl;
 extern "C" {
 
 int64_t eb_ringlu_workspace_bytes(int M, int N) {
-  if (M < 4 || N < 5 || pivot_rows(4 * N) < 1) return -1;
-  Handles* h = nullptr;
-  if (handles(0, nullptr, h) != EB_OK) return -1;
-  const int K = 4 * N;
-  int lwork = 0;
-  if (cusolverDnZgetrf_bufferSize(h->solver, K, K, nullptr, K, &lwork) != CUSOLVER_STATUS_SUCCESS)
-    return -1;
-  return (int64_t)plan(M, N, lwork).total;
+  if (M < 4 || N < 5 || panel_width(4 * N) == 0) return -1;
+  return (int64_t)plan(M, N).total;
 }
 
-}  // extern "C"
-
-namespace eb {
-namespace rl {
-
-// One ring of the block elimination for one factorisation (all work on stream st).
-int factor_ring(Handles* h, const Factor& f, int m, cudaStream_t st) {
-  const Layout& L = f.L;
-  const int M = L.M, K = L.K;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
-  int* info = reinterpret_cast<int*>(f.base + L.off_info);
-  cuDoubleComplex* work = reinterpret_cast<cuDoubleComplex*>(f.base + L.off_work);
-  cuDoubleComplex* D = f.blk(L.off_D, m);
-  if (cusolverDnZgetrf(h->solver, K, K, D, K, work, f.piv(m), info + m) != CUSOLVER_STATUS_SUCCESS)
-    return fail(EB_ERR_CUDA, "ringlu: getrf failed");
-  // L_a[m+a] = B_a[m+a] D_m^-1 = B U^-1 L^-1 P^T
-  for (int a = 1; a <= 2; ++a) {
-    if (m + a >= M) continue;
-    cuDoubleComplex* X = f.blk(a == 1 ? L.off_L1 : L.off_L2, m + a);
-    cublasZtrsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
-                CUBLAS_DIAG_NON_UNIT, K, K, &one, D, K, X, K);
-    cublasZtrsm(h->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
-                CUBLAS_DIAG_UNIT, K, K, &one, D, K, X, K);
-    const int rows = pivot_rows(K);
-    k_col_pivots<<<(K + rows - 1) / rows, 256, pivot_smem(K, rows), st>>>(K, rows, f.piv(m), X);
-  }
-  // Schur complements of the next two rings
-  if (m + 1 < M)
-    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L1, m + 1), K,
-                f.blk(L.off_C1, m), K, &one, f.blk(L.off_D, m + 1), K);
-  if (m + 2 < M) {
-    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L2, m + 2), K,
-                f.blk(L.off_C2, m), K, &one, f.blk(L.off_D, m + 2), K);
-    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L2, m + 2), K,
-                f.blk(L.off_C1, m), K, &one, f.blk(L.off_L1, m + 2), K);
-    cublasZgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone, f.blk(L.off_L1, m + 1), K,
-                f.blk(L.off_C2, m), K, &one, f.blk(L.off_C1, m + 1), K);
-  }
-  return EB_OK;
-}
-
-int check_info(const Factor& f, cudaStream_t st) {
-  const int M = f.L.M;
-  std::vector<int> hinfo(M);
-  if (cudaMemcpyAsync(hinfo.data(), f.base + f.L.off_info, sizeof(int) * M,
-                      cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess)
-    return check_launch("ringlu info");
-  for (int m = 0; m < M; ++m)
-    if (hinfo[m] != 0) return fail(EB_ERR_NAN, "ringlu: singular ring block");
-  return EB_OK;
-}
-
-}  // namespace rl
-}  // namespace eb
-
-extern "C" {
-
-int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts,
-                          const double* shifts, void* const* workspaces, int64_t workspace_bytes,
-                          void* const* streams) {
-  int rc = validate(b);
+int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
+                          void* workspace, int64_t workspace_stride, void* stream) {
+  Layout L;
+  int rc = check_group(b, n_shifts, workspace, workspace_stride, L);
   if (rc != EB_OK) return rc;
-  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
-  if (!J || !workspaces || !shifts || n_shifts < 1) return fail(EB_ERR_ARG, "ringlu: null argument");
-  const int M = b->single.M, N = b->single.N, K = 4 * N;
-  auto stream_of = [&](int s) {
-    return streams ? reinterpret_cast<cudaStream_t>(streams[s]) : (cudaStream_t) nullptr;
-  };
-  std::vector<Handles*> h(n_shifts);
-  for (int s = 0; s < n_shifts; ++s)
-    if ((rc = handles(s, stream_of(s), h[s])) != EB_OK) return rc;
-  int lwork = 0;
-  cusolverDnZgetrf_bufferSize(h[0]->solver, K, K, nullptr, K, &lwork);
-  const Layout L = plan(M, N, lwork);
-  if ((int64_t)L.total > workspace_bytes) return fail(EB_ERR_ARG, "ringlu: workspace too small");
-  if (cudaFuncSetAttribute(k_col_pivots, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)pivot_smem(K, pivot_rows(K))) != cudaSuccess)
-    return check_launch("ringlu pivot attribute");
-  std::vector<Factor> F(n_shifts);
+  if (!J || !shifts) return fail(EB_ERR_ARG, "ringlu: null argument");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cublasHandle_t h = nullptr;
+  if ((rc = blas_handle(st, h)) != EB_OK) return rc;
+  const Group g{L, static_cast<char*>(workspace), workspace_stride, n_shifts};
+  const int M = L.M, N = L.N;
   for (int s = 0; s < n_shifts; ++s) {
-    if (!workspaces[s]) return fail(EB_ERR_ARG, "ringlu: null workspace");
-    F[s] = Factor{L, static_cast<char*>(workspaces[s])};
-    cudaStream_t st = stream_of(s);
-    cudaMemsetAsync(F[s].base, 0, L.off_piv, st);  // the five block arrays
+    char* w = g.base + (int64_t)s * g.stride;
+    cudaMemsetAsync(w, 0, L.off_T, st);  // the five block arrays
+    cudaMemsetAsync(w + L.off_info, 0, sizeof(int) * 4, st);
     k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
-        M, N, J, shifts[2 * s], shifts[2 * s + 1], F[s].blk(L.off_D, 0), F[s].blk(L.off_L1, 0),
-        F[s].blk(L.off_L2, 0), F[s].blk(L.off_C1, 0), F[s].blk(L.off_C2, 0));
+        M, N, J, shifts[2 * s], shifts[2 * s + 1], reinterpret_cast<cuDoubleComplex*>(w + L.off_D),
+        reinterpret_cast<cuDoubleComplex*>(w + L.off_L1), reinterpret_cast<cuDoubleComplex*>(w + L.off_L2),
+        reinterpret_cast<cuDoubleComplex*>(w + L.off_C1), reinterpret_cast<cuDoubleComplex*>(w + L.off_C2));
   }
   if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
-  // Ring by ring; within a ring every shift's independent work goes to its own stream, so
-  // the latency-bound dense steps of different shifts overlap on the GPU.
   for (int m = 0; m < M; ++m)
-    for (int s = 0; s < n_shifts; ++s)
-      if ((rc = factor_ring(h[s], F[s], m, stream_of(s))) != EB_OK) return rc;
+    if ((rc = factor_ring(g, h, m, st)) != EB_OK) return rc;
   if ((rc = check_launch("ringlu factor")) != EB_OK) return rc;
+  std::vector<int> info(n_shifts);
   for (int s = 0; s < n_shifts; ++s)
-    if ((rc = check_info(F[s], stream_of(s))) != EB_OK) return rc;
+    if (cudaMemcpyAsync(&info[s], g.base + (int64_t)s * g.stride + L.off_info, sizeof(int),
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return check_launch("ringlu info");
+  if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("ringlu info");
+  for (int s = 0; s < n_shifts; ++s)
+    if (info[s] != 0) return fail(EB_ERR_NAN, "ringlu: singular or non-finite ring block");
   return EB_OK;
 }
 
 int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double shift_im,
                      void* workspace, int64_t workspace_bytes, void* stream) {
   const double shift[2] = {shift_re, shift_im};
-  void* ws[1] = {workspace};
-  void* st[1] = {stream};
-  return eb_ringlu_factor_many(b, J, 1, shift, ws, workspace_bytes, st);
+  return eb_ringlu_factor_many(b, J, 1, shift, workspace, workspace_bytes & ~(int64_t)255, stream);
 }
 
 int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
-                         int adjoint, void* const* workspaces, int64_t workspace_bytes,
+                         int adjoint, const void* workspace, int64_t workspace_stride,
                          const double* const* rhs, double* const* x, double tol, int max_refine,
-                         double* rel_residuals, void* const* streams) {
-  int rc = validate(b);
+                         double* rel_residuals, void* stream) {
+  Layout L;
+  int rc = check_group(b, n_shifts, workspace, workspace_stride, L);
   if (rc != EB_OK) return rc;
-  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ringlu: single instance only");
-  if (!J || !workspaces || !shifts || !rhs || !x || n_shifts < 1)
-    return fail(EB_ERR_ARG, "ringlu: null argument");
+  if (!J || !shifts || !rhs || !x) return fail(EB_ERR_ARG, "ringlu: null argument");
   for (int s = 0; s < n_shifts; ++s)
-    if (!workspaces[s] || !rhs[s] || !x[s]) return fail(EB_ERR_ARG, "ringlu: null argument");
-  const int M = b->single.M, N = b->single.N, K = 4 * N;
-  auto stream_of = [&](int s) {
-    return streams ? reinterpret_cast<cudaStream_t>(streams[s]) : (cudaStream_t) nullptr;
-  };
-  std::vector<Handles*> h(n_shifts);
-  for (int s = 0; s < n_shifts; ++s)
-    if ((rc = handles(s, stream_of(s), h[s])) != EB_OK) return rc;
-  int lwork = 0;
-  cusolverDnZgetrf_bufferSize(h[0]->solver, K, K, nullptr, K, &lwork);
-  const Layout L = plan(M, N, lwork);
-  if ((int64_t)L.total > workspace_bytes) return fail(EB_ERR_ARG, "ringlu: workspace too small");
+    if (!rhs[s] || !x[s]) return fail(EB_ERR_ARG, "ringlu: null argument");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cublasHandle_t h = nullptr;
+  if ((rc = blas_handle(st, h)) != EB_OK) return rc;
+  const Group g{L, static_cast<char*>(const_cast<void*>(workspace)), workspace_stride, n_shifts};
+  const int M = L.M, N = L.N;
   const int gc = grid_for((int64_t)M * N, 128);
-  std::vector<Factor> F(n_shifts);
+  auto ws = [&](int s) { return g.base + (int64_t)s * g.stride; };
   std::vector<double> rel(n_shifts, INFINITY);
-  std::vector<char> active(n_shifts, 1);
-  for (int s = 0; s < n_shifts; ++s) F[s] = Factor{L, static_cast<char*>(workspaces[s])};
-  auto y_of = [&](int s) { return reinterpret_cast<cuDoubleComplex*>(F[s].base + L.off_y); };
-  auto r_of = [&](int s) { return reinterpret_cast<double*>(F[s].base + L.off_r); };
-  // two doubles of scratch for the norms (the x ring vector is not used by the solve)
-  auto acc_of = [&](int s) { return reinterpret_cast<double*>(F[s].base + L.off_x); };
-  // x = A^-1 b, then refine x += A^-1 (b - A x) until the relative residual reaches tol. Every
-  // pass issues the work of all unfinished shifts on their streams before reading any norm.
+  std::vector<double> acc(2 * (size_t)n_shifts);
+  // x = A^-1 b, then refine x += A^-1 (b - A x) until every relative residual reaches tol
   for (int it = 0;; ++it) {
-    int n_active = 0;
+    for (int s = 0; s < n_shifts; ++s)
+      k_to_rings<<<gc, 128, 0, st>>>(M, N, it == 0 ? rhs[s] : reinterpret_cast<double*>(ws(s) + L.off_r),
+                                     reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_y));
+    if ((rc = ring_solve(g, h, adjoint != 0)) != EB_OK) return rc;
     for (int s = 0; s < n_shifts; ++s) {
-      if (!active[s]) continue;
-      ++n_active;
-      cudaStream_t st = stream_of(s);
-      k_to_rings<<<gc, 128, 0, st>>>(M, N, it == 0 ? rhs[s] : r_of(s), y_of(s));
-      if ((rc = ring_solve(h[s], F[s], y_of(s), adjoint != 0)) != EB_OK) return rc;
-      k_from_rings<<<gc, 128, 0, st>>>(M, N, y_of(s), x[s], it == 0 ? 0 : 1);
-      cudaMemsetAsync(acc_of(s), 0, 2 * sizeof(double), st);
-      k_residual_op<<<gc, 128, 0, st>>>(M, N, J, shifts[2 * s], shifts[2 * s + 1], adjoint, x[s],
-                                        rhs[s], r_of(s), acc_of(s));
-    }
-    if (n_active == 0) break;
-    if ((rc = check_launch("ringlu solve")) != EB_OK) return rc;
-    for (int s = 0; s < n_shifts; ++s) {
-      if (!active[s]) continue;
-      double hacc[2];
-      if (cudaMemcpyAsync(hacc, acc_of(s), sizeof(hacc), cudaMemcpyDeviceToHost, stream_of(s)) !=
-              cudaSuccess ||
-          cudaStreamSynchronize(stream_of(s)) != cudaSuccess)
+      double* a = reinterpret_cast<double*>(ws(s) + L.off_acc);
+      k_from_rings<<<gc, 128, 0, st>>>(M, N, reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_x), x[s],
+                                       it == 0 ? 0 : 1);
+      cudaMemsetAsync(a, 0, 2 * sizeof(double), st);
+      k_residual_op<<<gc, 128, 0, st>>>(M, N, J, shifts[2 * s], shifts[2 * s + 1], adjoint, x[s], rhs[s],
+                                        reinterpret_cast<double*>(ws(s) + L.off_r), a);
+      if (cudaMemcpyAsync(&acc[2 * s], a, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return check_launch("ringlu residual");
-      rel[s] = hacc[1] > 0 ? std::sqrt(hacc[0] / hacc[1]) : std::sqrt(hacc[0]);
-      if (!std::isfinite(rel[s])) {
-        if (rel_residuals)
-          for (int q = 0; q < n_shifts; ++q) rel_residuals[q] = rel[q];
-        return fail(EB_ERR_NAN, "ringlu: non-finite residual");
-      }
-      if (rel[s] <= tol || it >= max_refine) active[s] = 0;
     }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_launch("ringlu residual");
+    bool done = true, finite = true;
+    for (int s = 0; s < n_shifts; ++s) {
+      rel[s] = acc[2 * s + 1] > 0 ? std::sqrt(acc[2 * s] / acc[2 * s + 1]) : std::sqrt(acc[2 * s]);
+      finite = finite && std::isfinite(rel[s]);
+      done = done && rel[s] <= tol;
+    }
+    if (!finite) {
+      if (rel_residuals)
+        for (int s = 0; s < n_shifts; ++s) rel_residuals[s] = rel[s];
+      return fail(EB_ERR_NAN, "ringlu: non-finite residual");
+    }
+    if (done || it >= max_refine) break;
   }
   if (rel_residuals)
     for (int s = 0; s < n_shifts; ++s) rel_residuals[s] = rel[s];
   for (int s = 0; s < n_shifts; ++s)
     if (rel[s] > tol) return fail(EB_ERR_NOCONV, "ringlu: refinement did not reach the tolerance");
-  return EB_OK;
+  return check_launch("ringlu solve");
 }
 
 int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double shift_im,
@@ -534,12 +841,10 @@ int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double 
                     const double* rhs, double* x, double tol, int max_refine,
                     double* rel_residual, void* stream) {
   const double shift[2] = {shift_re, shift_im};
-  void* ws[1] = {const_cast<void*>(workspace)};
   const double* in[1] = {rhs};
   double* out[1] = {x};
-  void* st[1] = {stream};
-  return eb_ringlu_solve_many(b, J, 1, shift, adjoint, ws, workspace_bytes, in, out, tol,
-                              max_refine, rel_residual, st);
+  return eb_ringlu_solve_many(b, J, 1, shift, adjoint, workspace, workspace_bytes & ~(int64_t)255,
+                              in, out, tol, max_refine, rel_residual, stream);
 }
 
 }  // extern "C"

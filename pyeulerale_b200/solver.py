@@ -124,7 +124,7 @@ def _bind_ringlu() -> ctypes.CDLL:
             P]
         lib.eb_ringlu_factor_many.restype = ctypes.c_int
         lib.eb_ringlu_factor_many.argtypes = [ctypes.POINTER(_lib.Batch), P, ctypes.c_int, P, P,
-                                              ctypes.c_int64, P]
+                                              ctypes.c_int64, P]  # workspace base, stride
         lib.eb_ringlu_solve_many.restype = ctypes.c_int
         lib.eb_ringlu_solve_many.argtypes = [
             ctypes.POINTER(_lib.Batch), P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int64, P, P,
@@ -193,10 +193,11 @@ class RingLU:
 class RingLUMany:
     """Ring-LU factors of ``J - s I`` for several shifts ``s`` of one instance at once.
 
-    ``factor(J, shifts)`` runs ``eb_ringlu_factor_many``: the shifts' dense ring steps go to one
-    CUDA stream per shift and overlap on the device. ``solve(rhs, adjoint)`` solves one
-    right-hand side per shift through ``eb_ringlu_solve_many`` the same way. ``capacity``
-    fixes the number of workspaces (each ``ringlu_workspace_bytes(M, N)`` bytes).
+    ``factor(J, shifts)`` runs ``eb_ringlu_factor_many``: every elimination step is one launch
+    over all shifts (batched Gauss-Jordan ring inversions and strided-batched GEMMs).
+    ``solve(rhs, adjoint)`` solves one right-hand side per shift through
+    ``eb_ringlu_solve_many`` the same way. ``capacity`` fixes the number of shift workspaces
+    (each ``ringlu_workspace_bytes(M, N)`` bytes, in one device allocation).
     """
 
     def __init__(self, batch: _lib.Batch, capacity: int, tol: float = 1e-10,
@@ -209,49 +210,33 @@ class RingLUMany:
         need = self._lib.eb_ringlu_workspace_bytes(batch.single.M, batch.single.N)
         if need < 0:
             raise ValueError("ring LU needs a single instance with M >= 4, N >= 5")
-        self.bytes = int(need)
-        self.workspaces = [torch.empty(self.bytes, dtype=torch.uint8, device="cuda")
-                           for _ in range(int(capacity))]
-        self.streams = [torch.cuda.Stream() for _ in range(int(capacity))]
+        self.stride = (int(need) + 255) // 256 * 256
+        self.capacity = int(capacity)
+        self.workspace = torch.empty(self.stride * self.capacity, dtype=torch.uint8, device="cuda")
         self.J = None
         self.shifts: list[complex] = []
 
-    @property
-    def capacity(self) -> int:
-        return len(self.workspaces)
-
-    def _ptrs(self, n: int):
-        ws = (ctypes.c_void_p * n)(*[w.data_ptr() for w in self.workspaces[:n]])
-        st = (ctypes.c_void_p * n)(*[s.cuda_stream for s in self.streams[:n]])
-        return ws, st
-
-    def _join(self, n: int) -> None:
-        cur = self._torch.cuda.current_stream()
-        for s in self.streams[:n]:
-            cur.wait_stream(s)
-
-    def _fork(self, n: int) -> None:
-        cur = self._torch.cuda.current_stream()
-        for s in self.streams[:n]:
-            s.wait_stream(cur)
+    def _shift_array(self) -> np.ndarray:
+        sh = np.zeros(2 * len(self.shifts))
+        sh[0::2] = np.real(self.shifts)
+        sh[1::2] = np.imag(self.shifts)
+        return sh
 
     def factor(self, J, shifts) -> None:
         shifts = [complex(v) for v in np.atleast_1d(shifts)]
         n = len(shifts)
         if not 1 <= n <= self.capacity:
             raise ValueError(f"{n} shifts for {self.capacity} workspaces")
-        sh = np.zeros(2 * n)
-        sh[0::2] = np.real(shifts)
-        sh[1::2] = np.imag(shifts)
-        ws, st = self._ptrs(n)
-        self._fork(n)
+        self.J, self.shifts = None, shifts
+        sh = self._shift_array()
         rc = self._lib.eb_ringlu_factor_many(ctypes.byref(self.batch), J.data_ptr(), n,
-                                             sh.ctypes.data, ws, self.bytes, st)
-        self._join(n)
+                                             sh.ctypes.data, self.workspace.data_ptr(),
+                                             self.stride,
+                                             self._torch.cuda.current_stream().cuda_stream)
         if rc != _lib.EB_OK:
             raise _lib.EulerB200Error("eb_ringlu_factor_many", rc,
                                       self._lib.eb_last_error().decode())
-        self.J, self.shifts = J, shifts
+        self.J = J
 
     def solve(self, rhs, adjoint: bool = False, out=None):
         """Solves system ``s`` for ``rhs[s]`` (a sequence of, or a stacked, device tensor);
@@ -264,18 +249,15 @@ class RingLUMany:
         torch = self._torch
         x = (torch.empty_like(rhs) if isinstance(rhs, torch.Tensor)
              else [torch.empty_like(r) for r in rhs]) if out is None else out
-        sh = np.zeros(2 * n)
-        sh[0::2] = np.real(self.shifts)
-        sh[1::2] = np.imag(self.shifts)
-        ws, st = self._ptrs(n)
+        sh = self._shift_array()
         rp = (ctypes.c_void_p * n)(*[rhs[k].data_ptr() for k in range(n)])
         xp = (ctypes.c_void_p * n)(*[x[k].data_ptr() for k in range(n)])
         rel = (ctypes.c_double * n)()
-        self._fork(n)
         rc = self._lib.eb_ringlu_solve_many(ctypes.byref(self.batch), self.J.data_ptr(), n,
-                                            sh.ctypes.data, 1 if adjoint else 0, ws, self.bytes,
-                                            rp, xp, self.tol, self.max_refine, rel, st)
-        self._join(n)
+                                            sh.ctypes.data, 1 if adjoint else 0,
+                                            self.workspace.data_ptr(), self.stride, rp, xp,
+                                            self.tol, self.max_refine, rel,
+                                            torch.cuda.current_stream().cuda_stream)
         if rc != _lib.EB_OK:
             raise _lib.EulerB200Error("eb_ringlu_solve_many", rc,
                                       self._lib.eb_last_error().decode() + f" (rel {list(rel)})")
