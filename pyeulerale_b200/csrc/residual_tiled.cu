@@ -11,9 +11,12 @@
 //     centred on the state along the angular and the radial direction (each face's JST sensor
 //     is the max_c of the sensors centred on its two cells, f90:208-211; the wall and
 //     far-field rows use their ghost states as the missing neighbour);
-//  4. each thread evaluates the four faces of its cell in the cell's own orientation (the
-//     asymmetric max_c of the reference decides per cell, f90:111-120) and writes
-//     -(F_b + F_f + F_i + F_o) / area (f90:370-436).
+//  4. each face is evaluated once for its two cells: the reference evaluates it twice, once in
+//     each cell's orientation, and the two evaluations share the central and ALE parts exactly
+//     (negated); the asymmetric max_c decisions (f90:111-120) and the fourth-difference
+//     evaluation order are taken per orientation. Faces whose two evaluations use different
+//     stencils (next to the wall and the far field, f90:401-436) are evaluated per cell. Each
+//     cell then writes -(F_b + F_f + F_i + F_o) / area (f90:370-436).
 // Results agree with the reference to the rounding of the reordered arithmetic (<= 1e-12
 // relative); every branch (boundary cases, max_c tolerance) follows the reference.
 
@@ -36,6 +39,8 @@ struct TileSmem {
   double s_ang[kTM * (kTN + 2)];   // angular sensor centred on (r, c), c in [-1, kTN]
   double s_rad[(kTM + 2) * kTN];   // radial sensor centred on (r, c), r in [-1, kTM]
   double x[kVerts], z[kVerts], vx[kVerts], vz[kVerts];
+  double ff[4][kTN][kTM];          // flux through face f of each cell (from its f neighbour's face)
+  double fo[4][kTN][kTM];          // flux through face o of each cell (from its o neighbour's face)
 };
 
 __device__ __forceinline__ int sidx(int r, int c) { return (c + 2) * kSR + (r + 2); }
@@ -127,9 +132,44 @@ __device__ __forceinline__ Flux jst(const St& ll, const St& l, const St& r, cons
   return F;
 }
 
+// Both orientations of one JST face: F = make_face_flux(ll, l, r, rr, n) for the cell l and
+// F' = make_face_flux(rr, r, l, ll, -n) for the cell r (f90:189-220). The central and ALE parts
+// of F' are the exact negatives of F's; the orientations differ in the asymmetric max_c
+// decisions (spectral radius and sensor) and in the evaluation order of the fourth difference,
+// which are evaluated per orientation as the reference does.
+__device__ __forceinline__ void jst_pair(const St& ll, const St& l, const St& r, const St& rr,
+                                         double nx, double nz, double len, double vn, double sl,
+                                         double sr, const Instance& in, Flux& F, Flux& Fp) {
+  const double vl = (nx * l.j1 + nz * l.j2) * l.ir;
+  const double vr = (nx * r.j1 + nz * r.j2) * r.ir;
+  const double al = fabs(vl) + l.cs * len, ar = fabs(vr) + r.cs * len;
+  const double lam = max_cd(al, ar), lamp = max_cd(ar, al);
+  const double coef2 = in.k2 * max_cd(sl, sr) * lam;
+  const double coef2p = in.k2 * max_cd(sr, sl) * lamp;
+  const double c4 = in.k4 * lam - in.c4 * coef2;
+  const double c4p = in.k4 * lamp - in.c4 * coef2p;
+  const double coef4 = (0.0 > c4 + 1e-8) ? 0.0 : c4;
+  const double coef4p = (0.0 > c4p + 1e-8) ? 0.0 : c4p;
+  const double lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
+  const double llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
+  const double fl[4] = {l.rho * vl, l.j1 * vl + nx * l.p, l.j2 * vl + nz * l.p, (l.e + l.p) * vl};
+  const double fr[4] = {r.rho * vr, r.j1 * vr + nx * r.p, r.j2 * vr + nz * r.p, (r.e + r.p) * vr};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double c = (fl[k] + fr[k]) / 2.0;
+    const double d1 = rv[k] - lv[k];
+    const double d3 = rrv[k] - 3.0 * rv[k] + 3.0 * lv[k] - llv[k];
+    const double d3p = llv[k] - 3.0 * lv[k] + 3.0 * rv[k] - rrv[k];
+    const double a = (lv[k] + rv[k]) / 2.0 * vn;
+    F.f[k] = (c - (coef2 * d1 - coef4 * d3)) - a;
+    Fp.f[k] = (-c - (coef2p * -d1 - coef4p * d3p)) + a;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
 k_residual_tiled(Table t, const double* X, const double* V, const double* U, double* R) {
-  __shared__ TileSmem S;
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  TileSmem& S = *reinterpret_cast<TileSmem*>(tile_smem);
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;
   const int M = in.M, N = in.N;
   const int tiles_m = (M + kTM - 1) / kTM;
@@ -203,91 +243,116 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
   }
   __syncthreads();
 
-  // 3. the cell's four faces
+  // 3. faces. Thread (r, c) evaluates the angular face between cells (r, c-1) and (r, c) and the
+  // radial face between cells (r-1, c) and (r, c), each once for both adjacent cells where the
+  // reference's two evaluations have the same stencil; its own cell's fluxes (faces b and i)
+  // stay in registers, the neighbours' (faces f and o) go to shared memory. The tile's last
+  // face column / row is evaluated by threads 0..31 / 32..39 in addition.
   const int r = tid % kTM, c = tid / kTM;
   const int m = m0 + r, n = n0 + c;
-  if (m >= M || n >= N) return;
-  const int flag = boundary_flag(M, m);
+  const bool own = m < M && n < N;
+  Flux Fb{}, Fi{};
+  auto exists = [&](int rr, int cc) { return rr >= 0 && cc >= 0 && m0 + rr < M && n0 + cc < N; };
+  auto angular_face = [&](int fr, int fc, bool want_b, bool want_f, Flux& Fb_out) {
+    // l = (fr, fc), r = (fr, fc - 1): face b of (fr, fc) and face f of (fr, fc - 1)
+    const double nbx = S.z[vidx(fr, fc)] - S.z[vidx(fr + 1, fc)];
+    const double nbz = S.x[vidx(fr + 1, fc)] - S.x[vidx(fr, fc)];
+    const double vn = (S.vx[vidx(fr + 1, fc)] + S.vx[vidx(fr, fc)]) / 2.0 * nbx +
+                      (S.vz[vidx(fr + 1, fc)] + S.vz[vidx(fr, fc)]) / 2.0 * nbz;
+    const double len = sqrt(nbx * nbx + nbz * nbz);
+    Flux F, Fp;
+    jst_pair(staged(S, sidx(fr, fc + 1)), staged(S, sidx(fr, fc)), staged(S, sidx(fr, fc - 1)),
+             staged(S, sidx(fr, fc - 2)), nbx, nbz, len, vn, S.s_ang[fc * kTM + fr + kTM],
+             S.s_ang[(fc - 1) * kTM + fr + kTM], in, F, Fp);
+    if (want_b) Fb_out = F;
+    if (want_f)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) S.ff[k][fc - 1][fr] = Fp.f[k];
+  };
+  auto radial_face = [&](int fr, int fc, bool want_i, bool want_o, Flux& Fi_out) {
+    // l = (fr, fc), r = (fr - 1, fc): face i of (fr, fc) and face o of (fr - 1, fc)
+    const int fm = m0 + fr;
+    const double nix = S.z[vidx(fr, fc + 1)] - S.z[vidx(fr, fc)];
+    const double niz = S.x[vidx(fr, fc)] - S.x[vidx(fr, fc + 1)];
+    const double gx = (S.vx[vidx(fr, fc)] + S.vx[vidx(fr, fc + 1)]) / 2.0;
+    const double gz = (S.vz[vidx(fr, fc)] + S.vz[vidx(fr, fc + 1)]) / 2.0;
+    const double vn = gx * nix + gz * niz;
+    Flux F{}, Fp{};
+    if (fm == 0) {  // wall face of cell 0 (flag 1): central flux with the wall ghost
+      const St C = staged(S, sidx(fr, fc));
+      F = central(C, wall_ghost_st(C, nix, niz, gx, gz), nix, niz, vn);
+    } else if (fm == M) {  // far-field face of cell M-1 (flag 5): central flux with the ghost
+      const St C = staged(S, sidx(fr - 1, fc));
+      Fp = central(C, farfield_ghost_st(C, in), -nix, -niz, -vn);
+    } else {
+      const double len = sqrt(nix * nix + niz * niz);
+      const St L = staged(S, sidx(fr, fc)), R = staged(S, sidx(fr - 1, fc));
+      const double sl = S.s_rad[fc * (kTM + 2) + fr + 1], sr = S.s_rad[fc * (kTM + 2) + fr];
+      if (fm == 1) {
+        // face i of cell 1 (flag 2): central; face o of cell 0 (flag 1): JST whose outer
+        // neighbour is the wall ghost of cell 0
+        F = central(L, R, nix, niz, vn);
+        if (want_o) {
+          const double wx = S.z[vidx(fr - 1, fc + 1)] - S.z[vidx(fr - 1, fc)];
+          const double wz = S.x[vidx(fr - 1, fc)] - S.x[vidx(fr - 1, fc + 1)];
+          const double wgx = (S.vx[vidx(fr - 1, fc)] + S.vx[vidx(fr - 1, fc + 1)]) / 2.0;
+          const double wgz = (S.vz[vidx(fr - 1, fc)] + S.vz[vidx(fr - 1, fc + 1)]) / 2.0;
+          Fp = jst(wall_ghost_st(R, wx, wz, wgx, wgz), R, L, staged(S, sidx(fr + 1, fc)), -nix,
+                   -niz, len, -vn, sr, sl, in);
+        }
+      } else if (fm == M - 1) {
+        // face i of cell M-1 (flag 5): JST whose outer neighbour is the far-field ghost;
+        // face o of cell M-2 (flag 4): central
+        F = jst(farfield_ghost_st(L, in), L, R, staged(S, sidx(fr - 2, fc)), nix, niz, len, vn, sl,
+                sr, in);
+        Fp = central(R, L, -nix, -niz, -vn);
+      } else {
+        jst_pair(staged(S, sidx(fr + 1, fc)), L, R, staged(S, sidx(fr - 2, fc)), nix, niz, len, vn,
+                 sl, sr, in, F, Fp);
+      }
+    }
+    if (want_i) Fi_out = F;
+    if (want_o)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) S.fo[k][fc][fr - 1] = Fp.f[k];
+  };
+  if (m < M && (own || exists(r, c - 1))) angular_face(r, c, own, exists(r, c - 1), Fb);
+  if (m <= M && n < N) radial_face(r, c, own, exists(r - 1, c), Fi);
+  if (tid < kTM) {
+    if (exists(tid, kTN - 1)) {
+      Flux unused;
+      angular_face(tid, kTN, false, true, unused);
+    }
+  } else if (tid < kTM + kTN) {
+    if (exists(kTM - 1, tid - kTM)) {
+      Flux unused;
+      radial_face(kTM, tid - kTM, false, true, unused);
+    }
+  }
+  __syncthreads();
+  if (!own) return;
   const double bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
   const double fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
   const double fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
   const double box = S.x[vidx(r + 1, c)], boz = S.z[vidx(r + 1, c)];
-  const double gbix = S.vx[vidx(r, c)], gbiz = S.vz[vidx(r, c)];
-  const double gfix = S.vx[vidx(r, c + 1)], gfiz = S.vz[vidx(r, c + 1)];
-  const double gfox = S.vx[vidx(r + 1, c + 1)], gfoz = S.vz[vidx(r + 1, c + 1)];
-  const double gbox = S.vx[vidx(r + 1, c)], gboz = S.vz[vidx(r + 1, c)];
   const double area = fabs((fox - bix) * (boz - fiz) - (foz - biz) * (box - fix)) / 2.0;
-  // normals (make_normal, f90:306-311) and grid velocities (make_grid_velo, f90:320-324)
-  const double nix = fiz - biz, niz = bix - fix;
-  const double nfx = foz - fiz, nfz = fix - fox;
-  const double nox = boz - foz, noz = fox - box;
-  const double nbx = biz - boz, nbz = box - bix;
-  const double vni = (gbix + gfix) / 2.0 * nix + (gbiz + gfiz) / 2.0 * niz;
-  const double vnf = (gfix + gfox) / 2.0 * nfx + (gfiz + gfoz) / 2.0 * nfz;
-  const double vno = (gfox + gbox) / 2.0 * nox + (gfoz + gboz) / 2.0 * noz;
-  const double vnb = (gbox + gbix) / 2.0 * nbx + (gboz + gbiz) / 2.0 * nbz;
-  const St C = staged(S, sidx(r, c));
-  const double sac = S.s_ang[c * kTM + r + kTM];          // angular sensor centred on c
-  const double src = S.s_rad[c * (kTM + 2) + r + 1];      // radial sensor centred on c
-  // face b (l = c, r = b, ll = f, rr = bb)
-  const Flux Fb = jst(staged(S, sidx(r, c + 1)), C, staged(S, sidx(r, c - 1)),
-                      staged(S, sidx(r, c - 2)), nbx, nbz, sqrt(nbx * nbx + nbz * nbz), vnb,
-                      sac, S.s_ang[(c - 1) * kTM + r + kTM], in);
-  // face f (l = c, r = f, ll = b, rr = ff)
-  const Flux Ff = jst(staged(S, sidx(r, c - 1)), C, staged(S, sidx(r, c + 1)),
-                      staged(S, sidx(r, c + 2)), nfx, nfz, sqrt(nfx * nfx + nfz * nfz), vnf,
-                      sac, S.s_ang[(c + 1) * kTM + r + kTM], in);
-  Flux Fi, Fo;
-  const double leni = sqrt(nix * nix + niz * niz), leno = sqrt(nox * nox + noz * noz);
-  switch (flag) {
-    case 1: {
-      const St G = wall_ghost_st(C, nix, niz, (gbix + gfix) / 2.0, (gbiz + gfiz) / 2.0);
-      Fi = central(C, G, nix, niz, vni);
-      Fo = jst(G, C, staged(S, sidx(r + 1, c)), staged(S, sidx(r + 2, c)), nox, noz, leno, vno,
-               src, S.s_rad[c * (kTM + 2) + r + 2], in);
-      break;
-    }
-    case 2:
-      Fi = central(C, staged(S, sidx(r - 1, c)), nix, niz, vni);
-      Fo = jst(staged(S, sidx(r - 1, c)), C, staged(S, sidx(r + 1, c)),
-               staged(S, sidx(r + 2, c)), nox, noz, leno, vno, src,
-               S.s_rad[c * (kTM + 2) + r + 2], in);
-      break;
-    case 5: {
-      const St G = farfield_ghost_st(C, in);
-      Fi = jst(G, C, staged(S, sidx(r - 1, c)), staged(S, sidx(r - 2, c)), nix, niz, leni, vni,
-               src, S.s_rad[c * (kTM + 2) + r], in);
-      Fo = central(C, G, nox, noz, vno);
-      break;
-    }
-    default:
-      Fi = jst(staged(S, sidx(r + 1, c)), C, staged(S, sidx(r - 1, c)),
-               staged(S, sidx(r - 2, c)), nix, niz, leni, vni, src,
-               S.s_rad[c * (kTM + 2) + r], in);
-      if (flag == 4) {
-        Fo = central(C, staged(S, sidx(r + 1, c)), nox, noz, vno);
-      } else {
-        Fo = jst(staged(S, sidx(r - 1, c)), C, staged(S, sidx(r + 1, c)),
-                 staged(S, sidx(r + 2, c)), nox, noz, leno, vno, src,
-                 S.s_rad[c * (kTM + 2) + r + 2], in);
-      }
-      break;
-  }
   const double ia = 1.0 / area;
+  double res[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) res[k] = -(((Fb.f[k] + S.ff[k][c][r]) + Fi.f[k]) + S.fo[k][c][r]) * ia;
   double* out = R + 4 * (in.cell_offset + m + (int64_t)M * n);
-  const double r0 = -(((Fb.f[0] + Ff.f[0]) + Fi.f[0]) + Fo.f[0]) * ia;
-  const double r1 = -(((Fb.f[1] + Ff.f[1]) + Fi.f[1]) + Fo.f[1]) * ia;
-  const double r2 = -(((Fb.f[2] + Ff.f[2]) + Fi.f[2]) + Fo.f[2]) * ia;
-  const double r3 = -(((Fb.f[3] + Ff.f[3]) + Fi.f[3]) + Fo.f[3]) * ia;
-  reinterpret_cast<double2*>(out)[0] = make_double2(r0, r1);
-  reinterpret_cast<double2*>(out)[1] = make_double2(r2, r3);
+  reinterpret_cast<double2*>(out)[0] = make_double2(res[0], res[1]);
+  reinterpret_cast<double2*>(out)[1] = make_double2(res[2], res[3]);
 }
 
 int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
                           double* R, cudaStream_t stream, int max_tiles) {
   const Table t = make_table(b);
   dim3 grid(max_tiles, b->n_inst);
-  k_residual_tiled<<<grid, kThreads, 0, stream>>>(t, X, V, U, R);
+  if (cudaFuncSetAttribute(k_residual_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(TileSmem)) != cudaSuccess)
+    return check_launch("compute_odes attribute");
+  k_residual_tiled<<<grid, kThreads, sizeof(TileSmem), stream>>>(t, X, V, U, R);
   return check_launch("compute_odes");
 }
 
