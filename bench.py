@@ -11,7 +11,9 @@ table.
 One timed "step" is one residual evaluation R(Ma, U, X, V) of the whole batch (one launch).
 The JSON line reports cell-residual evaluations per second (``value``), and beside it the VJP
 rate (full set of reverse products per instance: d/dU, d/dX, d/dV, d/dMa) and the resolvent
-rate (ring-block LU factor + refined solve to 1e-10 relative residual per shift).
+rate: the pitch frequency response (64 shifts) plus the adjoint lift gradient of the PTC steady
+state of one instance, solved to 1e-10 relative residual, with the shifts factored together
+(batched) and one at a time through the drop-in class (plain).
 
 ``--impl reference`` times the CPU restatement of the reference (complex arithmetic, all host
 threads) on a bounded sample of the same workload. Under torchrun every rank processes its own
@@ -53,9 +55,11 @@ def parse_args():
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--instances", type=int, default=256, help="instances per GPU")
     p.add_argument("--shifts", type=int, default=4,
-                   help="resolvent shifts timed one at a time (plain path)")
-    p.add_argument("--batched-shifts", type=int, default=32,
-                   help="resolvent shifts timed through the multi-shift factor / solve")
+                   help="frequency-response shifts timed one at a time (plain path)")
+    p.add_argument("--batched-shifts", type=int, default=64,
+                   help="frequency-response shifts timed through the batched driver")
+    p.add_argument("--parts", default="residual,vjp,resolvent",
+                   help="comma-separated parts to run besides the residual (vjp, resolvent)")
     p.add_argument("--shift-group", type=int, default=16,
                    help="shifts factored concurrently (one workspace of ~2.7 GB each)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline budget")
@@ -214,9 +218,10 @@ def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
 
-    from pyeulerale_b200 import _lib, solver
+    from pyeulerale_b200 import _lib
     from pyeulerale_b200.batch import InstanceSet, InstanceSpec
 
+    parts = set(args.parts.split(","))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -301,91 +306,96 @@ def run_b200(args) -> None:
     e2e_value = world * cells * e2e_steps / t_e2e
 
     # VJP set on stored Jacobians (d/dU, d/dX, d/dV, d/dMa) per instance
-    J_u = torch.empty(144 * cells, **f64)
-    J_x = torch.empty(32 * cells, **f64)
-    J_v = torch.empty(32 * cells, **f64)
-    J_m = torch.empty(4 * cells, **f64)
-    inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u, stream=sp)
-    inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, J_x, stream=sp)
-    inst.call("eb_compute_odes_wrt_velocities", dX, dV, dU, J_v, stream=sp)
-    inst.call("eb_compute_odes_wrt_mach", dX, dV, dU, J_m, stream=sp)
-    w = torch.randn(8 * cells, **f64)
-    gU = torch.empty(8 * cells, **f64)
-    gX = torch.empty(4 * inst.n_verts, **f64)
-    gV = torch.empty(4 * inst.n_verts, **f64)
-    gM = torch.empty(2 * B, **f64)
+    vjp_rate = vjp_gbs = None
+    if "vjp" in parts:
+        J_u = torch.empty(144 * cells, **f64)
+        J_x = torch.empty(32 * cells, **f64)
+        J_v = torch.empty(32 * cells, **f64)
+        J_m = torch.empty(4 * cells, **f64)
+        inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u, stream=sp)
+        inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, J_x, stream=sp)
+        inst.call("eb_compute_odes_wrt_velocities", dX, dV, dU, J_v, stream=sp)
+        inst.call("eb_compute_odes_wrt_mach", dX, dV, dU, J_m, stream=sp)
+        w = torch.randn(8 * cells, **f64)
+        gU = torch.empty(8 * cells, **f64)
+        gX = torch.empty(4 * inst.n_verts, **f64)
+        gV = torch.empty(4 * inst.n_verts, **f64)
+        gM = torch.empty(2 * B, **f64)
 
-    def vjp():
-        inst.call("eb_apply_odes_wrt_states_rev", J_u, w, gU, stream=sp)
-        inst.call("eb_apply_odes_wrt_vertices_rev", J_x, w, gX, stream=sp)
-        inst.call("eb_apply_odes_wrt_vertices_rev", J_v, w, gV, stream=sp)
-        inst.call("eb_apply_odes_wrt_mach_rev", J_m, w, gM, stream=sp)
+        def vjp():
+            inst.call("eb_apply_odes_wrt_states_rev", J_u, w, gU, stream=sp)
+            inst.call("eb_apply_odes_wrt_vertices_rev", J_x, w, gX, stream=sp)
+            inst.call("eb_apply_odes_wrt_vertices_rev", J_v, w, gV, stream=sp)
+            inst.call("eb_apply_odes_wrt_mach_rev", J_m, w, gM, stream=sp)
 
-    for _ in range(args.warmup):
-        vjp()
-    barrier()
-    v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    vsteps = max(5, args.steps // 2)
-    v0.record(stream)
-    for _ in range(vsteps):
-        vjp()
-    v1.record(stream)
-    barrier()
-    t_vjp = max_over_ranks(v0.elapsed_time(v1) / 1e3)
-    vjp_rate = world * B * vsteps / t_vjp
-    vjp_gbs = BYTES_PER_CELL_VJP * cells * vsteps / t_vjp / 1e9
-    del J_x, J_v, J_m
+        for _ in range(args.warmup):
+            vjp()
+        barrier()
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        vsteps = max(5, args.steps // 2)
+        v0.record(stream)
+        for _ in range(vsteps):
+            vjp()
+        v1.record(stream)
+        barrier()
+        t_vjp = max_over_ranks(v0.elapsed_time(v1) / 1e3)
+        vjp_rate = world * B * vsteps / t_vjp
+        vjp_gbs = BYTES_PER_CELL_VJP * cells * vsteps / t_vjp / 1e9
+        del J_u, J_x, J_v, J_m
 
-    # resolvent: ring-block LU factor + refined solve per frequency-response shift,
-    # s = i k V / (c / 2) with k log-spaced on [0.01, 10]
-    single = InstanceSet([specs[0]])
-    J1 = J_u[:144 * single.n_cells]
-    rng = np.random.default_rng(rank)
-    b = torch.from_numpy(rng.standard_normal(8 * single.n_cells)).cuda()
+    # resolvent: the frequency response of the steady state (PTC from free stream), 64 shifts
+    # s = i k V / (c / 2), k log-spaced on [0.01, 10], plus the adjoint lift gradient; batched
+    # (shift_group shifts per factorisation call) against one shift at a time through the
+    # drop-in class
+    res = None
+    if "resolvent" in parts:
+        from pyeulerale_b200 import SpatialDiscretization, drivers
 
-    def freq_shifts(n):
-        return [1j * k * FLOW["mach"] * 1.4**0.5 / (GRID["chord"] / 2)
-                for k in np.logspace(-2, 1, max(n, 1))]
-
-    lu = solver.RingLU(single.batch, tol=1e-10)
-    shifts = freq_shifts(args.shifts)
-    lu.factor(J1, shifts[0])  # warm-up (handles, workspace)
-    lu.solve(b)
-    barrier()
-    t0 = time.perf_counter()
-    rels = []
-    for s in shifts:
-        lu.factor(J1, s)
-        _, rel = lu.solve(b)
-        rels.append(rel)
-    barrier()
-    t_solve = max_over_ranks(time.perf_counter() - t0)
-    solve_rate = world * len(shifts) / t_solve
-    del lu
-
-    # the same solves, shift_group shifts per factor / solve call (batched launches)
-    group = max(1, min(args.shift_group, args.batched_shifts))
-    many = solver.RingLUMany(single.batch, capacity=group, tol=1e-10)
-    bshifts = freq_shifts(args.batched_shifts)
-    many.factor(J1, bshifts[:group])  # warm-up
-    many.solve([b] * group)
-    barrier()
-    t_fac = t_sol = 0.0
-    brels = []
-    for g0 in range(0, len(bshifts), group):
-        chunk = bshifts[g0:g0 + group]
+        sd = SpatialDiscretization(X, mach_number=FLOW["mach"], angle_of_attack=FLOW["aoa_deg"],
+                                   coefficient_length=GRID["chord"],
+                                   coefficient_center=FLOW["center"])
         t0 = time.perf_counter()
-        many.factor(J1, chunk)
-        t1 = time.perf_counter()
-        _, r = many.solve([b] * len(chunk))
-        torch.cuda.synchronize()
-        t_fac += t1 - t0
-        t_sol += time.perf_counter() - t1
-        brels += r
-    barrier()
-    t_batched = max_over_ranks(t_fac + t_sol)
-    batched_rate = world * len(bshifts) / t_batched
-    del many
+        hist = drivers.ptc(sd, rtol=1e-10, max_iter=200)
+        t_ptc = time.perf_counter() - t0
+        ks = np.logspace(-2, 1, max(args.batched_shifts, 1))
+        ks_plain = ks[np.linspace(0, len(ks) - 1, max(min(args.shifts, len(ks)), 1)).astype(int)]
+        drivers.frequency_response(sd, GRID["chord"], FLOW["center"][0], ks_plain[:1])  # warm-up
+        barrier()
+        t0 = time.perf_counter()
+        cl_p, cm_p = drivers.frequency_response(sd, GRID["chord"], FLOW["center"][0], ks_plain)
+        grad_p = drivers.adjoint_lift_gradient(sd)
+        barrier()
+        t_plain = max_over_ranks(time.perf_counter() - t0)
+        group = max(1, min(args.shift_group, len(ks)))
+        drivers.frequency_response_batched(sd, GRID["chord"], FLOW["center"][0], ks[:group],
+                                           group=group)  # warm-up
+        barrier()
+        t0 = time.perf_counter()
+        cl_b, cm_b = drivers.frequency_response_batched(sd, GRID["chord"], FLOW["center"][0], ks,
+                                                        group=group)
+        grad_b = drivers.adjoint_lift_gradient(sd)
+        barrier()
+        t_batched = max_over_ranks(time.perf_counter() - t0)
+        sel = np.searchsorted(ks, ks_plain)
+        agree = max(float(np.max(np.abs(cl_b[sel] - cl_p)) / np.max(np.abs(cl_p))),
+                    float(np.max(np.abs(cm_b[sel] - cm_p)) / np.max(np.abs(cm_p))))
+        plain_rate = world * len(ks_plain) / t_plain
+        batched_rate = world * len(ks) / t_batched
+        res = {"value": batched_rate,
+               "unit": "transfer-function shifts/s (factor + refined solve to 1e-10 + forces)",
+               "workload": f"{len(ks)}-shift pitch frequency response of the PTC steady state "
+                           "of the 129x129 NACA-0004 grid plus the adjoint lift gradient",
+               "shifts": len(ks), "shift_group": group, "seconds": t_batched,
+               "plain": {"value": plain_rate, "shifts": len(ks_plain), "seconds": t_plain},
+               "batched_vs_plain": batched_rate / plain_rate,
+               "max_rel_diff_batched_vs_plain": agree,
+               "adjoint_gradient_rel_diff": float(np.max(np.abs(grad_b - grad_p))
+                                                  / np.max(np.abs(grad_p))),
+               "ptc": {"iterations": hist.iterations, "final_rel_residual": hist.rel_norms[-1],
+                       "seconds": t_ptc},
+               "method": "ring-block LU (batched Gauss-Jordan ring inversions + strided-batched "
+                         "ZGEMM), refined to 1e-10 relative residual"}
+        del sd
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -418,18 +428,10 @@ def run_b200(args) -> None:
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps,
         "clocks": clk,
-        "vjp": {"value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
-                "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4},
-        "resolvent": {"value": batched_rate, "unit": "resolvent solves/s (factor + solve)",
-                      "shifts": len(bshifts), "shift_group": group,
-                      "max_rel_residual": max(brels),
-                      "factor_s": t_fac, "solve_s": t_sol,
-                      "plain": {"value": solve_rate, "shifts": len(shifts),
-                                "max_rel_residual": max(rels)},
-                      "batched_vs_plain": batched_rate / solve_rate,
-                      "method": "ring-block LU (Gauss-Jordan ring inversions + strided-batched "
-                                "ZGEMM), refined to 1e-10; batched = all shifts of a group in "
-                                "each launch"},
+        "vjp": None if vjp_rate is None else {
+            "value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
+            "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4},
+        "resolvent": res,
     }
     print(json.dumps(line), flush=True)
 

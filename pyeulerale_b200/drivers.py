@@ -96,6 +96,83 @@ def frequency_response(solver, chord: float, axis_location: float,
     return np.array(cls), np.array(cms)
 
 
+def _device_apply(solver, name: str, jac, x, out_numel: int):
+    """y = jac-product(x) on the device; x, y interleaved complex float64 tensors."""
+    import torch
+
+    y = torch.empty(2 * out_numel, dtype=torch.float64, device="cuda")
+    solver._call(name, jac.data_ptr(), x.data_ptr(), y.data_ptr())
+    return y
+
+
+def frequency_response_batched(solver, chord: float, axis_location: float,
+                               reduced_frequencies, group: int = 16,
+                               tol: float = 1e-10) -> tuple[np.ndarray, np.ndarray]:
+    """``frequency_response`` with the shifts factored and solved together on the device.
+
+    The pitch-to-(c_l, c_m) transfer function at s = i k V_inf / (c/2) for every reduced
+    frequency k (examples/response/run.py:135-176): each shift solves
+    (dR/dU - s I) dU = -(dR/dX + s dR/dV) dX/dalpha; c_l(s) = <grad_F c_l, dF/dX dX + dF/dU dU>,
+    c_m(s) likewise plus <grad_X c_m, dX>. ``group`` shifts share each factorisation call
+    (``RingLUMany``: one launch per elimination step for the whole group); right-hand sides,
+    solutions and force perturbations stay on the device, only the 2 x len(k) coefficients
+    come back. The solver must be linearized at the state of interest.
+    """
+    import torch
+
+    from .solver import RingLUMany
+
+    ks = np.atleast_1d(np.asarray(reduced_frequencies, dtype=float))
+    speed = solver.mach_number * HEAT_RATIO**0.5
+    shifts = 1j * ks * speed / (chord / 2)
+    nc = solver.num_radial * solver.num_angular
+    nf = solver.forces.size
+    dX = pitch_vertices(solver, axis_location)
+    dXd = solver._cvec(dX)
+    rx = torch.view_as_complex(_device_apply(
+        solver, "eb_apply_odes_wrt_vertices_fwd", solver._dJ_x, dXd, 4 * nc).view(-1, 2))
+    rv = torch.view_as_complex(_device_apply(
+        solver, "eb_apply_odes_wrt_vertices_fwd", solver._dJ_v, dXd, 4 * nc).view(-1, 2))
+    dFx = torch.view_as_complex(_device_apply(
+        solver, "eb_apply_forces_wrt_vertices_fwd", solver._dJF_x, dXd, nf).view(-1, 2))
+    to_dev = lambda a: torch.from_numpy(  # noqa: E731
+        np.ascontiguousarray(np.asarray(a, dtype=complex).ravel(order="F"))).to("cuda")
+    cl_grad = to_dev(solver.compute_lift_coefficient_wrt_forces())
+    cm_grad = to_dev(solver.compute_moment_coefficient_wrt_forces())
+    cm_x = complex(np.vdot(solver.compute_moment_coefficient_wrt_vertices(), dX))
+    lu = RingLUMany(solver._batch(), capacity=min(group, len(shifts)), tol=tol)
+    cl = np.empty(len(shifts), dtype=complex)
+    cm = np.empty(len(shifts), dtype=complex)
+    for g0 in range(0, len(shifts), lu.capacity):
+        chunk = shifts[g0:g0 + lu.capacity]
+        st = torch.from_numpy(chunk).to("cuda")[:, None]
+        rhs = torch.view_as_real(-(rx[None, :] + st * rv[None, :])).reshape(len(chunk), -1)
+        rhs = rhs.contiguous()
+        lu.factor(solver._dJ_u, chunk)
+        x, _ = lu.solve(rhs)
+        dF = torch.stack([torch.view_as_complex(_device_apply(
+            solver, "eb_apply_forces_wrt_states_fwd", solver._dJF_u, x[k], nf).view(-1, 2))
+            for k in range(len(chunk))]) + dFx[None, :]
+        cl[g0:g0 + len(chunk)] = (dF @ cl_grad.conj()).cpu().numpy()
+        cm[g0:g0 + len(chunk)] = (dF @ cm_grad.conj()).cpu().numpy() + cm_x
+    return cl, cm
+
+
+def adjoint_lift_gradient(solver) -> np.ndarray:
+    """Gradient of the steady-state lift coefficient with respect to the grid vertices.
+
+    With R(U, X) = 0 at the solver's (converged, linearized) state, dc_l/dX =
+    (dF/dX)^T g - (dR/dX)^T lam with g = grad_F c_l and (dR/dU)^T lam = (dF/dU)^T g: one adjoint
+    solve (solve_odes_wrt_states_adj at shift 0) and three reverse products, the device
+    counterpart of the adjoint of examples/gain/run.py:107-109. Returns (2, M+1, N+1).
+    """
+    g = solver.compute_lift_coefficient_wrt_forces().astype(complex)
+    lam = solver.solve_odes_wrt_states_adj(solver.apply_forces_wrt_states_rev(d_forces=g))
+    grad = (solver.apply_forces_wrt_vertices_rev(d_forces=g)
+            - solver.apply_odes_wrt_vertices_rev(d_odes=lam.astype(complex)))
+    return np.asfortranarray(grad.real)
+
+
 def static_gain(solver, out=None) -> tuple[float, float]:
     """Lift slope dc_l/dalpha and its Mach derivative at zero angle of attack
     (examples/gain/run.py:81-145), with the adjoint of c_l and the exact second-order terms."""
