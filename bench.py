@@ -219,7 +219,7 @@ def run_b200(args) -> None:
     import torch.distributed as dist
 
     from pyeulerale_b200 import _lib
-    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec, max_over_ranks
 
     parts = set(args.parts.split(","))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -252,13 +252,6 @@ def run_b200(args) -> None:
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     # residual: warm-up, then K timed launches
     for _ in range(args.warmup):

@@ -265,6 +265,19 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const
                          const double* const* rhs, double* const* x, double tol, int max_refine,
                          double* rel_residuals, void* stream);
 
+/* ---- pressure coefficients --------------------------------------------------------------- */
+/* cp (real, one per cell, packed like the cells) of the states U: ((gamma-1)(E - |j|^2/2/rho) -
+ * 1) / q with q = gamma Ma^2 / 2 per instance (compute_pressure_coefficients,
+ * core.py:1423-1449). */
+int eb_compute_pressure_coefficients(const eb_batch* b, const double* U, double* cp,
+                                     void* stream);
+
+/* d_cp (complex, one per cell) = dcp/dU . d_states (complex (4, M, N) per instance)
+ * (apply_pressure_coefficients_wrt_states_fwd, core.py:1451-1488). */
+int eb_apply_pressure_coefficients_wrt_states_fwd(const eb_batch* b, const double* U,
+                                                  const double* d_states, double* d_cp,
+                                                  void* stream);
+
 /* ---- second-order building blocks ------------------------------------------------------ */
 /* Directional derivatives of the Jacobians: with a complex direction d on the variable
  * `dir_kind` (0 = states, 1 = vertices, 2 = velocities), these write dJ/de along Re(d) to

@@ -104,6 +104,8 @@ _SIGNATURES: dict[str, list] = {
     "eb_apply_forces_wrt_vertices_rev": ["b", "p", "p", "p", "s"],
     "eb_apply_odes_tangent": ["b", "p", "p", "p", "p", "p", "p", "p", "p", "p", "s"],
     "eb_convert_odes_wrt_states": ["b", "p", "p", "p", "p", "s"],
+    "eb_compute_pressure_coefficients": ["b", "p", "p", "s"],
+    "eb_apply_pressure_coefficients_wrt_states_fwd": ["b", "p", "p", "p", "s"],
     "eb_bsr_shifted_spmv": ["i64", "p", "p", "p", "d", "d", "p", "p", "s"],
     "eb_odes_wrt_mach_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],
     "eb_odes_wrt_states_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],

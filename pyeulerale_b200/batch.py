@@ -77,6 +77,23 @@ class InstanceSet:
     def __len__(self) -> int:
         return len(self.specs)
 
+    def set_mach(self, mach) -> None:
+        """Sets the free-stream Mach number of every instance (host and device tables)."""
+        import torch
+
+        values = [float(v) for v in (mach.tolist() if hasattr(mach, "tolist") else mach)]
+        if len(values) != len(self.specs):
+            raise ValueError(f"{len(values)} Mach numbers for {len(self.specs)} instances")
+        if all(v == self.host_table[i].mach for i, v in enumerate(values)):
+            return
+        for i, v in enumerate(values):
+            self.specs[i].mach = v
+            self.host_table[i].mach = v
+        raw = np.frombuffer(bytes(self.host_table), dtype=np.uint8).copy()
+        self.device_table.copy_(torch.from_numpy(raw))
+        if len(self.specs) == 1:
+            self.batch.single = self.host_table[0]
+
     def pack_vertices(self, arrays: list[np.ndarray] | None = None) -> np.ndarray:
         """Packed (2, ...) vertex-like arrays (default: the grids) as a flat float64 array."""
         arrays = arrays if arrays is not None else [s.vertices for s in self.specs]
@@ -107,3 +124,31 @@ def shard(items: list, rank: int, world: int) -> list:
     lo = (n * rank) // world
     hi = (n * (rank + 1)) // world
     return items[lo:hi]
+
+
+def gather(local: list) -> list:
+    """Every rank's ``local`` list concatenated in rank order, on every rank.
+
+    The instances are independent, so the only exchange is this host-side gather of the small
+    per-instance outputs (coefficients, norms); with one process it returns ``local``.
+    """
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(local)
+    parts: list = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, list(local))
+    return [x for part in parts for x in part]
+
+
+def max_over_ranks(seconds: float) -> float:
+    """The slowest rank's time (a job's time is the last rank's), on every rank."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return seconds
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([seconds], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())

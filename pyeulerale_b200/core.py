@@ -712,30 +712,32 @@ class SpatialDiscretization:
         return vertices_gradient
 
     def compute_pressure_coefficients(self, pressure_coefficients=None) -> np.ndarray:
-        """Pressure coefficients of all cells (core.py:1423-1449)."""
+        """Pressure coefficients of all cells, on the device (core.py:1423-1449)."""
         shape = (self.num_radial, self.num_angular)
         if pressure_coefficients is not None:
             self._check_array(pressure_coefficients, shape=shape,
                               dtype=np.dtypes.Float64DType())
         else:
             pressure_coefficients = np.asfortranarray(np.empty(dtype=float, shape=shape))
-        rho, jx, jz, e = self.states
-        pressure_coefficients[:] = ((HEAT_RATIO - 1.) * (e - (jx**2 + jz**2) / 2. / rho)
-                                    - 1.) / self._dynamic_pressure
+        torch = self._torch
+        self._upload(velocities=False)
+        cp = torch.empty(self._nc(), dtype=torch.float64, device="cuda")
+        self._call("eb_compute_pressure_coefficients", ptr(self._dU), ptr(cp))
+        pressure_coefficients[:] = np.reshape(cp.cpu().numpy(), shape, order="F")
         return pressure_coefficients
 
     def apply_pressure_coefficients_wrt_states_fwd(self, d_states,
                                                    d_pressure_coefficients=None) -> np.ndarray:
-        """``dcp/dU . dU`` (core.py:1451-1488)."""
+        """``dcp/dU . dU`` on the device (core.py:1451-1488)."""
         self._check_array(d_states, self._states.shape)
         shape = (self.num_radial, self.num_angular)
         if d_pressure_coefficients is not None:
             self._check_array(d_pressure_coefficients, shape=shape)
         else:
             d_pressure_coefficients = np.asfortranarray(np.empty(dtype=complex, shape=shape))
-        rho, jx, jz, _ = self.states
-        drho, djx, djz, de = d_states
-        d_pressure_coefficients[:] = (HEAT_RATIO - 1.) * (
-            de + (jx**2 + jz**2) / rho**2 / 2. * drho - (jx * djx + jz * djz) / rho
-        ) / self._dynamic_pressure
-        return d_pressure_coefficients
+        torch = self._torch
+        self._upload(velocities=False)
+        dcp = torch.empty(2 * self._nc(), dtype=torch.float64, device="cuda")
+        self._call("eb_apply_pressure_coefficients_wrt_states_fwd", ptr(self._dU),
+                   ptr(self._cvec(d_states)), ptr(dcp))
+        return self._store(d_pressure_coefficients, dcp, shape)

@@ -71,6 +71,38 @@ __global__ void k_free_stream(Table t, int64_t n_cells, double* U) {
   }
 }
 
+// Pressure coefficient ((gamma-1)(E - |j|^2/2/rho) - 1) / q, q = gamma Ma^2 / 2, of every cell
+// (compute_pressure_coefficients, core.py:1423-1449, in the reference's operation order).
+__global__ void k_pressure_coef(Table t, int64_t n_cells, const double* U, double* cp) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const double q = in.mach * in.mach * kGamma / 2;
+    const double2 a = __ldg(reinterpret_cast<const double2*>(U + 4 * g));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(U + 4 * g + 2));
+    cp[g] = (kGm1 * (b.y - (a.y * a.y + b.x * b.x) / 2. / a.x) - 1.) / q;
+  }
+}
+
+// Its tangent along complex dU (apply_pressure_coefficients_wrt_states_fwd, core.py:1451-1488):
+// (gamma-1)(dE + |j|^2/rho^2/2 drho - (jx djx + jz djz)/rho) / q.
+__global__ void k_pressure_coef_fwd(Table t, int64_t n_cells, const double* U, const double* dU,
+                                    double* dcp) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const Instance in = t.cell(g);
+    const double q = in.mach * in.mach * kGamma / 2;
+    const double rho = U[4 * g], jx = U[4 * g + 1], jz = U[4 * g + 2];
+    const double c1 = (jx * jx + jz * jz) / (rho * rho) / 2.;
+    const double* d = dU + 8 * g;
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {  // real, imaginary
+      const double drho = d[part], djx = d[2 + part], djz = d[4 + part], de = d[6 + part];
+      dcp[2 * g + part] = kGm1 * (de + c1 * drho - (jx * djx + jz * djz) / rho) / q;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(128) k_residual(Table t, int64_t n_cells, const double* X,
                                                   const double* V, const double* U, double* R) {
   for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
@@ -677,6 +709,26 @@ int eb_compute_forces(const eb_batch* b, const double* X, const double* U, doubl
   const Table t = make_table(b);
   k_forces<<<b->n_inst, 256, 0, EB_STREAM(stream)>>>(t, X, U, F, coef);
   return check_launch("compute_forces");
+}
+
+int eb_compute_pressure_coefficients(const eb_batch* b, const double* U, double* cp,
+                                     void* stream) {
+  EB_VALIDATE(b);
+  if (!U || !cp) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_pressure_coef<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, U, cp);
+  return check_launch("compute_pressure_coefficients");
+}
+
+int eb_apply_pressure_coefficients_wrt_states_fwd(const eb_batch* b, const double* U,
+                                                  const double* d_states, double* d_cp,
+                                                  void* stream) {
+  EB_VALIDATE(b);
+  if (!U || !d_states || !d_cp) return fail(EB_ERR_ARG, "null array");
+  const Table t = make_table(b);
+  k_pressure_coef_fwd<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, U,
+                                                                                 d_states, d_cp);
+  return check_launch("apply_pressure_coefficients_wrt_states_fwd");
 }
 
 int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double* d_mach,

@@ -68,9 +68,11 @@ def pitch_vertices(solver, axis_location: float) -> np.ndarray:
 
 
 def frequency_response(solver, chord: float, axis_location: float,
-                       reduced_frequencies, out=None) -> tuple[np.ndarray, np.ndarray]:
+                       reduced_frequencies, out=None, cp_file=None) -> tuple[np.ndarray, np.ndarray]:
     """Pitch-to-(c_l, c_m) transfer function at s = i k V_inf / (c/2)
-    (examples/response/run.py:125-176). Returns (c_l(s), c_m(s))."""
+    (examples/response/run.py:125-176). Returns (c_l(s), c_m(s)). With ``cp_file``, writes the
+    steady pressure coefficients and their pitch response at the last frequency in the
+    example's export format (examples/response/run.py:178-186)."""
     speed = solver.mach_number * HEAT_RATIO**0.5
     dX = pitch_vertices(solver, axis_location)
     cl_grad = solver.compute_lift_coefficient_wrt_forces()
@@ -93,6 +95,11 @@ def frequency_response(solver, chord: float, axis_location: float,
         cms.append(cm)
         if out is not None:
             print(f"{k:>15.3e} {cl:>+25.3e} {cm:>+25.3e}", file=out)
+    if cp_file is not None and len(cls):
+        from .export import export_pressure_coefficients
+
+        export_pressure_coefficients(cp_file, solver.vertices, solver.compute_pressure_coefficients(),
+                                     solver.apply_pressure_coefficients_wrt_states_fwd(dU))
     return np.array(cls), np.array(cms)
 
 

@@ -13,6 +13,10 @@ It writes, next to this script:
 * ``*.out`` -- the reference's committed golden outputs of its CI examples
   (``examples/response/Ma0p05.out``, ``Ma0p5.out``, ``examples/gain/Ma0p10.out``,
   ``Ma0p50.out``), the end-to-end pins of the residual history, transfer functions and gains;
+* ``cp_export_8x9.txt`` -- the uncompressed output of the reference's own
+  ``export_pressure_coefficients`` (examples/response/run.py:32-63, taken from that file
+  unmodified) for the 8x9 state below, its pressure coefficients and their tangent along a
+  seeded direction;
 * ``reference_8x9.npz`` -- outputs of the reference's own Python class
   (``src/py_euler_ale/core.py``, unmodified) running on the C++ oracle for the state of its
   unit tests (``tests/test_linearization.py:26-33``: seed 1, 0.5 % noise): residual, forces,
@@ -22,8 +26,11 @@ It writes, next to this script:
 
 from __future__ import annotations
 
+import ast
+import gzip
 import shutil
 import sys
+import tempfile
 from pathlib import Path
 
 import numpy as np
@@ -61,6 +68,17 @@ SECOND_ORDER = [
     ("compute_forces_wrt_vertices_inner_product_wrt_states", "forces", "vertices"),
     ("compute_forces_wrt_vertices_inner_product_wrt_vertices", "forces", "vertices"),
 ]
+
+
+def _reference_function(path: Path, name: str):
+    """One top-level function of a reference script, compiled from its source unmodified (the
+    script itself parses command-line arguments and runs a workload when executed)."""
+    tree = ast.parse(path.read_text())
+    node = next(n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == name)
+    module = ast.Module(body=[node], type_ignores=[])
+    namespace = {"np": np, "gzip": gzip}
+    exec(compile(module, str(path), "exec"), namespace)
+    return namespace[name]
 
 
 def main(root: Path = DEFAULT_REFERENCE) -> None:
@@ -108,6 +126,17 @@ def main(root: Path = DEFAULT_REFERENCE) -> None:
     out["solve/rhs"] = b
     out["solve/fwd"] = s.solve_odes_wrt_states_fwd(b, shift=shift)
     out["solve/adj"] = s.solve_odes_wrt_states_adj(b, shift=shift)
+    # pressure coefficients, their tangent, and the reference's export of both
+    d = rnd(shapes["states"])
+    out["cp"] = s.compute_pressure_coefficients()
+    out["cp_wrt/direction"] = d
+    out["cp_wrt/result"] = s.apply_pressure_coefficients_wrt_states_fwd(d)
+    export = _reference_function(root / "examples" / "response" / "run.py",
+                                 "export_pressure_coefficients")
+    with tempfile.TemporaryDirectory() as tmp:
+        export(file_name=str(Path(tmp) / "cp.gz"), vertices=s.vertices,
+               pressure_coef=out["cp"], pressure_coef_wrt_aoa=out["cp_wrt/result"])
+        (HERE / "cp_export_8x9.txt").write_bytes(gzip.decompress((Path(tmp) / "cp.gz").read_bytes()))
     np.savez_compressed(HERE / "reference_8x9.npz", **out)
     print("wrote", sorted(p.name for p in HERE.iterdir()))
 

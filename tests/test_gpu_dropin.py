@@ -81,3 +81,12 @@ def test_check_array_errors_like_reference(solver):
         solver.apply_odes_wrt_states_fwd(np.asfortranarray(np.zeros(solver.states.shape)))
     with pytest.raises(RuntimeError, match="FORTRAN-contiguous"):
         solver.apply_odes_wrt_states_fwd(np.zeros(solver.states.shape, dtype=complex, order="C"))
+
+
+def test_pressure_coefficients_on_device(solver, reference_8x9):
+    cp = solver.compute_pressure_coefficients()
+    assert cp.flags.f_contiguous and cp.dtype == np.float64
+    assert rel_err(cp, reference_8x9["cp"]) <= 1e-12  # same bar as residual and forces
+    d = np.asfortranarray(reference_8x9["cp_wrt/direction"])
+    got = solver.apply_pressure_coefficients_wrt_states_fwd(d)
+    assert rel_err(got, reference_8x9["cp_wrt/result"]) <= 1e-12
