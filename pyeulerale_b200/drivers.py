@@ -30,17 +30,25 @@ class PtcResult:
         return len(self.norms)
 
 
-def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None) -> PtcResult:
+def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None, ser: float = 0.1,
+        safeguard: bool = False, growth: float = 10.0, max_retries: int = 8) -> PtcResult:
     """Pseudo-transient continuation with switched evolution relaxation
-    (examples/response/run.py:84-123): the time step is 0.1 / (relative infinity-norm of the
+    (examples/response/run.py:84-123): the time step is ``ser`` / (relative infinity-norm of the
     residual), each step solves (dR/dU - dt^-1 I) dU = -R on the device, and the loop stops at
-    rel <= rtol (or NaN), leaving the solver linearized at the final state."""
+    rel <= rtol (or NaN), leaving the solver linearized at the final state.
+
+    ``safeguard`` (off by default, which is the reference's loop) rejects a step whose residual
+    is not finite or grows by more than ``growth``, and retries it with a ten times larger shift
+    (a smaller pseudo time step), up to ``max_retries`` times; the larger shift then decays by
+    half per accepted step. This keeps the iterates of cases whose undamped steps overshoot
+    into negative densities finite; whether they then converge depends on the case."""
     res = PtcResult()
     solver.compute_odes()
     norm_free_stream = np.max(np.abs(solver.odes))
     if out is not None:
         print(f"\nPseudo-transient continuation:\n{'it':>6} {'residual':>15} "
               f"{'rel residual':>15}", file=out)
+    floor = 0.0
     for it in range(max_iter):
         solver.compute_odes()
         norm = np.max(np.abs(solver.odes))
@@ -53,9 +61,22 @@ def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None) -> PtcResult:
         solver.compute_forces()
         if rel <= rtol or np.isnan(rel):
             break
-        time_step = 1.e-1 * rel**-1.
-        update = solver.solve_odes_wrt_states_fwd(d_odes=-solver.odes, shift=time_step**-1.)
-        solver.states[:] += update
+        time_step = ser * rel**-1.
+        shift = time_step**-1.
+        if not safeguard:
+            update = solver.solve_odes_wrt_states_fwd(d_odes=-solver.odes, shift=shift)
+            solver.states[:] += update
+            continue
+        shift = max(shift, floor)
+        base, rhs = solver.states.copy(), -solver.odes
+        for _ in range(max_retries + 1):
+            solver.states[:] = base + solver.solve_odes_wrt_states_fwd(d_odes=rhs, shift=shift)
+            solver.compute_odes()
+            trial = np.max(np.abs(solver.odes)) / norm_free_stream
+            if np.isfinite(trial) and trial <= growth * rel:
+                break
+            shift *= 10.0
+        floor = shift / 2.0 if shift > rel / ser else floor / 2.0
     return res
 
 

@@ -147,3 +147,28 @@ def test_ringlu_many_matches_single(cuda, golden_grids, name):
             one.factor(g["_dev"]["J_u"], s)
             x1, _ = one.solve(rhs[k], adjoint=adjoint)
             assert rel_err(xs[k].cpu().numpy(), x1.cpu().numpy()) <= 1e-9, (name, k, adjoint)
+
+
+def test_ringlu_wide_rings(cuda, oracle):
+    """Rings of 4 N = 1024 unknowns (N = 256: the two-rows-per-thread panel path)."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200 import solver
+
+    X = G.naca_ogrid(9, 257, 0.12, 1.0, 20.0, 0.05)
+    rng = np.random.default_rng(16)
+    case = dict(X=X, V=np.zeros_like(X), U=G.perturbed_states(8, 256, 0.6, 2.0, 0.01, rng),
+                mach=0.6, aoa=2.0)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    b = crandn(rng, (4, 8, 256))
+    A = bsr_matrix(oracle, g["J_u"]).astype(complex)
+    for shift in (0.0, 0.05j):
+        lu = solver.RingLU(gpu.batch, tol=1e-10)
+        lu.factor(g["_dev"]["J_u"], shift)
+        for adjoint in (False, True):
+            x, rel = lu.solve(gpu.dev(b), adjoint=adjoint)
+            op = ((A - np.conj(shift) * sp.eye(A.shape[0])).T if adjoint
+                  else (A - shift * sp.eye(A.shape[0]))).tocsc()
+            ref = spla.spsolve(op, b.ravel(order="F"))
+            got = gpu.host(x, (4, 8, 256), complex_=True).ravel(order="F")
+            assert rel <= 1e-10 and rel_err(got, ref) <= 1e-8, (shift, adjoint, rel)
