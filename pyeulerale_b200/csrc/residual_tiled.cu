@@ -166,57 +166,12 @@ __device__ __forceinline__ void jst_pair(const St& ll, const St& l, const St& r,
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
-k_residual_tiled(Table t, const double* X, const double* V, const double* U, double* R) {
-  extern __shared__ __align__(16) unsigned char tile_smem[];
-  TileSmem& S = *reinterpret_cast<TileSmem*>(tile_smem);
-  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;
+// Phases 2-4 of a tile whose states (with derived quantities) and vertices are staged in S:
+// sensors, faces, and the residual of the tile's cells. Every thread of the CTA calls it.
+__device__ __forceinline__ void tile_compute(TileSmem& S, const Instance& in, int m0, int n0,
+                                             double* R) {
   const int M = in.M, N = in.N;
-  const int tiles_m = (M + kTM - 1) / kTM;
-  const int tiles = tiles_m * ((N + kTN - 1) / kTN);
-  if ((int)blockIdx.x >= tiles) return;
-  const int m0 = (blockIdx.x % tiles_m) * kTM, n0 = (blockIdx.x / tiles_m) * kTN;
-  const double* Ui = U + 4 * in.cell_offset;
-  const double* Xi = X + 2 * in.vert_offset;
-  const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
   const int tid = threadIdx.x;
-
-  // 1. stage states (cross-shaped halo) and derived quantities
-  for (int e = tid; e < kStaged; e += kThreads) {
-    const int r = e % kSR - 2, c = e / kSR - 2;
-    const bool corner = (r < 0 || r >= kTM) && (c < 0 || c >= kTN);
-    const int m = m0 + r;
-    if (corner || m < 0 || m >= M) {
-      S.rho[e] = 1.0; S.j1[e] = 0.0; S.j2[e] = 0.0; S.e[e] = 1.0;
-      S.p[e] = 1.0; S.ir[e] = 1.0; S.cs[e] = 1.0;
-      continue;
-    }
-    const int n = wrap(n0 + c, N);
-    const double* q = Ui + 4 * (m + (int64_t)M * n);
-    const double2 a = __ldg(reinterpret_cast<const double2*>(q));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(q + 2));
-    const St s = derive(a.x, a.y, b.x, b.y);
-    S.rho[e] = s.rho; S.j1[e] = s.j1; S.j2[e] = s.j2; S.e[e] = s.e;
-    S.p[e] = s.p; S.ir[e] = s.ir; S.cs[e] = s.cs;
-  }
-  for (int e = tid; e < kVerts; e += kThreads) {
-    const int r = e % kVR, c = e / kVR;
-    const int m = min(m0 + r, M), n = min(n0 + c, N);
-    const int64_t v = m + (int64_t)(M + 1) * n;
-    const double2 xv = __ldg(reinterpret_cast<const double2*>(Xi + 2 * v));
-    S.x[e] = xv.x;
-    S.z[e] = xv.y;
-    if (Vi) {
-      const double2 vv = __ldg(reinterpret_cast<const double2*>(Vi + 2 * v));
-      S.vx[e] = vv.x;
-      S.vz[e] = vv.y;
-    } else {
-      S.vx[e] = 0.0;
-      S.vz[e] = 0.0;
-    }
-  }
-  __syncthreads();
-
   // 2. sensors centred on each needed state
   for (int e = tid; e < kTM * (kTN + 2); e += kThreads) {
     const int r = e % kTM, c = e / kTM - 1;
@@ -343,6 +298,60 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
   double* out = R + 4 * (in.cell_offset + m + (int64_t)M * n);
   reinterpret_cast<double2*>(out)[0] = make_double2(res[0], res[1]);
   reinterpret_cast<double2*>(out)[1] = make_double2(res[2], res[3]);
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+k_residual_tiled(Table t, const double* X, const double* V, const double* U, double* R) {
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  TileSmem& S = *reinterpret_cast<TileSmem*>(tile_smem);
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;
+  const int M = in.M, N = in.N;
+  const int tiles_m = (M + kTM - 1) / kTM;
+  const int tiles = tiles_m * ((N + kTN - 1) / kTN);
+  if ((int)blockIdx.x >= tiles) return;
+  const int m0 = (blockIdx.x % tiles_m) * kTM, n0 = (blockIdx.x / tiles_m) * kTN;
+  const double* Ui = U + 4 * in.cell_offset;
+  const double* Xi = X + 2 * in.vert_offset;
+  const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
+  const int tid = threadIdx.x;
+
+  // 1. stage states (cross-shaped halo) and derived quantities
+  for (int e = tid; e < kStaged; e += kThreads) {
+    const int r = e % kSR - 2, c = e / kSR - 2;
+    const bool corner = (r < 0 || r >= kTM) && (c < 0 || c >= kTN);
+    const int m = m0 + r;
+    if (corner || m < 0 || m >= M) {
+      S.rho[e] = 1.0; S.j1[e] = 0.0; S.j2[e] = 0.0; S.e[e] = 1.0;
+      S.p[e] = 1.0; S.ir[e] = 1.0; S.cs[e] = 1.0;
+      continue;
+    }
+    const int n = wrap(n0 + c, N);
+    const double* q = Ui + 4 * (m + (int64_t)M * n);
+    const double2 a = __ldg(reinterpret_cast<const double2*>(q));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(q + 2));
+    const St s = derive(a.x, a.y, b.x, b.y);
+    S.rho[e] = s.rho; S.j1[e] = s.j1; S.j2[e] = s.j2; S.e[e] = s.e;
+    S.p[e] = s.p; S.ir[e] = s.ir; S.cs[e] = s.cs;
+  }
+  for (int e = tid; e < kVerts; e += kThreads) {
+    const int r = e % kVR, c = e / kVR;
+    const int m = min(m0 + r, M), n = min(n0 + c, N);
+    const int64_t v = m + (int64_t)(M + 1) * n;
+    const double2 xv = __ldg(reinterpret_cast<const double2*>(Xi + 2 * v));
+    S.x[e] = xv.x;
+    S.z[e] = xv.y;
+    if (Vi) {
+      const double2 vv = __ldg(reinterpret_cast<const double2*>(Vi + 2 * v));
+      S.vx[e] = vv.x;
+      S.vz[e] = vv.y;
+    } else {
+      S.vx[e] = 0.0;
+      S.vz[e] = 0.0;
+    }
+  }
+  __syncthreads();
+
+  tile_compute(S, in, m0, n0, R);
 }
 
 int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
