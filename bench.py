@@ -60,7 +60,7 @@ def parse_args():
                    help="frequency-response shifts timed through the batched driver")
     p.add_argument("--parts", default="residual,vjp,resolvent",
                    help="comma-separated parts to run besides the residual (vjp, resolvent)")
-    p.add_argument("--shift-group", type=int, default=16,
+    p.add_argument("--shift-group", type=int, default=32,
                    help="shifts factored concurrently (one workspace of ~2.7 GB each)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline budget")
     p.add_argument("--no-cpu-baseline", action="store_true")

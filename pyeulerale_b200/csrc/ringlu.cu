@@ -54,24 +54,34 @@ int validate(const eb_batch* b);
 
 namespace rl {
 
+// A cuBLAS handle per concurrent lane (its workspace must not be shared by work that overlaps
+// on the device) and, for the lanes after the first, a stream of this library.
 struct Handle {
   int device = -1;
   cublasHandle_t blas = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
 };
 
-thread_local Handle g_handle;
+constexpr int kLanes = 2;
+thread_local Handle g_handle[kLanes];
 
-int blas_handle(cudaStream_t st, cublasHandle_t& out) {
+int blas_handle(cudaStream_t st, cublasHandle_t& out, int lane = 0) {
   int dev = 0;
   cudaGetDevice(&dev);
-  Handle& h = g_handle;
+  Handle& h = g_handle[lane];
   if (h.device != dev) {
     if (h.blas) cublasDestroy(h.blas);
     h.blas = nullptr;
+    h.stream = nullptr;  // streams and events of another device are left to that device
+    h.done = nullptr;
     if (cublasCreate(&h.blas) != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "cublasCreate failed");
+    if (lane > 0 && (cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) != cudaSuccess))
+      return check_launch("ringlu lane stream");
     h.device = dev;
   }
-  cublasSetStream(h.blas, st);
+  cublasSetStream(h.blas, lane > 0 ? h.stream : st);
   out = h.blas;
   return EB_OK;
 }
@@ -760,8 +770,31 @@ int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, cons
         reinterpret_cast<cuDoubleComplex*>(w + L.off_C1), reinterpret_cast<cuDoubleComplex*>(w + L.off_C2));
   }
   if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
-  for (int m = 0; m < M; ++m)
-    if ((rc = factor_ring(g, h, m, st)) != EB_OK) return rc;
+  if (n_shifts == 1) {
+    for (int m = 0; m < M; ++m)
+      if ((rc = factor_ring(g, h, m, st)) != EB_OK) return rc;
+  } else {
+    // Two halves of the shifts on two streams, ring by ring: one half's latency-bound
+    // Gauss-Jordan panels overlap the other half's GEMMs on the rest of the GPU.
+    cublasHandle_t h2 = nullptr;
+    if ((rc = blas_handle(st, h2, 1)) != EB_OK) return rc;
+    const Handle& lane = g_handle[1];
+    const int s1 = (n_shifts + 1) / 2;
+    const Group g1{L, g.base, g.stride, s1};
+    const Group g2{L, g.base + (int64_t)s1 * g.stride, g.stride, n_shifts - s1};
+    cudaEvent_t start = nullptr;
+    if (cudaEventCreateWithFlags(&start, cudaEventDisableTiming) != cudaSuccess)
+      return check_launch("ringlu event");
+    cudaEventRecord(start, st);
+    cudaStreamWaitEvent(lane.stream, start, 0);
+    cudaEventDestroy(start);
+    for (int m = 0; m < M; ++m) {
+      if ((rc = factor_ring(g1, h, m, st)) != EB_OK) return rc;
+      if ((rc = factor_ring(g2, h2, m, lane.stream)) != EB_OK) return rc;
+    }
+    cudaEventRecord(lane.done, lane.stream);
+    cudaStreamWaitEvent(st, lane.done, 0);
+  }
   if ((rc = check_launch("ringlu factor")) != EB_OK) return rc;
   std::vector<int> info(n_shifts);
   for (int s = 0; s < n_shifts; ++s)
