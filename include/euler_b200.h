@@ -234,16 +234,20 @@ int64_t eb_ringlu_workspace_bytes(int M, int N);
 int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double shift_im,
                      void* workspace, int64_t workspace_bytes, void* stream);
 
-/* eb_ringlu_factor for n_shifts shifts of the same J at once: shifts[2 s], shifts[2 s + 1] is
- * shift s (real, imaginary; host array), its workspace starts at workspace + s * workspace_stride
- * (stride >= eb_ringlu_workspace_bytes, a multiple of 256; workspace 256-byte aligned). Each
- * step of the elimination runs as one launch over all shifts, so a frequency sweep factors its
- * shifts together instead of one after another (the reference factors J - s I with SuperLU once
- * per reduced frequency, examples/response/run.py:138-144). Each shift's workspace then serves
+/* eb_ringlu_factor for n_shifts systems J[s] - shift_s I at once, all of the grid size of the
+ * single instance in `b`: J[s] (host array of device pointers) is system s's d(odes)/d(states)
+ * (the same pointer for every s for a frequency sweep, different ones for several instances of
+ * equal size), shifts[2 s], shifts[2 s + 1] its shift (real, imaginary; host array), and its
+ * workspace starts at workspace + s * workspace_stride (stride >= eb_ringlu_workspace_bytes, a
+ * multiple of 256; workspace 256-byte aligned). Each step of the elimination runs as one launch
+ * over all systems, so a frequency sweep factors its shifts together instead of one after
+ * another (the reference factors J - s I with SuperLU once per reduced frequency,
+ * examples/response/run.py:138-144, and once per PTC step, :117-120). Each workspace then serves
  * eb_ringlu_solve / eb_ringlu_solve_many. Synchronises `stream`; EB_ERR_NAN if a ring block of
- * any shift is singular. */
-int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
-                          void* workspace, int64_t workspace_stride, void* stream);
+ * any system is singular. */
+int eb_ringlu_factor_many(const eb_batch* b, const double* const* J, int n_shifts,
+                          const double* shifts, void* workspace, int64_t workspace_stride,
+                          void* stream);
 
 /* x = A^-1 rhs (adjoint = 1: x = A^-H rhs) with the factors of eb_ringlu_factor for the same
  * J and shift, then iterative refinement x += A^-1 (rhs - A x) until ||rhs - A x|| / ||rhs||
@@ -256,14 +260,14 @@ int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double 
                     double* rel_residual, void* stream);
 
 /* eb_ringlu_solve for the n_shifts factorisations of one eb_ringlu_factor_many call: system s
- * uses shift s, the workspace at workspace + s * workspace_stride, rhs[s] and x[s] (host arrays
- * of device pointers). The triangular sweeps of all systems run as batched launches; refinement
- * passes continue until every system reaches tol. rel_residuals (host, optional, n_shifts
- * entries) receives the final relative residuals. Synchronises `stream`. */
-int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
-                         int adjoint, const void* workspace, int64_t workspace_stride,
-                         const double* const* rhs, double* const* x, double tol, int max_refine,
-                         double* rel_residuals, void* stream);
+ * uses J[s], shift s, the workspace at workspace + s * workspace_stride, rhs[s] and x[s] (host
+ * arrays of device pointers). The triangular sweeps of all systems run as batched launches;
+ * refinement passes continue until every system reaches tol. rel_residuals (host, optional,
+ * n_shifts entries) receives the final relative residuals. Synchronises `stream`. */
+int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts,
+                         const double* shifts, int adjoint, const void* workspace,
+                         int64_t workspace_stride, const double* const* rhs, double* const* x,
+                         double tol, int max_refine, double* rel_residuals, void* stream);
 
 /* ---- pressure coefficients --------------------------------------------------------------- */
 /* cp (real, one per cell, packed like the cells) of the states U: ((gamma-1)(E - |j|^2/2/rho) -

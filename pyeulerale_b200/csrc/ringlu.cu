@@ -749,12 +749,15 @@ int64_t eb_ringlu_workspace_bytes(int M, int N) {
   return (int64_t)plan(M, N).total;
 }
 
-int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
-                          void* workspace, int64_t workspace_stride, void* stream) {
+int eb_ringlu_factor_many(const eb_batch* b, const double* const* J, int n_shifts,
+                          const double* shifts, void* workspace, int64_t workspace_stride,
+                          void* stream) {
   Layout L;
   int rc = check_group(b, n_shifts, workspace, workspace_stride, L);
   if (rc != EB_OK) return rc;
   if (!J || !shifts) return fail(EB_ERR_ARG, "ringlu: null argument");
+  for (int s = 0; s < n_shifts; ++s)
+    if (!J[s]) return fail(EB_ERR_ARG, "ringlu: null Jacobian");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cublasHandle_t h = nullptr;
   if ((rc = blas_handle(st, h)) != EB_OK) return rc;
@@ -765,7 +768,7 @@ int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, cons
     cudaMemsetAsync(w, 0, L.off_T, st);  // the five block arrays
     cudaMemsetAsync(w + L.off_info, 0, sizeof(int) * 4, st);
     k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
-        M, N, J, shifts[2 * s], shifts[2 * s + 1], reinterpret_cast<cuDoubleComplex*>(w + L.off_D),
+        M, N, J[s], shifts[2 * s], shifts[2 * s + 1], reinterpret_cast<cuDoubleComplex*>(w + L.off_D),
         reinterpret_cast<cuDoubleComplex*>(w + L.off_L1), reinterpret_cast<cuDoubleComplex*>(w + L.off_L2),
         reinterpret_cast<cuDoubleComplex*>(w + L.off_C1), reinterpret_cast<cuDoubleComplex*>(w + L.off_C2));
   }
@@ -810,19 +813,20 @@ int eb_ringlu_factor_many(const eb_batch* b, const double* J, int n_shifts, cons
 int eb_ringlu_factor(const eb_batch* b, const double* J, double shift_re, double shift_im,
                      void* workspace, int64_t workspace_bytes, void* stream) {
   const double shift[2] = {shift_re, shift_im};
-  return eb_ringlu_factor_many(b, J, 1, shift, workspace, workspace_bytes & ~(int64_t)255, stream);
+  const double* js[1] = {J};
+  return eb_ringlu_factor_many(b, js, 1, shift, workspace, workspace_bytes & ~(int64_t)255, stream);
 }
 
-int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const double* shifts,
-                         int adjoint, const void* workspace, int64_t workspace_stride,
-                         const double* const* rhs, double* const* x, double tol, int max_refine,
-                         double* rel_residuals, void* stream) {
+int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts,
+                         const double* shifts, int adjoint, const void* workspace,
+                         int64_t workspace_stride, const double* const* rhs, double* const* x,
+                         double tol, int max_refine, double* rel_residuals, void* stream) {
   Layout L;
   int rc = check_group(b, n_shifts, workspace, workspace_stride, L);
   if (rc != EB_OK) return rc;
   if (!J || !shifts || !rhs || !x) return fail(EB_ERR_ARG, "ringlu: null argument");
   for (int s = 0; s < n_shifts; ++s)
-    if (!rhs[s] || !x[s]) return fail(EB_ERR_ARG, "ringlu: null argument");
+    if (!J[s] || !rhs[s] || !x[s]) return fail(EB_ERR_ARG, "ringlu: null argument");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cublasHandle_t h = nullptr;
   if ((rc = blas_handle(st, h)) != EB_OK) return rc;
@@ -843,7 +847,7 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* J, int n_shifts, const
       k_from_rings<<<gc, 128, 0, st>>>(M, N, reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_x), x[s],
                                        it == 0 ? 0 : 1);
       cudaMemsetAsync(a, 0, 2 * sizeof(double), st);
-      k_residual_op<<<gc, 128, 0, st>>>(M, N, J, shifts[2 * s], shifts[2 * s + 1], adjoint, x[s], rhs[s],
+      k_residual_op<<<gc, 128, 0, st>>>(M, N, J[s], shifts[2 * s], shifts[2 * s + 1], adjoint, x[s], rhs[s],
                                         reinterpret_cast<double*>(ws(s) + L.off_r), a);
       if (cudaMemcpyAsync(&acc[2 * s], a, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return check_launch("ringlu residual");
@@ -874,9 +878,10 @@ int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double 
                     const double* rhs, double* x, double tol, int max_refine,
                     double* rel_residual, void* stream) {
   const double shift[2] = {shift_re, shift_im};
+  const double* js[1] = {J};
   const double* in[1] = {rhs};
   double* out[1] = {x};
-  return eb_ringlu_solve_many(b, J, 1, shift, adjoint, workspace, workspace_bytes & ~(int64_t)255,
+  return eb_ringlu_solve_many(b, js, 1, shift, adjoint, workspace, workspace_bytes & ~(int64_t)255,
                               in, out, tol, max_refine, rel_residual, stream);
 }
 

@@ -80,6 +80,168 @@ def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None, ser: float = 
     return res
 
 
+@dataclass
+class BatchedPtcResult:
+    """Per-instance histories of ``ptc_batched`` and the packed device states."""
+
+    rel_norms: list = field(default_factory=list)   # one list of relative norms per instance
+    states: object = None                             # packed float64 device tensor
+    vertices: object = None
+    velocities: object = None
+
+    @property
+    def iterations(self) -> list[int]:
+        return [len(h) for h in self.rel_norms]
+
+
+def _shape_groups(instances) -> dict:
+    groups: dict = {}
+    for i, sp in enumerate(instances.specs):
+        groups.setdefault((sp.M, sp.N), []).append(i)
+    return groups
+
+
+def _batched_solves(instances, J, shifts_of, rhs_of, out_of, adjoint: bool, workspace,
+                    tol: float) -> None:
+    """Solves (J_i - s_i I) x_i = b_i (or the adjoint) for the instances in ``shifts_of``, the
+    instances of one grid size together per factorisation call, as many per call as the
+    ``workspace`` (one uint8 device tensor) holds."""
+    from . import _lib
+    from .solver import RingLUMany, ringlu_workspace_bytes
+
+    groups = _shape_groups(instances)
+    for (M, N), members in groups.items():
+        todo = [i for i in members if i in shifts_of]
+        if not todo:
+            continue
+        stride = (ringlu_workspace_bytes(M, N) + 255) // 256 * 256
+        cap = max(1, min(len(todo), workspace.numel() // stride))
+        if workspace.numel() < stride:
+            raise ValueError(f"workspace of {workspace.numel()} bytes is below one {M}x{N} system")
+        batch = _lib.single_batch(_lib.make_instance(M, N, 0.5, 0.0))
+        lu = RingLUMany(batch, capacity=cap, tol=tol, workspace=workspace)
+        for c0 in range(0, len(todo), cap):
+            chunk = todo[c0:c0 + cap]
+            nc = M * N
+            offs = [instances.cell_offsets[i] for i in chunk]
+            lu.factor([J[144 * o:144 * (o + nc)] for o in offs], [shifts_of[i] for i in chunk])
+            xs, _ = lu.solve([rhs_of(i) for i in chunk], adjoint=adjoint)
+            for i, x in zip(chunk, xs):
+                out_of(i, x)
+
+
+def ptc_batched(instances, states=None, rtol: float = 1e-10, max_iter: int = 100,
+                ser: float = 0.1, workspace_bytes: int = 64 << 30, tol: float = 1e-10,
+                velocities=None) -> BatchedPtcResult:
+    """The PTC/SER loop of ``ptc`` for every instance of an ``InstanceSet`` at once.
+
+    Each iteration evaluates the residuals and d(odes)/d(states) of all instances in one launch
+    each, takes every unconverged instance's relative infinity norm (one segmented reduction),
+    and solves each instance's (dR/dU - dt^-1 I) dU = -R with the ring-block LU, the instances
+    of one grid size factored together (``eb_ringlu_factor_many`` with one Jacobian per
+    system) within ``workspace_bytes`` of factor storage. Instances stop individually at
+    rel <= rtol (or NaN). ``states`` (packed, host or device) defaults to the free stream.
+    """
+    import torch
+
+    inst = instances
+    f64 = dict(dtype=torch.float64, device="cuda")
+    dX = torch.from_numpy(inst.pack_vertices()).cuda()
+    dV = (torch.zeros_like(dX) if velocities is None
+          else torch.as_tensor(velocities, dtype=torch.float64).cuda())
+    dU = torch.empty(4 * inst.n_cells, **f64)
+    if states is None:
+        inst.call("eb_set_free_stream_state", dU)
+    else:
+        dU.copy_(torch.as_tensor(states, dtype=torch.float64))
+    R = torch.empty(4 * inst.n_cells, **f64)
+    J = torch.empty(144 * inst.n_cells, **f64)
+    lengths = torch.tensor([4 * sp.M * sp.N for sp in inst.specs], device="cuda")
+    seg_max = lambda v: torch.segment_reduce(v.abs(), "max", lengths=lengths)  # noqa: E731
+    workspace = torch.empty(int(workspace_bytes) // 256 * 256, dtype=torch.uint8, device="cuda")
+    inst.call("eb_compute_odes", dX, dV, dU, R)
+    norm0 = seg_max(R).cpu().numpy()
+    res = BatchedPtcResult(rel_norms=[[] for _ in inst.specs])
+    active = set(range(len(inst)))
+    for _ in range(max_iter):
+        inst.call("eb_compute_odes", dX, dV, dU, R)
+        rel = seg_max(R).cpu().numpy() / norm0
+        for i in sorted(active):
+            res.rel_norms[i].append(float(rel[i]))
+        active = {i for i in active if not (rel[i] <= rtol or np.isnan(rel[i]))}
+        if not active:
+            break
+        inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J)
+        shifts = {i: (ser * rel[i]**-1.)**-1. for i in active}
+
+        def rhs_of(i):
+            o, n = inst.cell_offsets[i], 4 * inst.specs[i].M * inst.specs[i].N
+            b = torch.zeros(2 * n, **f64)
+            b[0::2] = -R[4 * o:4 * o + n]
+            return b
+
+        def update(i, x):
+            o, n = inst.cell_offsets[i], 4 * inst.specs[i].M * inst.specs[i].N
+            dU[4 * o:4 * o + n] += x[0::2]
+
+        _batched_solves(inst, J, shifts, rhs_of, update, False, workspace, tol)
+    res.states, res.vertices, res.velocities = dU, dX, dV
+    return res
+
+
+def adjoint_lift_gradients_batched(instances, result: BatchedPtcResult,
+                                   workspace_bytes: int = 64 << 30,
+                                   tol: float = 1e-10) -> list[np.ndarray]:
+    """``adjoint_lift_gradient`` of every instance at the states of ``result``: the forces
+    Jacobians, d(odes)/d(states) and d(odes)/d(vertices) of all instances in one launch each,
+    the adjoint solves at shift 0 with the instances of one grid size factored together, and
+    the reverse products over all instances. Returns one (2, M+1, N+1) array per instance."""
+    import torch
+
+    inst = instances
+    f64 = dict(dtype=torch.float64, device="cuda")
+    dX, dV, dU = result.vertices, result.velocities, result.states
+    nc, nv, nw = inst.n_cells, inst.n_verts, inst.n_wall
+    g = torch.zeros(4 * nw, **f64)  # complex (2, N) per instance: d c_l / d F_z = 1 / (q c)
+    for sp, w in zip(inst.specs, inst.wall_offsets):
+        q = sp.mach**2 * HEAT_RATIO / 2
+        g[4 * w + 2:4 * (w + sp.N):4] = 1.0 / (q * sp.chord)
+    JFu, JFx = torch.empty(8 * nw, **f64), torch.empty(8 * nw, **f64)
+    inst.call("eb_compute_forces_wrt_states", dX, dU, JFu)
+    inst.call("eb_compute_forces_wrt_vertices", dX, dU, JFx)
+    gU = torch.empty(8 * nc, **f64)
+    inst.call("eb_apply_forces_wrt_states_rev", JFu, g, gU)
+    J = torch.empty(144 * nc, **f64)
+    inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J)
+    lam = torch.empty(8 * nc, **f64)
+
+    def rhs_of(i):
+        o, n = inst.cell_offsets[i], 8 * inst.specs[i].M * inst.specs[i].N
+        return gU[8 * o:8 * o + n]
+
+    def store(i, x):
+        o, n = inst.cell_offsets[i], 8 * inst.specs[i].M * inst.specs[i].N
+        lam[8 * o:8 * o + n] = x
+
+    workspace = torch.empty(int(workspace_bytes) // 256 * 256, dtype=torch.uint8, device="cuda")
+    _batched_solves(inst, J, {i: 0.0 for i in range(len(inst))}, rhs_of, store, True, workspace,
+                    tol)
+    del workspace, J
+    Jx = torch.empty(32 * nc, **f64)
+    inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, Jx)
+    gX_r, gX_f = torch.empty(4 * nv, **f64), torch.empty(4 * nv, **f64)
+    inst.call("eb_apply_odes_wrt_vertices_rev", Jx, lam, gX_r)
+    inst.call("eb_apply_forces_wrt_vertices_rev", JFx, g, gX_f)
+    grad = (gX_f - gX_r)[0::2].cpu().numpy()
+    out, o = [], 0
+    for sp in inst.specs:
+        n = 2 * (sp.M + 1) * (sp.N + 1)
+        out.append(np.asfortranarray(np.reshape(grad[o:o + n], (2, sp.M + 1, sp.N + 1),
+                                                order="F")))
+        o += n
+    return out
+
+
 def pitch_vertices(solver, axis_location: float) -> np.ndarray:
     """dX/dalpha of a rigid pitch about (axis_location, 0), per radian."""
     v = np.empty_like(solver.vertices, dtype=complex)

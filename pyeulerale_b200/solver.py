@@ -201,7 +201,7 @@ class RingLUMany:
     """
 
     def __init__(self, batch: _lib.Batch, capacity: int, tol: float = 1e-10,
-                 max_refine: int = 4) -> None:
+                 max_refine: int = 4, workspace=None) -> None:
         import torch
 
         self._torch = torch
@@ -212,7 +212,11 @@ class RingLUMany:
             raise ValueError("ring LU needs a single instance with M >= 4, N >= 5")
         self.stride = (int(need) + 255) // 256 * 256
         self.capacity = int(capacity)
-        self.workspace = torch.empty(self.stride * self.capacity, dtype=torch.uint8, device="cuda")
+        if workspace is None:
+            workspace = torch.empty(self.stride * self.capacity, dtype=torch.uint8, device="cuda")
+        elif workspace.numel() < self.stride * self.capacity or workspace.data_ptr() % 256:
+            raise ValueError("workspace too small or not 256-byte aligned")
+        self.workspace = workspace
         self.J = None
         self.shifts: list[complex] = []
 
@@ -223,20 +227,26 @@ class RingLUMany:
         return sh
 
     def factor(self, J, shifts) -> None:
+        """Factors J - s I for every shift s; ``J`` is one device Jacobian for all shifts or a
+        sequence of one per shift (instances of the same grid size)."""
         shifts = [complex(v) for v in np.atleast_1d(shifts)]
         n = len(shifts)
         if not 1 <= n <= self.capacity:
             raise ValueError(f"{n} shifts for {self.capacity} workspaces")
+        Js = list(J) if isinstance(J, (list, tuple)) else [J] * n
+        if len(Js) != n:
+            raise ValueError(f"{len(Js)} Jacobians for {n} shifts")
         self.J, self.shifts = None, shifts
         sh = self._shift_array()
-        rc = self._lib.eb_ringlu_factor_many(ctypes.byref(self.batch), J.data_ptr(), n,
+        jp = (ctypes.c_void_p * n)(*[j.data_ptr() for j in Js])
+        rc = self._lib.eb_ringlu_factor_many(ctypes.byref(self.batch), jp, n,
                                              sh.ctypes.data, self.workspace.data_ptr(),
                                              self.stride,
                                              self._torch.cuda.current_stream().cuda_stream)
         if rc != _lib.EB_OK:
             raise _lib.EulerB200Error("eb_ringlu_factor_many", rc,
                                       self._lib.eb_last_error().decode())
-        self.J = J
+        self.J = Js
 
     def solve(self, rhs, adjoint: bool = False, out=None):
         """Solves system ``s`` for ``rhs[s]`` (a sequence of, or a stacked, device tensor);
@@ -253,7 +263,8 @@ class RingLUMany:
         rp = (ctypes.c_void_p * n)(*[rhs[k].data_ptr() for k in range(n)])
         xp = (ctypes.c_void_p * n)(*[x[k].data_ptr() for k in range(n)])
         rel = (ctypes.c_double * n)()
-        rc = self._lib.eb_ringlu_solve_many(ctypes.byref(self.batch), self.J.data_ptr(), n,
+        jp = (ctypes.c_void_p * n)(*[j.data_ptr() for j in self.J])
+        rc = self._lib.eb_ringlu_solve_many(ctypes.byref(self.batch), jp, n,
                                             sh.ctypes.data, 1 if adjoint else 0,
                                             self.workspace.data_ptr(), self.stride, rp, xp,
                                             self.tol, self.max_refine, rel,

@@ -52,3 +52,32 @@ def test_adjoint_lift_gradient_dot_product(solver):
                       + solver.apply_forces_wrt_states_fwd(d_states=dU)).real
         adj = float(np.sum(grad * dX.real))
         assert abs(adj - fwd) <= 1e-9 * abs(fwd), (adj, fwd)
+
+
+def test_ptc_and_adjoint_batched_match_single(cuda):
+    """Three uneven instances (two of one grid size, factored together): the batched PTC
+    histories, steady states and adjoint lift gradients equal the drop-in's per instance."""
+    from pyeulerale_b200 import SpatialDiscretization, drivers
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    specs = [InstanceSpec(G.naca_ogrid(33, 33, 0.12, 1.0, 20.0, 0.01), 0.5, 1.25, 1.0, (0.25, 0.0)),
+             InstanceSpec(G.naca_ogrid(21, 25, 0.08, 1.0, 15.0, 0.02), 0.4, -1.0, 1.0, (0.25, 0.0)),
+             InstanceSpec(G.naca_ogrid(33, 33, 0.10, 1.0, 20.0, 0.01), 0.45, 2.0, 1.0, (0.25, 0.0))]
+    inst = InstanceSet(specs)
+    res = drivers.ptc_batched(inst, rtol=1e-10, max_iter=40, workspace_bytes=1 << 30)
+    grads = drivers.adjoint_lift_gradients_batched(inst, res, workspace_bytes=1 << 30)
+    states = inst.unpack_cells(res.states.cpu().numpy())
+    for k, sp in enumerate(specs):
+        s = SpatialDiscretization(sp.vertices, mach_number=sp.mach, angle_of_attack=sp.aoa_deg,
+                                  coefficient_length=sp.chord, coefficient_center=sp.center)
+        hist = drivers.ptc(s, rtol=1e-10, max_iter=40)
+        assert res.rel_norms[k][-1] <= 1e-10 and hist.rel_norms[-1] <= 1e-10
+        assert abs(len(res.rel_norms[k]) - hist.iterations) <= 1, (k, res.rel_norms[k],
+                                                                    hist.rel_norms)
+        early = [i for i, r in enumerate(hist.rel_norms) if r > 1e-7 and i < len(res.rel_norms[k])]
+        assert np.allclose([res.rel_norms[k][i] for i in early],
+                           [hist.rel_norms[i] for i in early], rtol=1e-6), k
+        assert rel_err(states[k], s.states.real) <= 1e-9, k
+        ref = drivers.adjoint_lift_gradient(s)
+        assert rel_err(grads[k], ref) <= 1e-8, (k, rel_err(grads[k], ref))
