@@ -58,8 +58,17 @@ def parse_args():
                    help="frequency-response shifts timed one at a time (plain path)")
     p.add_argument("--batched-shifts", type=int, default=64,
                    help="frequency-response shifts timed through the batched driver")
-    p.add_argument("--parts", default="residual,vjp,resolvent",
-                   help="comma-separated parts to run besides the residual (vjp, resolvent)")
+    p.add_argument("--parts", default="residual,vjp,resolvent,uneven",
+                   help="comma-separated parts to run besides the residual "
+                        "(vjp, resolvent, uneven)")
+    p.add_argument("--uneven-instances", type=int, default=48)
+    p.add_argument("--uneven-sizes", default="65,129",
+                   help="grid point counts (n x n O-grids) the uneven instances draw from")
+    p.add_argument("--uneven-iter", type=int, default=30, help="PTC iteration cap")
+    p.add_argument("--uneven-plain", type=int, default=3,
+                   help="instances timed one at a time for the comparison")
+    p.add_argument("--workspace-gb", type=float, default=80.0,
+                   help="device memory for batched factorisations")
     p.add_argument("--shift-group", type=int, default=32,
                    help="shifts factored concurrently (one workspace of ~2.7 GB each)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline budget")
@@ -390,6 +399,60 @@ def run_b200(args) -> None:
                          "ZGEMM), refined to 1e-10 relative residual"}
         del sd
 
+    # uneven instances: steady states (PTC) and adjoint lift gradients of many grids of
+    # different sizes, thicknesses, Mach numbers and angles, batched (one launch per kernel over
+    # all instances, equal-size instances factored together) against one instance at a time
+    uneven = None
+    if "uneven" in parts:
+        from pyeulerale_b200 import SpatialDiscretization, drivers
+        from pyeulerale_b200 import grid as G
+
+        urng = np.random.default_rng(4 + rank)
+        sizes = [int(v) for v in args.uneven_sizes.split(",")]
+        uspecs = []
+        for _ in range(args.uneven_instances):
+            n_pts = int(urng.choice(sizes))
+            tt = int(urng.choice([4, 6, 8, 10, 12]))
+            Xg = G.naca_ogrid(n_pts, n_pts, thickness=tt / 100, chord=1.0, far_radius=20.0,
+                              first_spacing=0.01)
+            uspecs.append(InstanceSpec(Xg, float(urng.uniform(0.3, 0.6)),
+                                       float(urng.uniform(-2.0, 3.0)), 1.0, (0.25, 0.0)))
+        uinst = InstanceSet(uspecs)
+        barrier()
+        t0 = time.perf_counter()
+        ures = drivers.ptc_batched(uinst, rtol=1e-10, max_iter=args.uneven_iter,
+                                   workspace_bytes=int(args.workspace_gb * (1 << 30)))
+        drivers.adjoint_lift_gradients_batched(uinst, ures,
+                                               workspace_bytes=int(args.workspace_gb * (1 << 30)))
+        barrier()
+        t_ub = max_over_ranks(time.perf_counter() - t0)
+        n_plain = min(args.uneven_plain, len(uspecs))
+        t0 = time.perf_counter()
+        for sp in uspecs[:n_plain]:
+            sd = SpatialDiscretization(sp.vertices, mach_number=sp.mach,
+                                       angle_of_attack=sp.aoa_deg, coefficient_length=sp.chord,
+                                       coefficient_center=sp.center)
+            hist = drivers.ptc(sd, rtol=1e-10, max_iter=args.uneven_iter)
+            if np.isfinite(hist.rel_norms[-1]):
+                try:
+                    drivers.adjoint_lift_gradient(sd)
+                except _lib.EulerB200Error:
+                    pass  # a singular adjoint system, as in the batched path
+            del sd
+        barrier()
+        t_up = max_over_ranks(time.perf_counter() - t0)
+        conv = sum(1 for h in ures.rel_norms if h and h[-1] <= 1e-10)
+        uneven = {"value": world * len(uspecs) / t_ub,
+                  "unit": "instances/s (PTC to 1e-10 + adjoint lift gradient)",
+                  "workload": f"{len(uspecs)} NACA-00tt O-grids of sizes {sizes} (tt in 4..12, "
+                              "Ma in [0.3, 0.6], alpha in [-2, 3] deg), per GPU",
+                  "seconds": t_ub, "converged": conv,
+                  "iterations_max": max(len(h) for h in ures.rel_norms),
+                  "plain": {"value": world * n_plain / t_up, "instances": n_plain,
+                            "seconds": t_up},
+                  "batched_vs_plain": (len(uspecs) / t_ub) / (n_plain / t_up)}
+        del ures, uinst
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         rate, sample = cpu_residual_rate(X, V, Us[:4], 1, args.cpu_seconds)
@@ -425,6 +488,7 @@ def run_b200(args) -> None:
             "value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
             "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4},
         "resolvent": res,
+        "uneven": uneven,
     }
     print(json.dumps(line), flush=True)
 

@@ -102,10 +102,12 @@ def _shape_groups(instances) -> dict:
 
 
 def _batched_solves(instances, J, shifts_of, rhs_of, out_of, adjoint: bool, workspace,
-                    tol: float) -> None:
+                    tol: float, on_fail=None) -> None:
     """Solves (J_i - s_i I) x_i = b_i (or the adjoint) for the instances in ``shifts_of``, the
     instances of one grid size together per factorisation call, as many per call as the
-    ``workspace`` (one uint8 device tensor) holds."""
+    ``workspace`` (one uint8 device tensor) holds. If a call fails (a singular or non-finite
+    system, a solve that misses ``tol``), its systems are retried one at a time and those that
+    still fail are passed to ``on_fail`` (or re-raised without one)."""
     from . import _lib
     from .solver import RingLUMany, ringlu_workspace_bytes
 
@@ -120,14 +122,27 @@ def _batched_solves(instances, J, shifts_of, rhs_of, out_of, adjoint: bool, work
             raise ValueError(f"workspace of {workspace.numel()} bytes is below one {M}x{N} system")
         batch = _lib.single_batch(_lib.make_instance(M, N, 0.5, 0.0))
         lu = RingLUMany(batch, capacity=cap, tol=tol, workspace=workspace)
-        for c0 in range(0, len(todo), cap):
-            chunk = todo[c0:c0 + cap]
-            nc = M * N
+        nc = M * N
+
+        def run(chunk):
             offs = [instances.cell_offsets[i] for i in chunk]
             lu.factor([J[144 * o:144 * (o + nc)] for o in offs], [shifts_of[i] for i in chunk])
             xs, _ = lu.solve([rhs_of(i) for i in chunk], adjoint=adjoint)
             for i, x in zip(chunk, xs):
                 out_of(i, x)
+
+        for c0 in range(0, len(todo), cap):
+            chunk = todo[c0:c0 + cap]
+            try:
+                run(chunk)
+            except _lib.EulerB200Error:
+                for i in chunk:
+                    try:
+                        run([i])
+                    except _lib.EulerB200Error:
+                        if on_fail is None:
+                            raise
+                        on_fail(i)
 
 
 def ptc_batched(instances, states=None, rtol: float = 1e-10, max_iter: int = 100,
@@ -184,7 +199,11 @@ def ptc_batched(instances, states=None, rtol: float = 1e-10, max_iter: int = 100
             o, n = inst.cell_offsets[i], 4 * inst.specs[i].M * inst.specs[i].N
             dU[4 * o:4 * o + n] += x[0::2]
 
-        _batched_solves(inst, J, shifts, rhs_of, update, False, workspace, tol)
+        def failed(i):  # a singular shifted Jacobian: the instance stops here, as diverged
+            o, n = inst.cell_offsets[i], 4 * inst.specs[i].M * inst.specs[i].N
+            dU[4 * o:4 * o + n] = float("nan")
+
+        _batched_solves(inst, J, shifts, rhs_of, update, False, workspace, tol, failed)
     res.states, res.vertices, res.velocities = dU, dX, dV
     return res
 
@@ -195,7 +214,8 @@ def adjoint_lift_gradients_batched(instances, result: BatchedPtcResult,
     """``adjoint_lift_gradient`` of every instance at the states of ``result``: the forces
     Jacobians, d(odes)/d(states) and d(odes)/d(vertices) of all instances in one launch each,
     the adjoint solves at shift 0 with the instances of one grid size factored together, and
-    the reverse products over all instances. Returns one (2, M+1, N+1) array per instance."""
+    the reverse products over all instances. Returns one (2, M+1, N+1) array per instance, or
+    None for an instance whose PTC did not converge (or whose adjoint system is singular)."""
     import torch
 
     inst = instances
@@ -223,9 +243,11 @@ def adjoint_lift_gradients_batched(instances, result: BatchedPtcResult,
         o, n = inst.cell_offsets[i], 8 * inst.specs[i].M * inst.specs[i].N
         lam[8 * o:8 * o + n] = x
 
+    ok = {i for i, h in enumerate(result.rel_norms) if h and np.isfinite(h[-1])}
+    bad = set(range(len(inst))) - ok
     workspace = torch.empty(int(workspace_bytes) // 256 * 256, dtype=torch.uint8, device="cuda")
-    _batched_solves(inst, J, {i: 0.0 for i in range(len(inst))}, rhs_of, store, True, workspace,
-                    tol)
+    _batched_solves(inst, J, {i: 0.0 for i in sorted(ok)}, rhs_of, store, True, workspace, tol,
+                    bad.add)
     del workspace, J
     Jx = torch.empty(32 * nc, **f64)
     inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, Jx)
@@ -234,10 +256,10 @@ def adjoint_lift_gradients_batched(instances, result: BatchedPtcResult,
     inst.call("eb_apply_forces_wrt_vertices_rev", JFx, g, gX_f)
     grad = (gX_f - gX_r)[0::2].cpu().numpy()
     out, o = [], 0
-    for sp in inst.specs:
+    for k, sp in enumerate(inst.specs):
         n = 2 * (sp.M + 1) * (sp.N + 1)
-        out.append(np.asfortranarray(np.reshape(grad[o:o + n], (2, sp.M + 1, sp.N + 1),
-                                                order="F")))
+        out.append(None if k in bad else np.asfortranarray(
+            np.reshape(grad[o:o + n], (2, sp.M + 1, sp.N + 1), order="F")))
         o += n
     return out
 
