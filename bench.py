@@ -44,7 +44,7 @@ BYTES_PER_CELL_VJP = 1152 + 256 + 256 + 32 + 4 * 64 + 64 + 2 * 32 + 8
 GRID = dict(radial_pts=129, angular_pts=129, thickness=0.04, chord=10.0, far_radius=200.0,
             first_spacing=0.1)
 FLOW = dict(mach=0.5, aoa_deg=0.0, center=(2.5, 0.0))
-PROFILE_SUMMARY = ROOT / "profiles" / "residual_naca0004_129x129.md"
+PROFILE_SUMMARY = ROOT / "profiles" / "residual_tiled_naca0004_129x129.md"
 
 
 def parse_args():
@@ -69,6 +69,10 @@ def parse_args():
                    help="instances timed one at a time for the comparison")
     p.add_argument("--workspace-gb", type=float, default=80.0,
                    help="device memory for batched factorisations")
+    p.add_argument("--profile-region", choices=["none", "residual", "batched"], default="none",
+                   help="bracket one region with cudaProfilerStart/Stop (for "
+                        "ncu --profile-from-start off): the timed residual launches or the "
+                        "batched frequency response")
     p.add_argument("--shift-group", type=int, default=32,
                    help="shifts factored concurrently (one workspace of ~2.7 GB each)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline budget")
@@ -268,11 +272,15 @@ def run_b200(args) -> None:
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        if args.profile_region == "residual":
+            torch.cuda.profiler.start()
         ev0.record(stream)
         for _ in range(args.steps):
             residual()
         ev1.record(stream)
         barrier()
+        if args.profile_region == "residual":
+            torch.cuda.profiler.stop()
     t_res = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     clk = clocks.summary()
     value = world * cells * args.steps / t_res
@@ -373,8 +381,12 @@ def run_b200(args) -> None:
                                            group=group)  # warm-up
         barrier()
         t0 = time.perf_counter()
+        if args.profile_region == "batched":
+            torch.cuda.profiler.start()
         cl_b, cm_b = drivers.frequency_response_batched(sd, GRID["chord"], FLOW["center"][0], ks,
                                                         group=group)
+        if args.profile_region == "batched":
+            torch.cuda.profiler.stop()
         grad_b = drivers.adjoint_lift_gradient(sd)
         barrier()
         t_batched = max_over_ranks(time.perf_counter() - t0)
