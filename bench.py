@@ -291,7 +291,13 @@ def run_b200(args) -> None:
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic_cell = read_traffic()
 
-    # end to end through the C ABI with host buffers: H2D of the step's inputs, D2H of R
+    # end to end through the C ABI with host buffers: every step copies its inputs (X, V, U)
+    # from pinned host memory and its result R back. Serial: one stream, copies and launch in
+    # sequence. Pipelined (the reported e2e): pyeulerale_b200.pipeline.ResidualPipeline, step
+    # k+1's inputs, step k's residual and step k-1's result in flight together.
+    from pyeulerale_b200.pipeline import ResidualPipeline
+
+    e2e_steps = max(3, args.steps // 5)
     for _ in range(max(1, args.warmup // 2)):
         dX.copy_(hX, non_blocking=True)
         dV.copy_(hV, non_blocking=True)
@@ -299,7 +305,6 @@ def run_b200(args) -> None:
         residual()
         hR.copy_(dR, non_blocking=True)
     barrier()
-    e2e_steps = max(3, args.steps // 5)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
@@ -310,10 +315,25 @@ def run_b200(args) -> None:
         hR.copy_(dR, non_blocking=True)
     e1.record(stream)
     barrier()
+    t_serial = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    del dX, dV, dU, dR  # the pipeline holds its own device buffers
+    pipe = ResidualPipeline(inst, depth=2)
+    for _ in range(max(2, args.warmup // 2)):
+        pipe.submit(hX, hV, hU, hR)
+    pipe.synchronize()
+    barrier()
+    e0.record(pipe.s_in)
+    for _ in range(e2e_steps):
+        pipe.submit(hX, hV, hU, hR)
+    e1.record(pipe.s_out)
+    pipe.synchronize()
+    barrier()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     h2d = (hX.numel() + hV.numel() + hU.numel()) * 8
     d2h = hR.numel() * 8
     e2e_value = world * cells * e2e_steps / t_e2e
+    e2e_serial = world * cells * e2e_steps / t_serial
+    dX, dV, dU = pipe.bufs[0]["X"], pipe.bufs[0]["V"], pipe.bufs[0]["U"]
 
     # VJP set on stored Jacobians (d/dU, d/dX, d/dV, d/dMa) per instance
     vjp_rate = vjp_gbs = None
@@ -493,7 +513,11 @@ def run_b200(args) -> None:
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                "path": "pyeulerale_b200.pipeline.ResidualPipeline (copies and launches of "
+                        "consecutive steps overlapped on three streams)",
+                "serial": {"value": e2e_serial,
+                           "path": "one stream: H2D of X, V, U, eb_compute_odes, D2H of R"}},
         "gpu_launches": args.steps,
         "clocks": clk,
         "vjp": None if vjp_rate is None else {

@@ -177,3 +177,30 @@ def test_residual_uneven_batch(cuda, oracle, golden_grids, entry):
     for k, (s, X, V, U) in enumerate(zip(specs, grids, vels, states)):
         ref = oracle_eval(oracle, dict(X=X, V=V, U=U, mach=s.mach, aoa=s.aoa_deg))["R"]
         assert rel_err(got[k], ref) <= TOL_R, (entry, k, rel_err(got[k], ref))
+
+
+def test_residual_pipeline_matches_direct_calls(cuda, golden_grids):
+    """Streaming steps (overlapped copies and launches) give each step's own residual."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+    from pyeulerale_b200.pipeline import ResidualPipeline
+
+    rng = np.random.default_rng(23)
+    X = golden_grids["naca0004_129x129"]
+    specs = [InstanceSpec(X, 0.5, 0.0), InstanceSpec(X, 0.45, 1.0)]
+    inst = InstanceSet(specs)
+    hX = cuda.from_numpy(inst.pack_vertices()).pin_memory()
+    hV = cuda.from_numpy(inst.pack_vertices([G.smooth_velocities(X, rng)] * 2)).pin_memory()
+    steps = []
+    for k in range(5):
+        U = [G.perturbed_states(s.M, s.N, s.mach, s.aoa_deg, 0.01, rng) for s in specs]
+        steps.append((cuda.from_numpy(inst.pack_cells(U)).pin_memory(),
+                      cuda.empty(4 * inst.n_cells, dtype=cuda.float64).pin_memory()))
+    pipe = ResidualPipeline(inst, depth=2)
+    for hU, hR in steps:
+        pipe.submit(hX, hV, hU, hR)
+    pipe.synchronize()
+    dR = cuda.empty(4 * inst.n_cells, dtype=cuda.float64, device="cuda")
+    for hU, hR in steps:
+        inst.call("eb_compute_odes", hX.cuda(), hV.cuda(), hU.cuda(), dR)
+        np.testing.assert_array_equal(hR.numpy(), dR.cpu().numpy())
