@@ -38,7 +38,9 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -61,6 +63,7 @@ struct Handle {
   cublasHandle_t blas = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  cudaEvent_t start = nullptr;
 };
 
 constexpr int kLanes = 2;
@@ -75,9 +78,11 @@ int blas_handle(cudaStream_t st, cublasHandle_t& out, int lane = 0) {
     h.blas = nullptr;
     h.stream = nullptr;  // streams and events of another device are left to that device
     h.done = nullptr;
+    h.start = nullptr;
     if (cublasCreate(&h.blas) != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "cublasCreate failed");
     if (lane > 0 && (cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking) != cudaSuccess ||
-                     cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) != cudaSuccess))
+                     cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming) != cudaSuccess))
       return check_launch("ringlu lane stream");
     h.device = dev;
   }
@@ -101,7 +106,7 @@ inline int panel_width(int K) {
 struct Layout {
   int M, N, K;
   size_t blk;  // bytes of one K x K complex block
-  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_T, off_perm, off_info, off_acc;
+  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_T, off_perm, off_info, off_acc, off_shift;
   size_t off_y, off_x, off_r;
   size_t total;
 };
@@ -127,6 +132,7 @@ Layout plan(int M, int N) {
   L.off_perm = take(sizeof(int) * (size_t)L.K);
   L.off_info = take(sizeof(int) * 4);
   L.off_acc = take(sizeof(double) * 2);
+  L.off_shift = take(sizeof(double) * 2);
   const size_t vec = sizeof(cuDoubleComplex) * (size_t)L.K * M;
   L.off_y = take(vec);
   L.off_x = take(vec);
@@ -137,9 +143,10 @@ Layout plan(int M, int N) {
 
 // Scatters the 4x4 blocks of the nine-slot Jacobian into the ring super-blocks
 // (column-major K x K) and subtracts the shift on the diagonal.
-__global__ void k_assemble(int M, int N, const double* J, double sr, double si,
+__global__ void k_assemble(int M, int N, const double* J, const double* shift,
                            cuDoubleComplex* D, cuDoubleComplex* B1, cuDoubleComplex* B2,
                            cuDoubleComplex* C1, cuDoubleComplex* C2) {
+  const double sr = shift[0], si = shift[1];
   const int64_t cells = (int64_t)M * N;
   const int K = 4 * N;
   const int64_t blk = (int64_t)K * K;
@@ -749,6 +756,132 @@ int64_t eb_ringlu_workspace_bytes(int M, int N) {
   return (int64_t)plan(M, N).total;
 }
 
+}  // extern "C"
+
+namespace eb {
+namespace rl {
+
+// Everything a factorisation launches, on stream st (and the second lane's stream): zeroing,
+// assembly from J[s] and the shift stored in each workspace, and the ring eliminations. The
+// sequence depends only on the workspace, the Jacobian pointers and the sizes, so it can be
+// captured once in a CUDA graph and replayed for any shifts.
+int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
+  const Layout& L = g.L;
+  const int M = L.M, N = L.N, n_shifts = g.S;
+  cublasHandle_t h = nullptr;
+  int rc = blas_handle(st, h);
+  if (rc != EB_OK) return rc;
+  for (int s = 0; s < n_shifts; ++s) {
+    char* w = g.base + (int64_t)s * g.stride;
+    cudaMemsetAsync(w, 0, L.off_T, st);  // the five block arrays
+    cudaMemsetAsync(w + L.off_info, 0, sizeof(int) * 4, st);
+    k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
+        M, N, J[s], reinterpret_cast<const double*>(w + L.off_shift),
+        reinterpret_cast<cuDoubleComplex*>(w + L.off_D), reinterpret_cast<cuDoubleComplex*>(w + L.off_L1),
+        reinterpret_cast<cuDoubleComplex*>(w + L.off_L2), reinterpret_cast<cuDoubleComplex*>(w + L.off_C1),
+        reinterpret_cast<cuDoubleComplex*>(w + L.off_C2));
+  }
+  if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
+  if (n_shifts == 1) {
+    for (int m = 0; m < M; ++m)
+      if ((rc = factor_ring(g, h, m, st)) != EB_OK) return rc;
+    return EB_OK;
+  }
+  // Two halves of the shifts on two streams, ring by ring: one half's latency-bound
+  // Gauss-Jordan panels overlap the other half's GEMMs on the rest of the GPU.
+  cublasHandle_t h2 = nullptr;
+  if ((rc = blas_handle(st, h2, 1)) != EB_OK) return rc;
+  const Handle& lane = g_handle[1];
+  const int s1 = (n_shifts + 1) / 2;
+  const Group g1{L, g.base, g.stride, s1};
+  const Group g2{L, g.base + (int64_t)s1 * g.stride, g.stride, n_shifts - s1};
+  cudaEventRecord(lane.start, st);
+  cudaStreamWaitEvent(lane.stream, lane.start, 0);
+  for (int m = 0; m < M; ++m) {
+    if ((rc = factor_ring(g1, h, m, st)) != EB_OK) return rc;
+    if ((rc = factor_ring(g2, h2, m, lane.stream)) != EB_OK) return rc;
+  }
+  cudaEventRecord(lane.done, lane.stream);
+  cudaStreamWaitEvent(st, lane.done, 0);
+  return EB_OK;
+}
+
+// Captured factorisations: the first call with a given (device, workspace, stride, sizes,
+// Jacobian pointers) runs eagerly (cuBLAS initialises outside any capture), the second
+// captures the launch sequence into a CUDA graph, later ones replay it. A few graphs are kept
+// per thread (least recently used first out). EB_RINGLU_GRAPHS=0 turns capture off.
+struct GraphKey {
+  int device, M, N, S;
+  const char* base;
+  int64_t stride;
+  std::vector<const double*> J;
+  bool operator==(const GraphKey& o) const {
+    return device == o.device && M == o.M && N == o.N && S == o.S && base == o.base &&
+           stride == o.stride && J == o.J;
+  }
+};
+struct GraphEntry {
+  GraphKey key;
+  cudaGraphExec_t exec = nullptr;  // null: seen once, not captured yet
+  uint64_t used = 0;
+  bool eager_only = false;         // capture failed once: run eagerly from now on
+};
+thread_local std::vector<GraphEntry> g_graphs;
+thread_local uint64_t g_graph_clock = 0;
+constexpr size_t kMaxGraphs = 8;
+
+bool graphs_enabled() {
+  const char* v = std::getenv("EB_RINGLU_GRAPHS");
+  return !(v && v[0] == '0');
+}
+
+int run_factor(const Group& g, const double* const* J, cudaStream_t st) {
+  if (!graphs_enabled()) return issue_factor(g, J, st);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  GraphKey key{dev, g.L.M, g.L.N, g.S, g.base, g.stride, std::vector<const double*>(J, J + g.S)};
+  GraphEntry* e = nullptr;
+  for (auto& x : g_graphs)
+    if (x.key == key) e = &x;
+  if (!e) {  // first sight: eager, remember the key
+    if (g_graphs.size() >= kMaxGraphs) {
+      auto lru = std::min_element(g_graphs.begin(), g_graphs.end(),
+                                  [](const GraphEntry& a, const GraphEntry& b) { return a.used < b.used; });
+      if (lru->exec) cudaGraphExecDestroy(lru->exec);
+      g_graphs.erase(lru);
+    }
+    g_graphs.push_back(GraphEntry{key, nullptr, ++g_graph_clock, false});
+    return issue_factor(g, J, st);
+  }
+  e->used = ++g_graph_clock;
+  if (e->eager_only) return issue_factor(g, J, st);
+  if (!e->exec) {
+    cudaGraph_t graph = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    int rc = EB_OK;
+    if (err == cudaSuccess) {
+      rc = issue_factor(g, J, st);
+      err = cudaStreamEndCapture(st, &graph);
+    }
+    if (rc == EB_OK && err == cudaSuccess && graph)
+      err = cudaGraphInstantiate(&e->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != EB_OK || err != cudaSuccess || !e->exec) {  // not capturable here: stay eager
+      cudaGetLastError();
+      e->exec = nullptr;
+      e->eager_only = true;
+      return issue_factor(g, J, st);
+    }
+  }
+  if (cudaGraphLaunch(e->exec, st) != cudaSuccess) return check_launch("ringlu graph launch");
+  return EB_OK;
+}
+
+}  // namespace rl
+}  // namespace eb
+
+extern "C" {
+
 int eb_ringlu_factor_many(const eb_batch* b, const double* const* J, int n_shifts,
                           const double* shifts, void* workspace, int64_t workspace_stride,
                           void* stream) {
@@ -759,45 +892,12 @@ int eb_ringlu_factor_many(const eb_batch* b, const double* const* J, int n_shift
   for (int s = 0; s < n_shifts; ++s)
     if (!J[s]) return fail(EB_ERR_ARG, "ringlu: null Jacobian");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  cublasHandle_t h = nullptr;
-  if ((rc = blas_handle(st, h)) != EB_OK) return rc;
   const Group g{L, static_cast<char*>(workspace), workspace_stride, n_shifts};
-  const int M = L.M, N = L.N;
-  for (int s = 0; s < n_shifts; ++s) {
-    char* w = g.base + (int64_t)s * g.stride;
-    cudaMemsetAsync(w, 0, L.off_T, st);  // the five block arrays
-    cudaMemsetAsync(w + L.off_info, 0, sizeof(int) * 4, st);
-    k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
-        M, N, J[s], shifts[2 * s], shifts[2 * s + 1], reinterpret_cast<cuDoubleComplex*>(w + L.off_D),
-        reinterpret_cast<cuDoubleComplex*>(w + L.off_L1), reinterpret_cast<cuDoubleComplex*>(w + L.off_L2),
-        reinterpret_cast<cuDoubleComplex*>(w + L.off_C1), reinterpret_cast<cuDoubleComplex*>(w + L.off_C2));
-  }
-  if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
-  if (n_shifts == 1) {
-    for (int m = 0; m < M; ++m)
-      if ((rc = factor_ring(g, h, m, st)) != EB_OK) return rc;
-  } else {
-    // Two halves of the shifts on two streams, ring by ring: one half's latency-bound
-    // Gauss-Jordan panels overlap the other half's GEMMs on the rest of the GPU.
-    cublasHandle_t h2 = nullptr;
-    if ((rc = blas_handle(st, h2, 1)) != EB_OK) return rc;
-    const Handle& lane = g_handle[1];
-    const int s1 = (n_shifts + 1) / 2;
-    const Group g1{L, g.base, g.stride, s1};
-    const Group g2{L, g.base + (int64_t)s1 * g.stride, g.stride, n_shifts - s1};
-    cudaEvent_t start = nullptr;
-    if (cudaEventCreateWithFlags(&start, cudaEventDisableTiming) != cudaSuccess)
-      return check_launch("ringlu event");
-    cudaEventRecord(start, st);
-    cudaStreamWaitEvent(lane.stream, start, 0);
-    cudaEventDestroy(start);
-    for (int m = 0; m < M; ++m) {
-      if ((rc = factor_ring(g1, h, m, st)) != EB_OK) return rc;
-      if ((rc = factor_ring(g2, h2, m, lane.stream)) != EB_OK) return rc;
-    }
-    cudaEventRecord(lane.done, lane.stream);
-    cudaStreamWaitEvent(st, lane.done, 0);
-  }
+  for (int s = 0; s < n_shifts; ++s)
+    if (cudaMemcpyAsync(g.base + (int64_t)s * g.stride + L.off_shift, shifts + 2 * s,
+                        2 * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return check_launch("ringlu shifts");
+  if ((rc = run_factor(g, J, st)) != EB_OK) return rc;
   if ((rc = check_launch("ringlu factor")) != EB_OK) return rc;
   std::vector<int> info(n_shifts);
   for (int s = 0; s < n_shifts; ++s)

@@ -172,3 +172,28 @@ def test_ringlu_wide_rings(cuda, oracle):
             ref = spla.spsolve(op, b.ravel(order="F"))
             got = gpu.host(x, (4, 8, 256), complex_=True).ravel(order="F")
             assert rel <= 1e-10 and rel_err(got, ref) <= 1e-8, (shift, adjoint, rel)
+
+
+def test_ringlu_graph_replay(cuda, golden_grids, monkeypatch):
+    """Eager, captured and replayed factorisations of the same workspace give the same
+    solutions for different shifts (the shifts live in device memory, the graph does not)."""
+    from pyeulerale_b200 import solver
+
+    case = make_case("naca0012_33", golden_grids, seed=8)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(2)
+    rhs = [gpu.dev(crandn(rng, (4, M, N))) for _ in range(2)]
+    shifts = [[0.1j, 2.0], [0.3 - 0.2j, 0.0], [1.5j, 0.02], [0.7, 0.05j]]
+    many = solver.RingLUMany(gpu.batch, capacity=2, tol=1e-10)
+    got = []
+    for sh in shifts:  # call 1 eager, call 2 captured, calls 3-4 replayed
+        many.factor(g["_dev"]["J_u"], sh)
+        got.append([x.cpu().numpy() for x in many.solve(rhs)[0]])
+    monkeypatch.setenv("EB_RINGLU_GRAPHS", "0")
+    for sh, xs in zip(shifts, got):
+        many.factor(g["_dev"]["J_u"], sh)
+        ref = [x.cpu().numpy() for x in many.solve(rhs)[0]]
+        for a, b in zip(xs, ref):
+            assert rel_err(a, b) <= 1e-12, sh
