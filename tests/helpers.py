@@ -26,6 +26,11 @@ def make_case(name: str, golden_grids: dict, seed: int = 0) -> dict:
         U = G.perturbed_states(32, 32, 0.6, 2.0, 0.01, rng)
         V = G.smooth_velocities(X, rng)
         return dict(X=X, V=V, U=U, mach=0.6, aoa=2.0)
+    if name == "min4x5":  # the smallest grid the reference handles: M = 4, N = 5
+        X = G.naca_ogrid(5, 6, thickness=0.12, chord=1.0, far_radius=10.0, first_spacing=0.05)
+        U = G.perturbed_states(4, 5, 0.5, 1.25, 0.01, rng)
+        V = G.smooth_velocities(X, rng)
+        return dict(X=X, V=V, U=U, mach=0.5, aoa=1.25)
     if name == "naca0004_129":
         X = golden_grids["naca0004_129x129"]
         U = G.perturbed_states(128, 128, 0.5, 0.0, 0.01, rng)

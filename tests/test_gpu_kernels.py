@@ -2,6 +2,8 @@
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -9,7 +11,7 @@ from helpers import Gpu, crandn, make_case, oracle_eval, rel_err
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129"]
+CASES = ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129", "min4x5"]
 
 # Tolerances: residual / forces differ from the reference arithmetic by summation order and
 # the real-vs-complex evaluation only; Jacobians are exact dual-number derivatives compared
@@ -204,3 +206,17 @@ def test_residual_pipeline_matches_direct_calls(cuda, golden_grids):
     for hU, hR in steps:
         inst.call("eb_compute_odes", hX.cuda(), hV.cuda(), hU.cuda(), dR)
         np.testing.assert_array_equal(hR.numpy(), dR.cpu().numpy())
+
+
+@pytest.mark.parametrize("M,N", [(3, 8), (8, 4), (0, 0)])
+def test_undersized_grids_are_rejected(cuda, M, N):
+    """Grids below M = 4, N = 5 (where the reference indexes out of bounds) fail on the host
+    with EB_ERR_ARG before any launch."""
+    from pyeulerale_b200 import _lib
+
+    b = _lib.single_batch(_lib.make_instance(M, N, 0.5, 0.0))
+    t = cuda.zeros(64, dtype=cuda.float64, device="cuda")
+    with pytest.raises(_lib.EulerB200Error) as err:
+        _lib.call("eb_compute_odes", ctypes.byref(b), t.data_ptr(), t.data_ptr(), t.data_ptr(),
+                  t.data_ptr(), None)
+    assert err.value.code == _lib.EB_ERR_ARG

@@ -74,7 +74,8 @@ def test_gmres_batched_shifts_match_single(cuda, golden_grids):
         assert rel_err(a, c) <= 1e-8, (k, info_b)
 
 
-@pytest.mark.parametrize("name", ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129"])
+@pytest.mark.parametrize("name", ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129",
+                                  "min4x5"])
 @pytest.mark.parametrize("shift", [0.3 + 0.7j, 2.0, 0.0, 0.0012j])
 def test_ringlu_direct_solve(cuda, oracle, golden_grids, name, shift):
     """Ring-block LU resolvent: 1e-10 residual and agreement with SuperLU, both directions."""
