@@ -315,38 +315,58 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
   const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
   const int tid = threadIdx.x;
 
-  // 1. stage states (cross-shaped halo) and derived quantities
-  for (int e = tid; e < kStaged; e += kThreads) {
+  // 1. stage states (cross-shaped halo) and derived quantities, vertices and grid velocities.
+  // A thread first issues all of its global loads (at most two staged states and two vertex
+  // pairs: kStaged = 432 and kVerts = 297 are below 2 * kThreads), then derives and stores, so
+  // its loads are in flight together instead of one round after another.
+  static_assert(kStaged <= 2 * kThreads && kVerts <= 2 * kThreads, "two staging rounds");
+  double2 sa[2], sb[2], xv[2], vv[2];
+  bool sval[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int e = tid + k * kThreads;
     const int r = e % kSR - 2, c = e / kSR - 2;
     const bool corner = (r < 0 || r >= kTM) && (c < 0 || c >= kTN);
     const int m = m0 + r;
-    if (corner || m < 0 || m >= M) {
-      S.rho[e] = 1.0; S.j1[e] = 0.0; S.j2[e] = 0.0; S.e[e] = 1.0;
-      S.p[e] = 1.0; S.ir[e] = 1.0; S.cs[e] = 1.0;
-      continue;
+    sval[k] = e < kStaged && !corner && m >= 0 && m < M;
+    sa[k] = make_double2(1.0, 0.0);
+    sb[k] = make_double2(0.0, 1.0);
+    if (sval[k]) {
+      int n = n0 + c;  // periodic in the angular index: n0 + c lies in [-2, N + kTN + 1]
+      while (n < 0) n += N;
+      while (n >= N) n -= N;
+      const double* q = Ui + 4 * (m + (int64_t)M * n);
+      sa[k] = __ldg(reinterpret_cast<const double2*>(q));
+      sb[k] = __ldg(reinterpret_cast<const double2*>(q + 2));
     }
-    const int n = wrap(n0 + c, N);
-    const double* q = Ui + 4 * (m + (int64_t)M * n);
-    const double2 a = __ldg(reinterpret_cast<const double2*>(q));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(q + 2));
-    const St s = derive(a.x, a.y, b.x, b.y);
-    S.rho[e] = s.rho; S.j1[e] = s.j1; S.j2[e] = s.j2; S.e[e] = s.e;
-    S.p[e] = s.p; S.ir[e] = s.ir; S.cs[e] = s.cs;
+    const int ev = tid + k * kThreads;
+    xv[k] = make_double2(0.0, 0.0);
+    vv[k] = make_double2(0.0, 0.0);
+    if (ev < kVerts) {
+      const int vm = min(m0 + ev % kVR, M), vn = min(n0 + ev / kVR, N);
+      const int64_t v = vm + (int64_t)(M + 1) * vn;
+      xv[k] = __ldg(reinterpret_cast<const double2*>(Xi + 2 * v));
+      if (Vi) vv[k] = __ldg(reinterpret_cast<const double2*>(Vi + 2 * v));
+    }
   }
-  for (int e = tid; e < kVerts; e += kThreads) {
-    const int r = e % kVR, c = e / kVR;
-    const int m = min(m0 + r, M), n = min(n0 + c, N);
-    const int64_t v = m + (int64_t)(M + 1) * n;
-    const double2 xv = __ldg(reinterpret_cast<const double2*>(Xi + 2 * v));
-    S.x[e] = xv.x;
-    S.z[e] = xv.y;
-    if (Vi) {
-      const double2 vv = __ldg(reinterpret_cast<const double2*>(Vi + 2 * v));
-      S.vx[e] = vv.x;
-      S.vz[e] = vv.y;
-    } else {
-      S.vx[e] = 0.0;
-      S.vz[e] = 0.0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int e = tid + k * kThreads;
+    if (e < kStaged) {
+      if (sval[k]) {
+        const St st = derive(sa[k].x, sa[k].y, sb[k].x, sb[k].y);
+        S.rho[e] = st.rho; S.j1[e] = st.j1; S.j2[e] = st.j2; S.e[e] = st.e;
+        S.p[e] = st.p; S.ir[e] = st.ir; S.cs[e] = st.cs;
+      } else {  // outside the grid or an unused corner: finite placeholders
+        S.rho[e] = 1.0; S.j1[e] = 0.0; S.j2[e] = 0.0; S.e[e] = 1.0;
+        S.p[e] = 1.0; S.ir[e] = 1.0; S.cs[e] = 1.0;
+      }
+    }
+    if (e < kVerts) {
+      S.x[e] = xv[k].x;
+      S.z[e] = xv[k].y;
+      S.vx[e] = vv[k].x;
+      S.vz[e] = vv[k].y;
     }
   }
   __syncthreads();
