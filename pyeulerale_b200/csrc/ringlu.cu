@@ -382,15 +382,33 @@ __global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int
   }
   __syncthreads();
   if (bad) return;  // singular block: pivots incomplete, the caller fails
-  for (int e = tid; e < NB * kUpdRowsT; e += 256) {
-    const int k = e / kUpdRowsT, x = e % kUpdRowsT, rr = r0 + x;
-    cuDoubleComplex g = rr < K ? out[(size_t)K * (j0 + k) + rr] : make_cuDoubleComplex(0.0, 0.0);
-    if (rr == pv[k]) g.x -= 1.0;
-    G[k][x] = g;
+  // the G and R tiles: every load of this thread first, then the shared-memory stores
+  constexpr int kGI = (NB * kUpdRowsT + 255) / 256, kRI = (NB * kUpdColsT + 255) / 256;
+  cuDoubleComplex gv[kGI], rv[kRI];
+#pragma unroll
+  for (int q = 0; q < kGI; ++q) {
+    const int e = tid + 256 * q, k = e / kUpdRowsT, rr = r0 + e % kUpdRowsT;
+    gv[q] = make_cuDoubleComplex(0.0, 0.0);
+    if (e < NB * kUpdRowsT && rr < K) gv[q] = out[(size_t)K * (j0 + k) + rr];
   }
-  for (int e = tid; e < NB * kUpdColsT; e += 256) {
-    const int k = e / kUpdColsT, x = e % kUpdColsT, col = c0 + x;
-    R[k][x] = col < K ? in[(size_t)K * col + pv[k]] : make_cuDoubleComplex(0.0, 0.0);
+#pragma unroll
+  for (int q = 0; q < kRI; ++q) {
+    const int e = tid + 256 * q, k = e / kUpdColsT, col = c0 + e % kUpdColsT;
+    rv[q] = make_cuDoubleComplex(0.0, 0.0);
+    if (e < NB * kUpdColsT && col < K) rv[q] = in[(size_t)K * col + pv[k]];
+  }
+#pragma unroll
+  for (int q = 0; q < kGI; ++q) {
+    const int e = tid + 256 * q, k = e / kUpdRowsT, x = e % kUpdRowsT;
+    if (e < NB * kUpdRowsT) {
+      if (r0 + x == pv[k]) gv[q].x -= 1.0;
+      G[k][x] = gv[q];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kRI; ++q) {
+    const int e = tid + 256 * q;
+    if (e < NB * kUpdColsT) R[e / kUpdColsT][e % kUpdColsT] = rv[q];
   }
   __syncthreads();
   if (row >= K) return;
