@@ -356,10 +356,9 @@ __global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int
                                                    size_t off_in, size_t off_out, size_t off_perm,
                                                    size_t off_info) {
   constexpr int kPer = kUpdRowsT * kUpdColsT / 256;  // outputs per thread
+  constexpr int kGI = (NB * kUpdRowsT + 255) / 256, kRI = (NB * kUpdColsT + 255) / 256;
   __shared__ cuDoubleComplex G[NB][kUpdRowsT];
   __shared__ cuDoubleComplex R[NB][kUpdColsT];
-  __shared__ int pv[NB];
-  __shared__ int bad;
   const int ctiles = (K + kUpdColsT - 1) / kUpdColsT;
   const int c0 = (blockIdx.x % ctiles) * kUpdColsT, r0 = (blockIdx.x / ctiles) * kUpdRowsT;
   const cuDoubleComplex* in = at<cuDoubleComplex>(ws0, stride, off_in);
@@ -367,41 +366,43 @@ __global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int
   const int* perm = at<int>(ws0, stride, off_perm);
   const int tid = threadIdx.x;
   const int r = tid % kUpdRowsT, row = r0 + r, cb = tid / kUpdRowsT;
-  // prefetch this thread's inputs (columns cb, cb + 4, ...)
-  cuDoubleComplex acc[kPer];
+  // All of this thread's loads first: its inputs (columns cb, cb + 4, ...), its elements of the
+  // G tile (panel columns) and of the R tile (pivot rows, addressed through perm, which is
+  // checked before use); then the shared-memory stores and one barrier that also agrees on
+  // whether the panel was singular.
+  cuDoubleComplex acc[kPer], gv[kGI], rv[kRI];
 #pragma unroll
   for (int q = 0; q < kPer; ++q) {
     const int col = c0 + cb + 4 * q;
     acc[q] = row < K && col < K ? in[(size_t)K * col + row] : make_cuDoubleComplex(0.0, 0.0);
   }
-  if (tid == 0) bad = *at<int>(ws0, stride, off_info);
-  __syncthreads();
-  if (tid < NB) {
-    pv[tid] = perm[j0 + tid];
-    if (pv[tid] < 0 || pv[tid] >= K) atomicExch(&bad, 1);
-  }
-  __syncthreads();
-  if (bad) return;  // singular block: pivots incomplete, the caller fails
-  // the G and R tiles: every load of this thread first, then the shared-memory stores
-  constexpr int kGI = (NB * kUpdRowsT + 255) / 256, kRI = (NB * kUpdColsT + 255) / 256;
-  cuDoubleComplex gv[kGI], rv[kRI];
+  int bad = *at<int>(ws0, stride, off_info) != 0;
+  int pg[kGI];
 #pragma unroll
   for (int q = 0; q < kGI; ++q) {
     const int e = tid + 256 * q, k = e / kUpdRowsT, rr = r0 + e % kUpdRowsT;
     gv[q] = make_cuDoubleComplex(0.0, 0.0);
-    if (e < NB * kUpdRowsT && rr < K) gv[q] = out[(size_t)K * (j0 + k) + rr];
+    pg[q] = -1;
+    if (e < NB * kUpdRowsT) {
+      pg[q] = perm[j0 + k];
+      if (rr < K) gv[q] = out[(size_t)K * (j0 + k) + rr];
+    }
   }
 #pragma unroll
   for (int q = 0; q < kRI; ++q) {
     const int e = tid + 256 * q, k = e / kUpdColsT, col = c0 + e % kUpdColsT;
     rv[q] = make_cuDoubleComplex(0.0, 0.0);
-    if (e < NB * kUpdColsT && col < K) rv[q] = in[(size_t)K * col + pv[k]];
+    if (e < NB * kUpdColsT) {
+      const int pr = perm[j0 + k];
+      if (pr < 0 || pr >= K) bad = 1;
+      else if (col < K) rv[q] = in[(size_t)K * col + pr];
+    }
   }
 #pragma unroll
   for (int q = 0; q < kGI; ++q) {
     const int e = tid + 256 * q, k = e / kUpdRowsT, x = e % kUpdRowsT;
     if (e < NB * kUpdRowsT) {
-      if (r0 + x == pv[k]) gv[q].x -= 1.0;
+      if (r0 + x == pg[q]) gv[q].x -= 1.0;
       G[k][x] = gv[q];
     }
   }
@@ -410,7 +411,7 @@ __global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int
     const int e = tid + 256 * q;
     if (e < NB * kUpdColsT) R[e / kUpdColsT][e % kUpdColsT] = rv[q];
   }
-  __syncthreads();
+  if (__syncthreads_or(bad)) return;  // singular block: pivots incomplete, the caller fails
   if (row >= K) return;
   cuDoubleComplex g[NB];
 #pragma unroll
