@@ -300,8 +300,11 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
       perm[j0 + jj] = p;
       chosen[p] = 1;
     }
+    // Each row is kept rotated by jj columns: the pivot column of this step is a[.][0] and the
+    // next one a[.][1]; after the elimination the row rotates by one more column, so after NB
+    // steps it is back in order. The staged pivot row is rotated the same way.
     const cuDoubleComplex* prow = cand[par][w];
-    const cuDoubleComplex ap = prow[jj];
+    const cuDoubleComplex ap = prow[0];
     const double d = 1.0 / (ap.x * ap.x + ap.y * ap.y);
     const cuDoubleComplex inv = make_cuDoubleComplex(ap.x * d, -ap.y * d);
     best = -1.0;
@@ -309,30 +312,27 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
 #pragma unroll
     for (int r = 0; r < ROWS; ++r) {
       const int i = tid + r * kPanelThreads;
-      cuDoubleComplex f = a[r][0];
-#pragma unroll
-      for (int k = 1; k < NB; ++k)
-        if (k == jj) f = a[r][k];
       if (i == p) {
 #pragma unroll
-        for (int k = 0; k < NB; ++k) a[r][k] = k == jj ? inv : cmul(a[r][k], inv);
+        for (int k = 1; k < NB; ++k) a[r][k] = cmul(a[r][k], inv);
+        a[r][0] = inv;
       } else {
-        const cuDoubleComplex fi = cmul(f, inv);
+        const cuDoubleComplex fi = cmul(a[r][0], inv);
 #pragma unroll
-        for (int k = 0; k < NB; ++k)
-          a[r][k] = k == jj ? make_cuDoubleComplex(-fi.x, -fi.y) : cfms(fi, prow[k], a[r][k]);
+        for (int k = 1; k < NB; ++k) a[r][k] = cfms(fi, prow[k], a[r][k]);
+        a[r][0] = make_cuDoubleComplex(-fi.x, -fi.y);
       }
       if (jj + 1 < NB && i < K && i != p && !chosen[i]) {
-        cuDoubleComplex c = a[r][0];
-#pragma unroll
-        for (int k = 1; k < NB; ++k)
-          if (k == jj + 1) c = a[r][k];
-        const double cv = c.x * c.x + c.y * c.y;
+        const double cv = a[r][1].x * a[r][1].x + a[r][1].y * a[r][1].y;
         if (cv > best) {
           best = cv;
           bi = i;
         }
       }
+      const cuDoubleComplex first = a[r][0];
+#pragma unroll
+      for (int k = 0; k + 1 < NB; ++k) a[r][k] = a[r][k + 1];
+      a[r][NB - 1] = first;
     }
   }
 #pragma unroll
