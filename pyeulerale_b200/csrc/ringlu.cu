@@ -218,8 +218,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
                size_t off_perm, size_t off_info) {
   constexpr int kWarps = kPanelThreads / 32;
   __shared__ cuDoubleComplex cand[2][kWarps][NB];
-  __shared__ double cand_v[2][kWarps];
-  __shared__ int cand_i[2][kWarps];
+  __shared__ unsigned long long cand_key[2][kWarps];
   __shared__ unsigned char chosen[kMaxK];
   const cuDoubleComplex* in = at<cuDoubleComplex>(ws0, stride, off_in);
   cuDoubleComplex* out = at<cuDoubleComplex>(ws0, stride, off_out);
@@ -258,41 +257,40 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
 #pragma unroll 1
   for (int jj = 0; jj < NB; ++jj) {
     const int par = jj & 1;
+    // Arg-max as a max of 64-bit keys: the bits of |a|^2 (>= 0, so ordered like the values)
+    // with the low 10 mantissa bits replaced by 1023 - row, so equal (to 2^-42 relative) moduli
+    // go to the smaller row; 0 is "no candidate".
+    unsigned long long key =
+        bi < kMaxK ? (((unsigned long long)__double_as_longlong(best) & ~0x3FFull) |
+                      (unsigned long long)(kMaxK - 1 - bi))
+                   : 0ull;
+    const unsigned long long mine = key;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
-      }
+      const unsigned long long ok = __shfl_xor_sync(0xffffffffu, key, o);
+      key = ok > key ? ok : key;
     }
+    if (key != 0ull && mine == key) {  // this thread owns the warp's best row: stage it
+      const int wi = kMaxK - 1 - (int)(key & 0x3FFull);
 #pragma unroll
-    for (int r = 0; r < ROWS; ++r)
-      if (bi == tid + r * kPanelThreads) {
+      for (int r = 0; r < ROWS; ++r)
+        if (wi == tid + r * kPanelThreads) {
 #pragma unroll
-        for (int k = 0; k < NB; ++k) cand[par][warp][k] = a[r][k];
-      }
-    if (lane == 0) {
-      cand_v[par][warp] = best;
-      cand_i[par][warp] = bi;
+          for (int k = 0; k < NB; ++k) cand[par][warp][k] = a[r][k];
+        }
     }
+    if (lane == 0) cand_key[par][warp] = key;
     __syncthreads();
-    double v = lane < kWarps ? cand_v[par][lane] : -1.0;
-    int p = lane < kWarps ? cand_i[par][lane] : kMaxK;
-    int w = lane;
+    unsigned long long kb = lane < kWarps ? cand_key[par][lane] : 0ull;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, p, o);
-      const int ow = __shfl_xor_sync(0xffffffffu, w, o);
-      if (ov > v || (ov == v && oi < p)) {
-        v = ov;
-        p = oi;
-        w = ow;
-      }
+      const unsigned long long ok = __shfl_xor_sync(0xffffffffu, kb, o);
+      kb = ok > kb ? ok : kb;
     }
-    if (!(v > 0.0 && v <= 1.7e308 && p < K)) {  // the same decision in every thread
+    const int p = kMaxK - 1 - (int)(kb & 0x3FFull);
+    const int w = (p % kPanelThreads) / 32;  // the warp of the thread that owns row p
+    const double v = __longlong_as_double((long long)(kb & ~0x3FFull));
+    if (!(kb != 0ull && v > 0.0 && v <= 1.7e308 && p < K)) {  // the same decision in every thread
       if (tid == 0) atomicExch(info, 1);
       return;
     }
