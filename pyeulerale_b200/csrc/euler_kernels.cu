@@ -367,11 +367,15 @@ __global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, int64_t n_c
 
 // apply_odes_wrt_vertices_rev, f90:1044-1072, gathered per vertex (no wrap: the closing
 // vertex column n = N is distinct from n = 0, as in the reference).
-__global__ void __launch_bounds__(128) k_apply_vertices_rev(Table t, int64_t n_verts,
+__global__ void __launch_bounds__(256) k_apply_vertices_rev(Table t, int64_t n_verts,
                                                             const double* J, const double* w,
                                                             double* y) {
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_verts;
-       g += (int64_t)gridDim.x * blockDim.x) {
+  // Two threads per vertex: thread d computes component d from column d of each 4x2 block
+  // (32 contiguous bytes), which keeps the registers per thread low and many loads in flight.
+  for (int64_t gq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gq < 2 * n_verts;
+       gq += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = gq >> 1;
+    const int d = (int)(gq & 1);
     const Instance in = t.vert(g);
     const int M = in.M, N = in.N;
     const int64_t local = g - in.vert_offset;
@@ -383,36 +387,26 @@ __global__ void __launch_bounds__(128) k_apply_vertices_rev(Table t, int64_t n_v
     // FO of (m-1, n-1) and BO of (m-1, n).
     const int cm[4] = {m, m, m - 1, m - 1};
     const int cn[4] = {n, n - 1, n - 1, n};
-    C2 acc[2] = {{0, 0}, {0, 0}};
+    C2 acc = {0, 0};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (cm[k] < 0 || cm[k] >= M || cn[k] < 0 || cn[k] >= N) continue;
       const int64_t c = cm[k] + (int64_t)M * cn[k];
-      const double* bp = Ji + slot_stride * k + 8 * c;
-      double blk[8];
+      const double* col = Ji + slot_stride * k + 8 * c + 4 * d;
+      const double2 b01 = __ldg(reinterpret_cast<const double2*>(col));
+      const double2 b23 = __ldg(reinterpret_cast<const double2*>(col + 2));
+      const double bl[4] = {b01.x, b01.y, b23.x, b23.y};
+      double tr = 0.0, ti = 0.0;
 #pragma unroll
-      for (int e = 0; e < 8; e += 2) {
-        const double2 v = __ldg(reinterpret_cast<const double2*>(bp + e));
-        blk[e] = v.x;
-        blk[e + 1] = v.y;
+      for (int r = 0; r < 4; ++r) {
+        const C2 wv = ldc(wi + 8 * c + 2 * r);
+        tr += wv.re * bl[r];
+        ti += wv.im * bl[r];
       }
-      C2 wv[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) wv[r] = ldc(wi + 8 * c + 2 * r);
-#pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        double tr = 0.0, ti = 0.0;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          tr += wv[r].re * blk[r + 4 * d];
-          ti += wv[r].im * blk[r + 4 * d];
-        }
-        acc[d].re += tr;
-        acc[d].im += ti;
-      }
+      acc.re += tr;
+      acc.im += ti;
     }
-    stc(y + 4 * g, acc[0]);
-    stc(y + 4 * g + 2, acc[1]);
+    stc(y + 4 * g + 2 * d, acc);
   }
 }
 
@@ -781,7 +775,7 @@ int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const dou
   EB_VALIDATE(b);
   if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_vertices_rev<<<grid_for(b->n_verts, 128), 128, 0, EB_STREAM(stream)>>>(
+  k_apply_vertices_rev<<<grid_for(2 * b->n_verts, 256), 256, 0, EB_STREAM(stream)>>>(
       t, b->n_verts, J, d_odes, d_vertices);
   return check_launch("apply_odes_wrt_vertices_rev");
 }
