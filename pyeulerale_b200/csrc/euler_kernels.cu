@@ -431,18 +431,24 @@ __global__ void k_apply_mach_fwd(Table t, int64_t n_cells, const double* J, cons
 }
 
 // apply_odes_wrt_mach_rev, f90:632-650: one CTA per instance, warp-shuffle reduction.
-__global__ void __launch_bounds__(256) k_apply_mach_rev(Table t, const double* J,
+__global__ void __launch_bounds__(512) k_apply_mach_rev(Table t, const double* J,
                                                         const double* w, double* dm) {
   const Instance in = t.dev ? t.dev[blockIdx.x] : t.single;
   const int64_t cells = (int64_t)in.M * in.N;
   double sr = 0.0, si = 0.0;
+  // 16-byte loads, and the cell loop unrolled so that several cells' loads are in flight
+#pragma unroll 4
   for (int64_t c = threadIdx.x; c < cells; c += blockDim.x) {
     const int64_t g = in.cell_offset + c;
+    const double2 j01 = __ldg(reinterpret_cast<const double2*>(J + 4 * g));
+    const double2 j23 = __ldg(reinterpret_cast<const double2*>(J + 4 * g + 2));
+    const double jr[4] = {j01.x, j01.y, j23.x, j23.y};
     double tr = 0.0, ti = 0.0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      tr += w[8 * g + 2 * r] * J[4 * g + r];
-      ti += w[8 * g + 2 * r + 1] * J[4 * g + r];
+      const double2 wv = __ldg(reinterpret_cast<const double2*>(w + 8 * g + 2 * r));
+      tr += wv.x * jr[r];
+      ti += wv.y * jr[r];
     }
     sr += tr;
     si += ti;
@@ -452,7 +458,7 @@ __global__ void __launch_bounds__(256) k_apply_mach_rev(Table t, const double* J
     sr += __shfl_xor_sync(0xffffffffu, sr, o);
     si += __shfl_xor_sync(0xffffffffu, si, o);
   }
-  __shared__ double red[2][8];
+  __shared__ double red[2][16];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane == 0) {
     red[0][warp] = sr;
@@ -736,7 +742,7 @@ int eb_apply_odes_wrt_mach_rev(const eb_batch* b, const double* J, const double*
   EB_VALIDATE(b);
   if (!J || !d_mach || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_mach_rev<<<b->n_inst, 256, 0, EB_STREAM(stream)>>>(t, J, d_odes, d_mach);
+  k_apply_mach_rev<<<b->n_inst, 512, 0, EB_STREAM(stream)>>>(t, J, d_odes, d_mach);
   return check_launch("apply_odes_wrt_mach_rev");
 }
 
