@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
 constexpr int kUpdRowsT = 64;
 constexpr int kUpdColsT = 32;
 template <int NB>
-__global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int64_t stride,
+__global__ void __launch_bounds__(256, 3) k_gj_update(int K, int j0, char* ws0, int64_t stride,
                                                    size_t off_in, size_t off_out, size_t off_perm,
                                                    size_t off_info) {
   constexpr int kPer = kUpdRowsT * kUpdColsT / 256;  // outputs per thread
@@ -411,16 +411,18 @@ __global__ void __launch_bounds__(256) k_gj_update(int K, int j0, char* ws0, int
   }
   if (__syncthreads_or(bad)) return;  // singular block: pivots incomplete, the caller fails
   if (row >= K) return;
-  cuDoubleComplex g[NB];
+  // k outside the columns: one G value live at a time (few registers, more resident CTAs);
+  // every output still sums k = 0 .. NB-1 in order
 #pragma unroll
-  for (int k = 0; k < NB; ++k) g[k] = G[k][r];
+  for (int k = 0; k < NB; ++k) {
+    const cuDoubleComplex g = G[k][r];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) acc[q] = cfma(g, R[k][cb + 4 * q], acc[q]);
+  }
 #pragma unroll
   for (int q = 0; q < kPer; ++q) {
-    const int c = cb + 4 * q, col = c0 + c;
-    if (col >= K || (col >= j0 && col < j0 + NB)) continue;
-#pragma unroll
-    for (int k = 0; k < NB; ++k) acc[q] = cfma(g[k], R[k][c], acc[q]);
-    out[(size_t)K * col + row] = acc[q];
+    const int col = c0 + cb + 4 * q;
+    if (col < K && !(col >= j0 && col < j0 + NB)) out[(size_t)K * col + row] = acc[q];
   }
 }
 
