@@ -12,9 +12,9 @@
 //     is the max_c of the sensors centred on its two cells, f90:208-211; the wall and
 //     far-field rows use their ghost states as the missing neighbour);
 //  4. each face is evaluated once for its two cells: the reference evaluates it twice, once in
-//     each cell's orientation, and the two evaluations share the central and ALE parts exactly
-//     (negated); the asymmetric max_c decisions (f90:111-120) and the fourth-difference
-//     evaluation order are taken per orientation. Faces whose two evaluations use different
+//     each cell's orientation, and the two evaluations share the central and ALE parts and the
+//     differences (negated), which are formed once; the asymmetric max_c decisions
+//     (f90:111-120) are taken per orientation. Faces whose two evaluations use different
 //     stencils (next to the wall and the far field, f90:401-436) are evaluated per cell. Each
 //     cell then writes -(F_b + F_f + F_i + F_o) / area (f90:370-436).
 // Results agree with the reference to the rounding of the reordered arithmetic (<= 1e-12
@@ -133,10 +133,12 @@ __device__ __forceinline__ Flux jst(const St& ll, const St& l, const St& r, cons
 }
 
 // Both orientations of one JST face: F = make_face_flux(ll, l, r, rr, n) for the cell l and
-// F' = make_face_flux(rr, r, l, ll, -n) for the cell r (f90:189-220). The central and ALE parts
-// of F' are the exact negatives of F's; the orientations differ in the asymmetric max_c
-// decisions (spectral radius and sensor) and in the evaluation order of the fourth difference,
-// which are evaluated per orientation as the reference does.
+// F' = make_face_flux(rr, r, l, ll, -n) for the cell r (f90:189-220). Mathematically F' shares
+// F's central and ALE parts and its first and third differences, all negated; the orientations
+// differ only in the asymmetric max_c decisions (spectral radius and sensor), which are taken per
+// orientation as the reference takes them. The shared parts are formed once: the central flux
+// minus the grid-velocity flux as (F(l) + F(r)) . n / 2 - (l + r) vn / 2 with the face-relative
+// normal velocities vl - vn and vr - vn, and the third difference in F's orientation.
 __device__ __forceinline__ void jst_pair(const St& ll, const St& l, const St& r, const St& rr,
                                          double nx, double nz, double len, double vn, double sl,
                                          double sr, const Instance& in, Flux& F, Flux& Fp) {
@@ -150,19 +152,19 @@ __device__ __forceinline__ void jst_pair(const St& ll, const St& l, const St& r,
   const double c4p = in.k4 * lamp - in.c4 * coef2p;
   const double coef4 = (0.0 > c4 + 1e-8) ? 0.0 : c4;
   const double coef4p = (0.0 > c4p + 1e-8) ? 0.0 : c4p;
+  const double wl = vl - vn, wr = vr - vn, ps = l.p + r.p;
+  const double ca[4] = {0.5 * fma(l.rho, wl, r.rho * wr),
+                        0.5 * fma(l.j1, wl, fma(r.j1, wr, nx * ps)),
+                        0.5 * fma(l.j2, wl, fma(r.j2, wr, nz * ps)),
+                        0.5 * fma(l.e, wl, fma(r.e, wr, fma(l.p, vl, r.p * vr)))};
   const double lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
   const double llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
-  const double fl[4] = {l.rho * vl, l.j1 * vl + nx * l.p, l.j2 * vl + nz * l.p, (l.e + l.p) * vl};
-  const double fr[4] = {r.rho * vr, r.j1 * vr + nx * r.p, r.j2 * vr + nz * r.p, (r.e + r.p) * vr};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const double c = (fl[k] + fr[k]) / 2.0;
     const double d1 = rv[k] - lv[k];
-    const double d3 = rrv[k] - 3.0 * rv[k] + 3.0 * lv[k] - llv[k];
-    const double d3p = llv[k] - 3.0 * lv[k] + 3.0 * rv[k] - rrv[k];
-    const double a = (lv[k] + rv[k]) / 2.0 * vn;
-    F.f[k] = (c - (coef2 * d1 - coef4 * d3)) - a;
-    Fp.f[k] = (-c - (coef2p * -d1 - coef4p * d3p)) + a;
+    const double d3 = fma(3.0, lv[k], fma(-3.0, rv[k], rrv[k])) - llv[k];
+    F.f[k] = fma(coef4, d3, fma(-coef2, d1, ca[k]));
+    Fp.f[k] = fma(-coef4p, d3, fma(coef2p, d1, -ca[k]));
   }
 }
 
