@@ -10,10 +10,12 @@ table.
 
 One timed "step" is one residual evaluation R(Ma, U, X, V) of the whole batch (one launch).
 The JSON line reports cell-residual evaluations per second (``value``), and beside it the VJP
-rate (full set of reverse products per instance: d/dU, d/dX, d/dV, d/dMa) and the resolvent
-rate: the pitch frequency response (64 shifts) plus the adjoint lift gradient of the PTC steady
-state of one instance, solved to 1e-10 relative residual, with the shifts factored together
-(batched) and one at a time through the drop-in class (plain).
+rate (full set of reverse products per instance: d/dU, d/dX, d/dV, d/dMa), the linearisation
+rates (the d(odes)/d(states) Jacobian, the matrix-free tangent, the forward products, the
+shifted BSR SpMV) and the resolvent rate: the pitch frequency response (64 shifts) plus the
+adjoint lift gradient of the PTC steady state of one instance, solved to 1e-10 relative
+residual, with the shifts factored together (batched) and one at a time through the drop-in
+class (plain).
 
 ``--impl reference`` times the CPU restatement of the reference (complex arithmetic, all host
 threads) on a bounded sample of the same workload. Under torchrun every rank processes its own
@@ -41,6 +43,14 @@ METRIC = "cell-residual evals/s; VJP/s; batched resolvent solves/s vs plain at 1
 UNIT = "cell-residual evals/s"
 BYTES_PER_CELL_RESIDUAL = 96          # U 32 + X 16 + V 16 + R 32 (FP64)
 BYTES_PER_CELL_VJP = 1152 + 256 + 256 + 32 + 4 * 64 + 64 + 2 * 32 + 8
+BYTES_PER_CELL_JAC_STATES = 32 + 16 + 16 + 1152   # U, X, V in; nine 4x4 blocks out
+# U, X, V, complex dU, dX, dV in; complex dR out
+BYTES_PER_CELL_TANGENT = 32 + 16 + 16 + 64 + 32 + 32 + 64
+# per product: Jacobian + complex direction in, complex d_odes out (states 1152 + 64 + 64,
+# vertices and velocities 256 + 32 + 64 each, Mach 32 + 64)
+BYTES_PER_CELL_JVP = 1280 + 2 * 352 + 96
+LINEAR_SPMV_INSTANCES = 16          # BSR matrices cycled by the SpMV timing (~343 MB)
+SPMV_STREAMS = 4                    # streams the captured SpMVs are spread over
 GRID = dict(radial_pts=129, angular_pts=129, thickness=0.04, chord=10.0, far_radius=200.0,
             first_spacing=0.1)
 FLOW = dict(mach=0.5, aoa_deg=0.0, center=(2.5, 0.0))
@@ -58,9 +68,9 @@ def parse_args():
                    help="frequency-response shifts timed one at a time (plain path)")
     p.add_argument("--batched-shifts", type=int, default=64,
                    help="frequency-response shifts timed through the batched driver")
-    p.add_argument("--parts", default="residual,vjp,resolvent,uneven",
+    p.add_argument("--parts", default="residual,vjp,linear,resolvent,uneven",
                    help="comma-separated parts to run besides the residual "
-                        "(vjp, resolvent, uneven)")
+                        "(vjp, linear, resolvent, uneven)")
     p.add_argument("--uneven-instances", type=int, default=48)
     p.add_argument("--uneven-sizes", default="65,129",
                    help="grid point counts (n x n O-grids) the uneven instances draw from")
@@ -156,6 +166,16 @@ class ClockSampler:
 
 # ---- CPU baseline (the oracle) --------------------------------------------------------------
 
+def cpu_model() -> str:
+    """The host CPU's model name and logical core count (Linux /proc/cpuinfo)."""
+    try:
+        names = [ln.split(":", 1)[1].strip() for ln in open("/proc/cpuinfo")
+                 if ln.startswith("model name")]
+        return f"{names[0]} ({len(names)} logical cores)" if names else "unknown"
+    except OSError:
+        return "unknown"
+
+
 def cpu_residual_rate(X, V, Us, threads: int, budget_s: float) -> tuple[float, str]:
     """Cells/s of the complex-arithmetic oracle residual on a bounded sample."""
     from oracle.shim import SpatialDiscretizationModule, load_library
@@ -202,12 +222,13 @@ def run_reference(args) -> None:
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * 129 * 129 / value, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * 128 * 128 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded NACA-0004 O-grid)",
         "config": {"workload": "residual of the 129x129 NACA-0004 O-grid (128x128 cells), "
                                "Ma 0.5, alpha 0, complex arithmetic as the reference",
                    "cells_per_instance": 128 * 128},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "cpu": cpu_model(),
                          "sample": f"per step: {sample}; C++ restatement of "
                                    "src/spatial_discretization.f90 (oracle/sd_oracle.cpp)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -373,6 +394,117 @@ def run_b200(args) -> None:
         vjp_gbs = BYTES_PER_CELL_VJP * cells * vsteps / t_vjp / 1e9
         del J_u, J_x, J_v, J_m
 
+    # linearisation: the 4x4-block Jacobian d(odes)/d(states) of every instance, the
+    # matrix-free forward tangent (complex dU, dX, dV, dMa in one stencil pass) of every
+    # instance, and the shifted BSR SpMV (A - s I) x cycled over the BSR forms of
+    # LINEAR_SPMV_INSTANCES instances (more bytes than L2 holds, so every pass reads HBM)
+    linear = None
+    if "linear" in parts:
+        def per_call(fn, n):
+            for _ in range(args.warmup):
+                fn()
+            barrier()
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(n):
+                fn()
+            z.record(stream)
+            barrier()
+            return max_over_ranks(a.elapsed_time(z) / 1e3) / n
+
+        J_u = torch.empty(144 * cells, **f64)
+        t_jac = per_call(lambda: inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u,
+                                           stream=sp), 5)
+        gen = torch.Generator(device="cuda").manual_seed(77 + rank)
+        tU = torch.randn(8 * cells, generator=gen, **f64)
+        tX = torch.randn(4 * inst.n_verts, generator=gen, **f64)
+        tV = torch.randn(4 * inst.n_verts, generator=gen, **f64)
+        tM = torch.randn(2 * B, generator=gen, **f64)
+        tR = torch.empty(8 * cells, **f64)
+        t_tan = per_call(lambda: inst.call("eb_apply_odes_tangent", dX, dV, dU, tU, tX, tV, tM,
+                                           tR, None, stream=sp), max(5, args.steps // 4))
+        # JVP set: the four forward products with stored Jacobians, each into its own d_odes
+        J_x = torch.empty(32 * cells, **f64)
+        J_v = torch.empty(32 * cells, **f64)
+        J_m = torch.empty(4 * cells, **f64)
+        inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, J_x, stream=sp)
+        inst.call("eb_compute_odes_wrt_velocities", dX, dV, dU, J_v, stream=sp)
+        inst.call("eb_compute_odes_wrt_mach", dX, dV, dU, J_m, stream=sp)
+        jR = [torch.empty(8 * cells, **f64) for _ in range(4)]
+
+        def jvp():
+            inst.call("eb_apply_odes_wrt_states_fwd", J_u, tU, jR[0], stream=sp)
+            inst.call("eb_apply_odes_wrt_vertices_fwd", J_x, tX, jR[1], stream=sp)
+            inst.call("eb_apply_odes_wrt_vertices_fwd", J_v, tV, jR[2], stream=sp)
+            inst.call("eb_apply_odes_wrt_mach_fwd", J_m, tM, jR[3], stream=sp)
+
+        t_jvp = per_call(jvp, max(5, args.steps // 4))
+        del J_x, J_v, J_m, jR
+        M1, N1 = specs[0].M, specs[0].N
+        rows, nnzb = M1 * N1, (9 * M1 - 6) * N1
+        one = InstanceSet(specs[:1])
+        n_mat = min(LINEAR_SPMV_INSTANCES, B)
+        mats = []
+        for i in range(n_mat):
+            data = torch.empty(16 * nnzb, **f64)
+            idx = torch.empty(nnzb, dtype=torch.int32, device="cuda")
+            ptr = torch.empty(rows + 1, dtype=torch.int32, device="cuda")
+            one.call("eb_convert_odes_wrt_states", J_u[144 * inst.cell_offsets[i]:], data, idx,
+                     ptr, stream=sp)
+            mats.append((data, idx, ptr))
+        sx = torch.randn(8 * rows * n_mat, generator=gen, **f64)
+        sy = torch.empty(8 * rows * n_mat, **f64)
+
+        def spmv_all(st):
+            for i, (data, idx, ptr) in enumerate(mats):
+                _lib.call("eb_bsr_shifted_spmv", rows, data.data_ptr(), idx.data_ptr(),
+                          ptr.data_ptr(), 0.0, 1.5, sx[8 * rows * i:].data_ptr(),
+                          sy[8 * rows * i:].data_ptr(), st)
+
+        # one SpMV moves ~21 MB (~4 us of HBM time), less than the host needs to issue a call
+        # and about one launch's ramp and tail: the n_mat independent calls are captured once
+        # in a CUDA graph, spread over SPMV_STREAMS streams so that their launches overlap,
+        # and the graph is replayed
+        spmv_all(sp)
+        barrier()
+        spmv_graph = torch.cuda.CUDAGraph()
+        side = [torch.cuda.Stream() for _ in range(SPMV_STREAMS)]
+        with torch.cuda.graph(spmv_graph):
+            cap = torch.cuda.current_stream()
+            for k, s in enumerate(side):
+                s.wait_stream(cap)
+                with torch.cuda.stream(s):
+                    for i in range(k, n_mat, SPMV_STREAMS):
+                        data, idx, ptr = mats[i]
+                        _lib.call("eb_bsr_shifted_spmv", rows, data.data_ptr(),
+                                  idx.data_ptr(), ptr.data_ptr(), 0.0, 1.5,
+                                  sx[8 * rows * i:].data_ptr(), sy[8 * rows * i:].data_ptr(),
+                                  s.cuda_stream)
+            for s in side:
+                cap.wait_stream(s)
+        t_spmv = per_call(spmv_graph.replay, max(5, args.steps // 4)) / n_mat
+        spmv_bytes = nnzb * (128 + 4) + (rows + 1) * 4 + rows * (64 + 64)
+        linear = {
+            "jacobian_states": {"value": world * cells / t_jac, "unit": "cells/s",
+                                "achieved_gbs": BYTES_PER_CELL_JAC_STATES * cells / t_jac / 1e9,
+                                "bytes_per_cell": BYTES_PER_CELL_JAC_STATES},
+            "tangent": {"value": world * cells / t_tan, "unit": "cells/s",
+                        "achieved_gbs": BYTES_PER_CELL_TANGENT * cells / t_tan / 1e9,
+                        "bytes_per_cell": BYTES_PER_CELL_TANGENT,
+                        "direction": "complex dU, dX, dV, dMa together"},
+            "jvp": {"value": world * B / t_jvp,
+                    "unit": "JVP/s (dR/dU, dR/dX, dR/dV, dR/dMa forward products per instance)",
+                    "achieved_gbs": BYTES_PER_CELL_JVP * cells / t_jvp / 1e9,
+                    "bytes_per_cell": BYTES_PER_CELL_JVP, "launches_per_jvp_batch": 4},
+            "bsr_spmv": {"value": world / t_spmv, "unit": "SpMV/s (one 128x128 instance)",
+                         "achieved_gbs": spmv_bytes / t_spmv / 1e9,
+                         "bytes_per_spmv": spmv_bytes, "nnzb": nnzb,
+                         "matrices_cycled": n_mat,
+                         "issue": f"the {n_mat} calls captured in one CUDA graph on "
+                                  f"{SPMV_STREAMS} streams, replayed"},
+            "peak_gbs": peak}
+        del J_u, tU, tX, tV, tR, mats, sx, sy, spmv_graph, side
+
     # resolvent: the frequency response of the steady state (PTC from free stream), 64 shifts
     # s = i k V / (c / 2), k log-spaced on [0.01, 10], plus the adjoint lift gradient; batched
     # (shift_group shifts per factorisation call) against one shift at a time through the
@@ -488,7 +620,7 @@ def run_b200(args) -> None:
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         rate, sample = cpu_residual_rate(X, V, Us[:4], 1, args.cpu_seconds)
-        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "cpu": cpu_model(),
                "sample": f"{sample}; single-threaded like the reference; C++ restatement "
                          "of src/spatial_discretization.f90 in complex arithmetic"}
     if world > 1:
@@ -523,6 +655,7 @@ def run_b200(args) -> None:
         "vjp": None if vjp_rate is None else {
             "value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
             "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4},
+        "linear": linear,
         "resolvent": res,
         "uneven": uneven,
     }

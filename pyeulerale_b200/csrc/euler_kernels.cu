@@ -127,37 +127,72 @@ __global__ void __launch_bounds__(128) k_residual(Table t, int64_t n_cells, cons
   }
 }
 
-// Matrix-free forward tangent with a complex direction on every input: Dual<double, 2>
-// carries (Re, Im) of the direction.
+// Matrix-free forward tangent with a complex direction on every input, two threads per cell:
+// thread h of a cell (h = 0: real part, 1: imaginary part of the direction) evaluates make_ode
+// in one-component duals (Dual<double, 1>) seeded with its part. The stencil states are read
+// face by face through a provider (the repeated reads hit L1), so only one face's operands are
+// live at a time; holding the whole nine-state stencil as duals in registers spilled kilobytes
+// per thread.
+using D1 = Dual<double, 1>;
+
+struct TangentStates {
+  const double* U;   // the instance's states
+  const double* dU;  // the instance's complex state direction, or nullptr
+  int M, N, m, n, h;
+  __device__ __forceinline__ S4<D1> operator()(int s) const {
+    const int64_t j = (m + slot_dm(s)) + (int64_t)M * wrap(n + slot_dn(s), N);
+    const S4<double> u = ld4(U + 4 * j);
+    S4<D1> r;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      r.v[k].v = u.v[k];
+      r.v[k].d[0] = dU ? __ldg(dU + 8 * j + 2 * k + h) : 0.0;
+    }
+    return r;
+  }
+};
+
+__device__ __forceinline__ P2<D1> tangent_point(const double* P, const double* dP, int64_t v,
+                                                int h) {
+  P2<D1> r;
+  const P2<double> x = P ? ld2(P + 2 * v) : P2<double>{0.0, 0.0};
+  r.x.v = x.x;
+  r.z.v = x.z;
+  r.x.d[0] = dP ? __ldg(dP + 4 * v + h) : 0.0;
+  r.z.d[0] = dP ? __ldg(dP + 4 * v + 2 + h) : 0.0;
+  return r;
+}
+
 __global__ void __launch_bounds__(128) k_tangent(Table t, int64_t n_cells, const double* X,
                                                  const double* V, const double* U,
                                                  const double* dU, const double* dX,
                                                  const double* dV, const double* dMa,
                                                  double* dR, double* R) {
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t gq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gq < 2 * n_cells;
+       gq += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = gq >> 1;
+    const int h = (int)(gq & 1);
     const Instance in = t.cell(g);
+    const int M = in.M, N = in.N;
     const int64_t local = g - in.cell_offset;
-    Plain p;
-    load_plain(in, local, X, V, U, p);
-    Direction du, dx, dv;
-    if (dU) load_direction(in, p, kDirStates, dU, du);
-    if (dX) load_direction(in, p, kDirVertices, dX, dx);
-    if (dV) load_direction(in, p, kDirVelocities, dV, dv);
-    Cell<D2, D2, D2, D2> c;
+    const int m = (int)(local % M), n = (int)(local / M);
+    const int flag = boundary_flag(M, m);
+    const int64_t v_bi = m + (int64_t)(M + 1) * n, v_fi = m + (int64_t)(M + 1) * (n + 1);
+    const int64_t corner[4] = {v_bi, v_fi, v_fi + 1, v_bi + 1};  // kBI, kFI, kFO, kBO
+    const double* Xi = X + 2 * in.vert_offset;
+    const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
+    const double* dXi = dX ? dX + 4 * in.vert_offset : nullptr;
+    const double* dVi = dV ? dV + 4 * in.vert_offset : nullptr;
+    P2<D1> x[4], w[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      c.x[k].x = bval<D2>(p.x[k].x, dX ? dx.xr[k].x : 0.0, dX ? dx.xi[k].x : 0.0);
-      c.x[k].z = bval<D2>(p.x[k].z, dX ? dx.xr[k].z : 0.0, dX ? dx.xi[k].z : 0.0);
-      c.w[k].x = bval<D2>(p.w[k].x, dV ? dv.xr[k].x : 0.0, dV ? dv.xi[k].x : 0.0);
-      c.w[k].z = bval<D2>(p.w[k].z, dV ? dv.xr[k].z : 0.0, dV ? dv.xi[k].z : 0.0);
+      x[k] = tangent_point(Xi, dXi, corner[k], h);
+      w[k] = tangent_point(Vi, dVi, corner[k], h);
     }
-#pragma unroll
-    for (int s = 0; s < 9; ++s)
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        c.u[s].v[k] = bval<D2>(p.u[s].v[k], dU ? du.ur[s].v[k] : 0.0, dU ? du.ui[s].v[k] : 0.0);
-    double mre = 0.0, mim = 0.0;
+    const Geometry<D1, D1> geo = geometry(x, w);
+    D1 mach;
+    mach.v = in.mach;
+    mach.d[0] = 0.0;
     if (dMa) {
       // one complex per instance; the instance index is the table position
       int lo = 0;
@@ -168,21 +203,24 @@ __global__ void __launch_bounds__(128) k_tangent(Table t, int64_t n_cells, const
           if (t.dev[mid].cell_offset <= g) lo = mid; else hi = mid - 1;
         }
       }
-      mre = dMa[2 * lo];
-      mim = dMa[2 * lo + 1];
+      mach.d[0] = dMa[2 * lo + h];
     }
-    c.mach = bval<D2>(in.mach, mre, mim);
-    c.flag = p.flag;
-    const S4<D2> o = make_ode(c, in);
-    double* out = dR + 8 * g;
+    const TangentStates u{U + 4 * in.cell_offset, dU ? dU + 8 * in.cell_offset : nullptr,
+                          M, N, m, n, h};
+    // -(((F_b + F_f) + F_i) + F_o) / area, the order of make_ode
+    S4<D1> acc = face<D1>(kFaceB, flag, u, geo, mach, in);
+    const S4<D1> ff = face<D1>(kFaceF, flag, u, geo, mach, in);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc.v[k] = acc.v[k] + ff.v[k];
+    const S4<D1> fi = face<D1>(kFaceI, flag, u, geo, mach, in);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc.v[k] = acc.v[k] + fi.v[k];
+    const S4<D1> fo = face<D1>(kFaceO, flag, u, geo, mach, in);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      out[2 * k] = o.v[k].d[0];
-      out[2 * k + 1] = o.v[k].d[1];
-    }
-    if (R) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) R[4 * g + k] = o.v[k].v;
+      const D1 o = -(acc.v[k] + fo.v[k]) / geo.area;
+      dR[8 * g + 2 * k + h] = o.d[0];
+      if (R && h == 0) R[4 * g + k] = o.v;
     }
   }
 }
@@ -241,52 +279,60 @@ __global__ void __launch_bounds__(256) k_forces(Table t, const double* X, const 
 
 // ---- Jacobian products -------------------------------------------------------------------
 
-// apply_odes_wrt_states_fwd, f90:825-864: y_c = sum_s J_s(c) x_nb(c,s) in the reference's
-// order (c, b, bb, f, ff, then ii, i, oo, o).
-__global__ void __launch_bounds__(128) k_apply_states_fwd(Table t, int64_t n_cells,
-                                                          const double* J, const double* x,
-                                                          double* y) {
-  const int order[9] = {kC, kB, kBB, kF, kFF, kII, kI, kOO, kO};
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    const Instance in = t.cell(g);
-    const int M = in.M, N = in.N;
-    const int64_t local = g - in.cell_offset;
-    const int m = (int)(local % M), n = (int)(local / M);
-    const int64_t slot_stride = 16 * (int64_t)M * N;
-    const double* Jc = J + 144 * in.cell_offset + 16 * local;
-    const double* xi = x + 8 * in.cell_offset;
-    C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+// apply_odes_wrt_states_fwd, f90:825-864: y_c = sum_s J_s(c) x_nb(c,s), with four threads per
+// output cell. Thread i takes column i of each of the cell's 4x4 blocks (32 contiguous bytes;
+// the four threads of a cell read a block's 128 bytes together, the eight cells of a warp 1 KB)
+// and component i of the neighbour's state, and accumulates all four rows; two shuffle steps
+// add the four columns' sums and thread i writes row i. Each column's products are summed over
+// the slots before the columns are added (the reference sums each block's product row by row),
+// a reordering at the rounding level. The loop runs per warp so that every lane reaches the
+// shuffles.
+__global__ void __launch_bounds__(256) k_apply_states_fwd4(Table t, int64_t n_cells,
+                                                           const double* J, const double* x,
+                                                           double* y) {
+  const int i = threadIdx.x & 3;
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t wq = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wq * 8 < n_cells;
+       wq += n_warps) {
+    const int64_t g = 8 * wq + ((threadIdx.x & 31) >> 2);
+    const bool live = g < n_cells;
+    double ar[4] = {0.0, 0.0, 0.0, 0.0}, ai[4] = {0.0, 0.0, 0.0, 0.0};
+    if (live) {
+      const Instance in = t.cell(g);
+      const int M = in.M, N = in.N;
+      const int64_t local = g - in.cell_offset;
+      const int m = (int)(local % M), n = (int)(local / M);
+      const int64_t slot_stride = 16 * (int64_t)M * N;
+      const double* Jc = J + 144 * in.cell_offset + 16 * local + 4 * i;
+      const double* xi = x + 8 * in.cell_offset + 2 * i;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const int s = order[q];
-      if (!slot_active(s, m, M)) continue;
-      const double* blk = Jc + slot_stride * s;
-      const int64_t j = (m + slot_dm(s)) + (int64_t)M * wrap(n + slot_dn(s), N);
-      C2 xv[4];
+      for (int s = 0; s < 9; ++s) {
+        if (!slot_active(s, m, M)) continue;
+        const int64_t j = (m + slot_dm(s)) + (int64_t)M * wrap(n + slot_dn(s), N);
+        const double2 b01 = __ldg(reinterpret_cast<const double2*>(Jc + slot_stride * s));
+        const double2 b23 = __ldg(reinterpret_cast<const double2*>(Jc + slot_stride * s + 2));
+        const C2 xv = ldc(xi + 8 * j);
+        const double bl[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
-      for (int i = 0; i < 4; ++i) xv[i] = ldc(xi + 8 * j + 2 * i);
-      double bl[16];
-#pragma unroll
-      for (int e = 0; e < 16; e += 2) {
-        const double2 v = *reinterpret_cast<const double2*>(blk + e);
-        bl[e] = v.x;
-        bl[e + 1] = v.y;
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        double tr = 0.0, ti = 0.0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          tr += bl[r + 4 * i] * xv[i].re;
-          ti += bl[r + 4 * i] * xv[i].im;
+        for (int r = 0; r < 4; ++r) {
+          ar[r] = fma(bl[r], xv.re, ar[r]);
+          ai[r] = fma(bl[r], xv.im, ai[r]);
         }
-        acc[r].re += tr;
-        acc[r].im += ti;
       }
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) stc(y + 8 * g + 2 * r, acc[r]);
+    for (int o = 1; o <= 2; o <<= 1)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        ar[r] += __shfl_xor_sync(0xffffffffu, ar[r], o);
+        ai[r] += __shfl_xor_sync(0xffffffffu, ai[r], o);
+      }
+    if (live) {
+      const C2 out = i == 0 ? C2{ar[0], ai[0]}
+                   : i == 1 ? C2{ar[1], ai[1]}
+                   : i == 2 ? C2{ar[2], ai[2]} : C2{ar[3], ai[3]};
+      stc(y + 8 * g + 2 * i, out);
+    }
   }
 }
 
@@ -627,32 +673,70 @@ __global__ void k_convert_bsr(int M, int N, const double* J, double* data, int32
   }
 }
 
-// y = (A - shift I) x for a BSR matrix with 1-based indices (complex x, y).
-__global__ void k_bsr_spmv(int64_t rows, const double* data, const int32_t* indices,
-                           const int32_t* indptr, double sr, double si, const double* x,
-                           double* y) {
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-    for (int32_t p = indptr[r] - 1; p < indptr[r + 1] - 1; ++p) {
-      const double* blk = data + 16 * (int64_t)p;
-      const int64_t c = indices[p] - 1;
+// y = (A - shift I) x for a BSR matrix with 1-based indices (complex x, y). Eight threads per
+// block row: thread l of a row loads the 16-byte pair (2l, 2l + 1) of each 4x4 block (column
+// l / 2, rows 2 (l % 2) and 2 (l % 2) + 1, the blocks being column-major), so the eight threads
+// read a block's 128 bytes in one coalesced access, and multiplies it by component l / 2 of
+// the block column's x; shuffles over the four threads with the same row pair add the columns,
+// and threads 0 and 1 of the row write rows 0-1 and 2-3. The loop runs per warp (four rows)
+// so that every lane reaches the shuffles.
+__global__ void __launch_bounds__(256) k_bsr_spmv(int64_t rows, const double* data,
+                                                  const int32_t* indices, const int32_t* indptr,
+                                                  double sr, double si, const double* x,
+                                                  double* y) {
+  const int l = threadIdx.x & 7;
+  const int col = l >> 1, q0 = 2 * (l & 1);
+  const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t wq = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wq * 4 < rows;
+       wq += n_warps) {
+    const int64_t r = 4 * wq + ((threadIdx.x & 31) >> 3);
+    const bool live = r < rows;
+    double a0r = 0.0, a0i = 0.0, a1r = 0.0, a1i = 0.0;
+    const int32_t p0 = live ? indptr[r] - 1 : 0, p1 = live ? indptr[r + 1] - 1 : 0;
+    // The first kRowBlocks blocks of the row (all of them for the nine-point stencil pattern):
+    // every index, block and x load is issued before the products, so the row costs one
+    // dependent load chain instead of one per block.
+    constexpr int kRowBlocks = 9;
+    double2 b[kRowBlocks], xv[kRowBlocks];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const C2 xv = ldc(x + 8 * c + 2 * i);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          acc[q].re += blk[q + 4 * i] * xv.re;
-          acc[q].im += blk[q + 4 * i] * xv.im;
-        }
-      }
+    for (int k = 0; k < kRowBlocks; ++k) {
+      const int32_t p = p0 + k;
+      const bool ok = p < p1;
+      const int64_t c = ok ? __ldg(indices + p) - 1 : 0;
+      b[k] = ok ? __ldg(reinterpret_cast<const double2*>(data + 16 * (int64_t)p) + l)
+                : make_double2(0.0, 0.0);
+      xv[k] = ok ? __ldg(reinterpret_cast<const double2*>(x + 8 * c + 2 * col))
+                 : make_double2(0.0, 0.0);
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const C2 xv = ldc(x + 8 * r + 2 * q);
-      acc[q].re -= sr * xv.re - si * xv.im;
-      acc[q].im -= sr * xv.im + si * xv.re;
-      stc(y + 8 * r + 2 * q, acc[q]);
+    for (int k = 0; k < kRowBlocks; ++k) {
+      a0r = fma(b[k].x, xv[k].x, a0r);
+      a0i = fma(b[k].x, xv[k].y, a0i);
+      a1r = fma(b[k].y, xv[k].x, a1r);
+      a1i = fma(b[k].y, xv[k].y, a1i);
+    }
+    for (int32_t p = p0 + kRowBlocks; p < p1; ++p) {  // longer rows of a general BSR matrix
+      const double2 bp = __ldg(reinterpret_cast<const double2*>(data + 16 * (int64_t)p) + l);
+      const int64_t c = __ldg(indices + p) - 1;
+      const double2 xp = __ldg(reinterpret_cast<const double2*>(x + 8 * c + 2 * col));
+      a0r = fma(bp.x, xp.x, a0r);
+      a0i = fma(bp.x, xp.y, a0i);
+      a1r = fma(bp.y, xp.x, a1r);
+      a1i = fma(bp.y, xp.y, a1i);
+    }
+#pragma unroll
+    for (int o = 2; o <= 4; o <<= 1) {
+      a0r += __shfl_xor_sync(0xffffffffu, a0r, o);
+      a0i += __shfl_xor_sync(0xffffffffu, a0i, o);
+      a1r += __shfl_xor_sync(0xffffffffu, a1r, o);
+      a1i += __shfl_xor_sync(0xffffffffu, a1i, o);
+    }
+    if (live && col == 0) {
+      const double2* xr = reinterpret_cast<const double2*>(x + 8 * r + 2 * q0);
+      const double2 x0 = xr[0], x1 = xr[1];
+      double2* yr = reinterpret_cast<double2*>(y + 8 * r + 2 * q0);
+      yr[0] = make_double2(a0r - (sr * x0.x - si * x0.y), a0i - (sr * x0.y + si * x0.x));
+      yr[1] = make_double2(a1r - (sr * x1.x - si * x1.y), a1i - (sr * x1.y + si * x1.x));
     }
   }
 }
@@ -751,7 +835,7 @@ int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const doubl
   EB_VALIDATE(b);
   if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_states_fwd<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+  k_apply_states_fwd4<<<grid_for(4 * b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
       t, b->n_cells, J, d_states, d_odes);
   return check_launch("apply_odes_wrt_states_fwd");
 }
@@ -832,8 +916,8 @@ int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, c
   EB_VALIDATE(b);
   if (!X || !U || !dR) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_tangent<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
-                                                                       dU, dX, dV, dMa, dR, R);
+  k_tangent<<<grid_for(2 * b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+      t, b->n_cells, X, V, U, dU, dX, dV, dMa, dR, R);
   return check_launch("apply_odes_tangent");
 }
 
@@ -853,7 +937,9 @@ int eb_bsr_shifted_spmv(int64_t n_rows, const double* data, const int32_t* indic
                         const double* x, double* y, void* stream) {
   if (n_rows <= 0 || !data || !indices || !index_pointers || !x || !y)
     return fail(EB_ERR_ARG, "bad BSR arguments");
-  k_bsr_spmv<<<grid_for(n_rows, 128), 128, 0, EB_STREAM(stream)>>>(
+  if (((uintptr_t)data | (uintptr_t)x | (uintptr_t)y) & 15)
+    return fail(EB_ERR_ARG, "BSR data, x and y must be 16-byte aligned");
+  k_bsr_spmv<<<grid_for(8 * n_rows, 256), 256, 0, EB_STREAM(stream)>>>(
       n_rows, data, indices, index_pointers, shift_re, shift_im, x, y);
   return check_launch("bsr_shifted_spmv");
 }
