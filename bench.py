@@ -236,6 +236,45 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def cpu_resolvent_rate(X, V, U, mach: float, shift: complex) -> dict:
+    """Shifted solves/s of the reference's own resolvent method on the host: the Jacobian from
+    the oracle, then per shift the CSR assembly and SuperLU (scipy.sparse.linalg.spsolve), as
+    SpatialDiscretization._assemble_csr / solve_odes_wrt_states_fwd do (core.py:512-565).
+    One shift is the bounded sample (SuperLU is single-threaded)."""
+    from scipy.sparse import bsr_array
+    from scipy.sparse.linalg import spsolve
+
+    from oracle.shim import SpatialDiscretizationModule
+
+    M, N = U.shape[1], U.shape[2]
+    disc = SpatialDiscretizationModule()
+    disc.aoa[...] = FLOW["aoa_deg"]
+    t0 = time.perf_counter()
+    J = np.zeros((4, 4, M, N, 9), order="F")
+    disc.compute_odes_wrt_states(mach, np.asarray(X, complex), np.asarray(V, complex),
+                                 np.asarray(U, complex), J)
+    nnzb = (9 * M - 6) * N
+    data = np.empty((4, 4, nnzb), order="F")
+    idx = np.empty(nnzb, dtype=np.intc)
+    ptr = np.empty(M * N + 1, dtype=np.intc)
+    disc.convert_odes_wrt_states(J, data, idx, ptr)
+    t_lin = time.perf_counter() - t0
+    b = np.array([1.0, 1j]) @ np.random.default_rng(5).standard_normal((2, 4 * M * N))
+    t0 = time.perf_counter()
+    A = bsr_array((np.moveaxis(data, -1, 0), idx - 1, ptr - 1), dtype=complex).tocsr()
+    A.setdiag(A.diagonal() - shift)
+    x = spsolve(A, b)
+    t_solve = time.perf_counter() - t0
+    rel = float(np.linalg.norm(A @ x - b) / np.linalg.norm(b))
+    return {"value": 1.0 / t_solve, "unit": "shifted solves/s", "cores": 1, "kind": "port",
+            "cpu": cpu_model(),
+            "sample": f"one solve at shift {shift:.4g} of the {M}x{N}-cell steady-state "
+                      f"Jacobian in {t_solve:.1f} s (relative residual {rel:.1e}); the Jacobian "
+                      f"and its BSR form (oracle, complex step) took {t_lin:.1f} s once",
+            "method": "CSR assembly + SuperLU (scipy.sparse.linalg.spsolve) per shift, as "
+                      "core.py:512-565"}
+
+
 # ---- B200 arm -------------------------------------------------------------------------------
 
 def read_traffic() -> float | None:
@@ -561,6 +600,12 @@ def run_b200(args) -> None:
                        "seconds": t_ptc},
                "method": "ring-block LU (batched Gauss-Jordan ring inversions + strided-batched "
                          "ZGEMM), refined to 1e-10 relative residual"}
+        if rank == 0 and not args.no_cpu_baseline:
+            res["cpu_reference_method"] = cpu_resolvent_rate(
+                sd.vertices, sd.velocities, sd.states, FLOW["mach"],
+                1j * ks[0] * FLOW["mach"] * 1.4 ** 0.5 / (GRID["chord"] / 2))
+            res["batched_vs_cpu_reference_method"] = \
+                batched_rate / res["cpu_reference_method"]["value"]
         del sd
 
     # uneven instances: steady states (PTC) and adjoint lift gradients of many grids of
