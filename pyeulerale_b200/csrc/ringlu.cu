@@ -103,10 +103,19 @@ inline int panel_width(int K) {
   return 0;
 }
 
+// Width of the Gauss-Jordan column blocks whose trailing update is one ZGEMM (when it divides
+// K and a stream's group has at least kGjBlockMinShifts shifts; otherwise every panel updates
+// the whole block itself). On the 129x129 grid (K = 512) the blocked form takes 0.180 instead
+// of 0.200 ms per ring and shift with 16 shifts per group, breaks even at 4 and is 13 % slower
+// with one shift, whose thin ZGEMMs do not fill the GPU.
+constexpr int kGjBlock = 64;
+constexpr int kGjBlockMinShifts = 8;
+
 struct Layout {
   int M, N, K;
   size_t blk;  // bytes of one K x K complex block
-  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_T, off_perm, off_info, off_acc, off_shift;
+  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_T, off_Rp, off_perm, off_info, off_acc,
+      off_shift;
   size_t off_y, off_x, off_r;
   size_t total;
 };
@@ -129,6 +138,7 @@ Layout plan(int M, int N) {
   L.off_C1 = take(L.blk * M);
   L.off_C2 = take(L.blk * M);
   L.off_T = take(L.blk);
+  L.off_Rp = take(sizeof(cuDoubleComplex) * (size_t)kGjBlock * L.K);
   L.off_perm = take(sizeof(int) * (size_t)L.K);
   L.off_info = take(sizeof(int) * 4);
   L.off_acc = take(sizeof(double) * 2);
@@ -343,22 +353,25 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
   }
 }
 
-// Gauss-Jordan update, out of place: out[:, c] = in[:, c] + G R[:, c] for every column c
-// outside the panel, where R[k, c] = in[perm[j0 + k], c] and G[:, k] = out[:, j0 + k] -
-// e_{perm[j0 + k]} (the panel columns that k_gj_panel wrote). One CTA per 64-row x 32-column
-// tile; a thread prefetches its 8 inputs before the rank-NB products. Grid: tiles x shifts.
+// Gauss-Jordan update, out of place: out[:, c] = in[:, c] + G R[:, c] for every column c of
+// [c_lo, c_hi) outside the panel, where R[k, c] = in[perm[j0 + k], c] and G[:, k] =
+// out[:, j0 + k] - e_{perm[j0 + k]} (the panel columns that k_gj_panel wrote). One CTA per
+// 64-row x 32-column tile; a thread prefetches its 8 inputs before the rank-NB products.
+// Grid: tiles x shifts.
 constexpr int kUpdRowsT = 64;
 constexpr int kUpdColsT = 32;
 template <int NB>
-__global__ void __launch_bounds__(256, 3) k_gj_update(int K, int j0, char* ws0, int64_t stride,
-                                                   size_t off_in, size_t off_out, size_t off_perm,
+__global__ void __launch_bounds__(256, 3) k_gj_update(int K, int j0, int c_lo, int c_hi,
+                                                   char* ws0, int64_t stride, size_t off_in,
+                                                   size_t off_out, size_t off_perm,
                                                    size_t off_info) {
   constexpr int kPer = kUpdRowsT * kUpdColsT / 256;  // outputs per thread
   constexpr int kGI = (NB * kUpdRowsT + 255) / 256, kRI = (NB * kUpdColsT + 255) / 256;
   __shared__ cuDoubleComplex G[NB][kUpdRowsT];
   __shared__ cuDoubleComplex R[NB][kUpdColsT];
-  const int ctiles = (K + kUpdColsT - 1) / kUpdColsT;
-  const int c0 = (blockIdx.x % ctiles) * kUpdColsT, r0 = (blockIdx.x / ctiles) * kUpdRowsT;
+  const int ctiles = (c_hi - c_lo + kUpdColsT - 1) / kUpdColsT;
+  const int c0 = c_lo + (blockIdx.x % ctiles) * kUpdColsT;
+  const int r0 = (blockIdx.x / ctiles) * kUpdRowsT;
   const cuDoubleComplex* in = at<cuDoubleComplex>(ws0, stride, off_in);
   cuDoubleComplex* out = at<cuDoubleComplex>(ws0, stride, off_out);
   const int* perm = at<int>(ws0, stride, off_perm);
@@ -372,7 +385,7 @@ __global__ void __launch_bounds__(256, 3) k_gj_update(int K, int j0, char* ws0, 
 #pragma unroll
   for (int q = 0; q < kPer; ++q) {
     const int col = c0 + cb + 4 * q;
-    acc[q] = row < K && col < K ? in[(size_t)K * col + row] : make_cuDoubleComplex(0.0, 0.0);
+    acc[q] = row < K && col < c_hi ? in[(size_t)K * col + row] : make_cuDoubleComplex(0.0, 0.0);
   }
   int bad = *at<int>(ws0, stride, off_info) != 0;
   int pg[kGI];
@@ -393,7 +406,7 @@ __global__ void __launch_bounds__(256, 3) k_gj_update(int K, int j0, char* ws0, 
     if (e < NB * kUpdColsT) {
       const int pr = perm[j0 + k];
       if (pr < 0 || pr >= K) bad = 1;
-      else if (col < K) rv[q] = in[(size_t)K * col + pr];
+      else if (col < c_hi) rv[q] = in[(size_t)K * col + pr];
     }
   }
 #pragma unroll
@@ -422,7 +435,31 @@ __global__ void __launch_bounds__(256, 3) k_gj_update(int K, int j0, char* ws0, 
 #pragma unroll
   for (int q = 0; q < kPer; ++q) {
     const int col = c0 + cb + 4 * q;
-    if (col < K && !(col >= j0 && col < j0 + NB)) out[(size_t)K * col + row] = acc[q];
+    if (col < c_hi && !(col >= j0 && col < j0 + NB)) out[(size_t)K * col + row] = acc[q];
+  }
+}
+
+// Two-level Gauss-Jordan: after the panel steps of a block of BW columns [b0, b0 + BW) (pivot
+// rows P = perm[b0 .. b0 + BW - 1]), every column c outside the block becomes
+// W[:, c] + (W[:, block] - E_P) W[P, c]. This kernel moves the pivot rows W[P, c] of those
+// columns into R (BW x K, column-major) and zeroes them in W, which turns the update into
+// W[:, c] += W[:, block] R[:, c], one strided-batched ZGEMM per column range. Grid: K columns
+// x shifts; skipped when a panel met a singular pivot (the factorisation then fails anyway).
+__global__ void __launch_bounds__(64) k_gj_take_pivot_rows(int K, int b0, int BW, char* ws0,
+                                                          int64_t stride, size_t off_W,
+                                                          size_t off_R, size_t off_perm,
+                                                          size_t off_info) {
+  const int c = blockIdx.x;
+  if (c >= b0 && c < b0 + BW) return;
+  if (*at<int>(ws0, stride, off_info) != 0) return;
+  cuDoubleComplex* W = at<cuDoubleComplex>(ws0, stride, off_W);
+  cuDoubleComplex* R = at<cuDoubleComplex>(ws0, stride, off_R);
+  const int* perm = at<int>(ws0, stride, off_perm);
+  for (int k = threadIdx.x; k < BW; k += blockDim.x) {
+    const int p = perm[b0 + k];
+    if (p < 0 || p >= K) continue;
+    R[(size_t)BW * c + k] = W[(size_t)K * c + p];
+    W[(size_t)K * c + p] = make_cuDoubleComplex(0.0, 0.0);
   }
 }
 
@@ -635,35 +672,70 @@ int blas_ok(cublasStatus_t st, const char* what) {
   return st == CUBLAS_STATUS_SUCCESS ? EB_OK : fail(EB_ERR_CUDA, what);
 }
 
+// Panel steps j0 .. j0 + NB - 1 (in -> out) and their update of the columns [c_lo, c_hi).
 template <int NB, int ROWS>
-void gj_pass(const Group& g, int j0, size_t off_in, size_t off_out, cudaStream_t st) {
+void gj_pass(const Group& g, int j0, int c_lo, int c_hi, size_t off_in, size_t off_out,
+             cudaStream_t st) {
   const int K = g.L.K;
-  const int tiles = ((K + kUpdColsT - 1) / kUpdColsT) * ((K + kUpdRowsT - 1) / kUpdRowsT);
+  const int tiles = ((c_hi - c_lo + kUpdColsT - 1) / kUpdColsT) * ((K + kUpdRowsT - 1) / kUpdRowsT);
   k_gj_panel<NB, ROWS><<<dim3(1, g.S), kPanelThreads, 0, st>>>(K, j0, g.base, g.stride, off_in, off_out,
                                                                g.L.off_perm, g.L.off_info);
-  k_gj_update<NB><<<dim3(tiles, g.S), 256, 0, st>>>(K, j0, g.base, g.stride, off_in, off_out,
-                                                           g.L.off_perm, g.L.off_info);
+  k_gj_update<NB><<<dim3(tiles, g.S), 256, 0, st>>>(K, j0, c_lo, c_hi, g.base, g.stride, off_in,
+                                                    off_out, g.L.off_perm, g.L.off_info);
 }
 
-// D_m <- D_m^-1 for every shift (Gauss-Jordan, ping-pong between D_m and the scratch block T).
-int invert_ring(const Group& g, int m, cudaStream_t st) {
+void gj_pass_any(const Group& g, int nb, int rows, int j0, int c_lo, int c_hi, size_t in,
+                 size_t out, cudaStream_t st) {
+  if (rows == 1) {
+    if (nb == 16) gj_pass<16, 1>(g, j0, c_lo, c_hi, in, out, st);
+    else if (nb == 8) gj_pass<8, 1>(g, j0, c_lo, c_hi, in, out, st);
+    else gj_pass<4, 1>(g, j0, c_lo, c_hi, in, out, st);
+  } else {
+    if (nb == 8) gj_pass<8, 2>(g, j0, c_lo, c_hi, in, out, st);
+    else gj_pass<4, 2>(g, j0, c_lo, c_hi, in, out, st);
+  }
+}
+
+// D_m <- D_m^-1 for every shift by Gauss-Jordan with implicit row pivoting (ping-pong between
+// D_m and the scratch block T). In the blocked form the columns go in blocks of kGjBlock:
+// the panels of a block update only the block's columns (an even number of passes, so the
+// block ends in D_m), and the rest of D_m takes the block's combined rank-kGjBlock update as
+// strided-batched ZGEMMs (tensor-core DMMA) instead of kGjBlock / nb streaming passes.
+int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
   const Layout& L = g.L;
   const int K = L.K, nb = panel_width(K), rows = (K + kPanelThreads - 1) / kPanelThreads;
   const size_t buf[2] = {g.boff(L.off_D, m), L.off_T};
   const int passes = K / nb;
-  for (int p = 0; p < passes; ++p) {
-    const size_t in = buf[p & 1], out = buf[(p + 1) & 1];
-    const int j0 = p * nb;
-    if (rows == 1) {
-      if (nb == 16) gj_pass<16, 1>(g, j0, in, out, st);
-      else if (nb == 8) gj_pass<8, 1>(g, j0, in, out, st);
-      else gj_pass<4, 1>(g, j0, in, out, st);
-    } else {
-      if (nb == 8) gj_pass<8, 2>(g, j0, in, out, st);
-      else gj_pass<4, 2>(g, j0, in, out, st);
+  const bool blocked = K % kGjBlock == 0 && (kGjBlock / nb) % 2 == 0 && g.S >= kGjBlockMinShifts;
+  if (!blocked) {
+    for (int p = 0; p < passes; ++p)
+      gj_pass_any(g, nb, rows, p * nb, 0, K, buf[p & 1], buf[(p + 1) & 1], st);
+  } else {
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+    const int64_t es = g.es();
+    cuDoubleComplex* W = g.blk(L.off_D, m);
+    cuDoubleComplex* Rp = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_Rp);
+    for (int b0 = 0; b0 < K; b0 += kGjBlock) {
+      for (int q = 0; q < kGjBlock / nb; ++q)
+        gj_pass_any(g, nb, rows, b0 + q * nb, b0, b0 + kGjBlock, buf[q & 1], buf[(q + 1) & 1], st);
+      if (K == kGjBlock) break;
+      k_gj_take_pivot_rows<<<dim3(K, g.S), 64, 0, st>>>(K, b0, kGjBlock, g.base, g.stride, buf[0],
+                                                        L.off_Rp, L.off_perm, L.off_info);
+      const int ranges[2][2] = {{0, b0}, {b0 + kGjBlock, K}};
+      for (const auto& rg : ranges) {
+        const int n_cols = rg[1] - rg[0];
+        if (n_cols <= 0) continue;
+        int rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, n_cols, kGjBlock,
+                                                   &one, W + (size_t)K * b0, K, es,
+                                                   Rp + (size_t)kGjBlock * rg[0], kGjBlock, es,
+                                                   &one, W + (size_t)K * rg[0], K, es, g.S),
+                         "ringlu: gemm Gauss-Jordan block update");
+        if (rc != EB_OK) return rc;
+      }
     }
   }
-  const size_t W = buf[passes & 1], other = buf[(passes + 1) & 1];
+  const size_t W = blocked ? buf[0] : buf[passes & 1];
+  const size_t other = blocked ? buf[1] : buf[(passes + 1) & 1];
   k_gj_permute<<<dim3(std::min(K, 1024), g.S), 256, sizeof(int) * K, st>>>(K, g.base, g.stride, W, other,
                                                                           L.off_perm, L.off_info);
   if (other != buf[0] &&
@@ -681,7 +753,7 @@ int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
   const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
   const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
   const int64_t es = g.es();
-  int rc = invert_ring(g, m, st);
+  int rc = invert_ring(g, h, m, st);
   if (rc != EB_OK) return rc;
   if (m + 1 < M) {
     // T = L1[m+1] = B1'[m+1] Dinv_m;  D[m+1] -= T C1'[m]

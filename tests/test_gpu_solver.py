@@ -150,6 +150,39 @@ def test_ringlu_many_matches_single(cuda, golden_grids, name):
             assert rel_err(xs[k].cpu().numpy(), x1.cpu().numpy()) <= 1e-9, (name, k, adjoint)
 
 
+@pytest.mark.parametrize("grid", ["naca0012_33", "wide"])
+def test_ringlu_blocked_matches_single(cuda, golden_grids, grid):
+    """16 shifts (two stream groups of 8) take the blocked Gauss-Jordan inversion (64-column
+    blocks, ZGEMM trailing updates); one shift at a time takes the unblocked one. Both agree,
+    both directions, on K = 128 (16-column panels) and K = 1024 (8-column panels)."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200 import solver
+
+    rng = np.random.default_rng(21)
+    if grid == "wide":
+        X = G.naca_ogrid(9, 257, 0.12, 1.0, 20.0, 0.05)
+        case = dict(X=X, V=np.zeros_like(X), U=G.perturbed_states(8, 256, 0.6, 2.0, 0.01, rng),
+                    mach=0.6, aoa=2.0)
+    else:
+        case = make_case(grid, golden_grids, seed=5)
+    gpu = Gpu(cuda, case)
+    g = gpu.evaluate()
+    M, N = gpu.M, gpu.N
+    assert (4 * N) % 64 == 0
+    shifts = [1j * k for k in np.logspace(-2, 1, 14)] + [0.0, 1.5 - 0.25j]
+    rhs = [gpu.dev(crandn(rng, (4, M, N))) for _ in shifts]
+    many = solver.RingLUMany(gpu.batch, capacity=len(shifts), tol=1e-10)
+    many.factor(g["_dev"]["J_u"], shifts)
+    one = solver.RingLU(gpu.batch, tol=1e-10)
+    for adjoint in (False, True):
+        xs, rels = many.solve(rhs, adjoint=adjoint)
+        assert max(rels) <= 1e-10, rels
+        for k in (0, 7, 8, 15):  # first and last shift of each group
+            one.factor(g["_dev"]["J_u"], shifts[k])
+            x1, _ = one.solve(rhs[k], adjoint=adjoint)
+            assert rel_err(xs[k].cpu().numpy(), x1.cpu().numpy()) <= 1e-9, (grid, k, adjoint)
+
+
 def test_ringlu_wide_rings(cuda, oracle):
     """Rings of 4 N = 1024 unknowns (N = 256: the two-rows-per-thread panel path)."""
     from pyeulerale_b200 import grid as G
