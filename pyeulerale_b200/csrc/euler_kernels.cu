@@ -24,6 +24,9 @@ namespace eb {
 
 int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
                           double* R, cudaStream_t stream, int max_tiles);
+int launch_tangent_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
+                         const double* dU, const double* dX, const double* dV, const double* dMa,
+                         double* dR, double* R, cudaStream_t stream, int max_tiles);
 int residual_tiles(int M, int N);
 
 thread_local std::string g_last_error;
@@ -124,104 +127,6 @@ __global__ void __launch_bounds__(128) k_residual(Table t, int64_t n_cells, cons
     double2* out = reinterpret_cast<double2*>(R + 4 * g);
     out[0] = make_double2(o.v[0], o.v[1]);
     out[1] = make_double2(o.v[2], o.v[3]);
-  }
-}
-
-// Matrix-free forward tangent with a complex direction on every input, two threads per cell:
-// thread h of a cell (h = 0: real part, 1: imaginary part of the direction) evaluates make_ode
-// in one-component duals (Dual<double, 1>) seeded with its part. The stencil states are read
-// face by face through a provider (the repeated reads hit L1), so only one face's operands are
-// live at a time; holding the whole nine-state stencil as duals in registers spilled kilobytes
-// per thread.
-using D1 = Dual<double, 1>;
-
-struct TangentStates {
-  const double* U;   // the instance's states
-  const double* dU;  // the instance's complex state direction, or nullptr
-  int M, N, m, n, h;
-  __device__ __forceinline__ S4<D1> operator()(int s) const {
-    const int64_t j = (m + slot_dm(s)) + (int64_t)M * wrap(n + slot_dn(s), N);
-    const S4<double> u = ld4(U + 4 * j);
-    S4<D1> r;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      r.v[k].v = u.v[k];
-      r.v[k].d[0] = dU ? __ldg(dU + 8 * j + 2 * k + h) : 0.0;
-    }
-    return r;
-  }
-};
-
-__device__ __forceinline__ P2<D1> tangent_point(const double* P, const double* dP, int64_t v,
-                                                int h) {
-  P2<D1> r;
-  const P2<double> x = P ? ld2(P + 2 * v) : P2<double>{0.0, 0.0};
-  r.x.v = x.x;
-  r.z.v = x.z;
-  r.x.d[0] = dP ? __ldg(dP + 4 * v + h) : 0.0;
-  r.z.d[0] = dP ? __ldg(dP + 4 * v + 2 + h) : 0.0;
-  return r;
-}
-
-__global__ void __launch_bounds__(128) k_tangent(Table t, int64_t n_cells, const double* X,
-                                                 const double* V, const double* U,
-                                                 const double* dU, const double* dX,
-                                                 const double* dV, const double* dMa,
-                                                 double* dR, double* R) {
-  for (int64_t gq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gq < 2 * n_cells;
-       gq += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t g = gq >> 1;
-    const int h = (int)(gq & 1);
-    const Instance in = t.cell(g);
-    const int M = in.M, N = in.N;
-    const int64_t local = g - in.cell_offset;
-    const int m = (int)(local % M), n = (int)(local / M);
-    const int flag = boundary_flag(M, m);
-    const int64_t v_bi = m + (int64_t)(M + 1) * n, v_fi = m + (int64_t)(M + 1) * (n + 1);
-    const int64_t corner[4] = {v_bi, v_fi, v_fi + 1, v_bi + 1};  // kBI, kFI, kFO, kBO
-    const double* Xi = X + 2 * in.vert_offset;
-    const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
-    const double* dXi = dX ? dX + 4 * in.vert_offset : nullptr;
-    const double* dVi = dV ? dV + 4 * in.vert_offset : nullptr;
-    P2<D1> x[4], w[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      x[k] = tangent_point(Xi, dXi, corner[k], h);
-      w[k] = tangent_point(Vi, dVi, corner[k], h);
-    }
-    const Geometry<D1, D1> geo = geometry(x, w);
-    D1 mach;
-    mach.v = in.mach;
-    mach.d[0] = 0.0;
-    if (dMa) {
-      // one complex per instance; the instance index is the table position
-      int lo = 0;
-      if (t.dev) {
-        int hi = t.n - 1;
-        while (lo < hi) {
-          int mid = (lo + hi + 1) >> 1;
-          if (t.dev[mid].cell_offset <= g) lo = mid; else hi = mid - 1;
-        }
-      }
-      mach.d[0] = dMa[2 * lo + h];
-    }
-    const TangentStates u{U + 4 * in.cell_offset, dU ? dU + 8 * in.cell_offset : nullptr,
-                          M, N, m, n, h};
-    // -(((F_b + F_f) + F_i) + F_o) / area, the order of make_ode
-    S4<D1> acc = face<D1>(kFaceB, flag, u, geo, mach, in);
-    const S4<D1> ff = face<D1>(kFaceF, flag, u, geo, mach, in);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc.v[k] = acc.v[k] + ff.v[k];
-    const S4<D1> fi = face<D1>(kFaceI, flag, u, geo, mach, in);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc.v[k] = acc.v[k] + fi.v[k];
-    const S4<D1> fo = face<D1>(kFaceO, flag, u, geo, mach, in);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const D1 o = -(acc.v[k] + fo.v[k]) / geo.area;
-      dR[8 * g + 2 * k + h] = o.d[0];
-      if (R && h == 0) R[4 * g + k] = o.v;
-    }
   }
 }
 
@@ -915,10 +820,11 @@ int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, c
                           const double* dMa, double* dR, double* R, void* stream) {
   EB_VALIDATE(b);
   if (!X || !U || !dR) return fail(EB_ERR_ARG, "null array");
-  const Table t = make_table(b);
-  k_tangent<<<grid_for(2 * b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
-      t, b->n_cells, X, V, U, dU, dX, dV, dMa, dR, R);
-  return check_launch("apply_odes_tangent");
+  int dim = b->max_dim;
+  if (b->n_inst == 1 && b->d_table == nullptr) dim = std::max(b->single.M, b->single.N);
+  if (dim < 5) return fail(EB_ERR_ARG, "batch max_dim must be the largest M or N");
+  return launch_tangent_tiled(b, X, V, U, dU, dX, dV, dMa, dR, R, EB_STREAM(stream),
+                              residual_tiles(dim, dim));
 }
 
 int eb_convert_odes_wrt_states(const eb_batch* b, const double* J, double* data,

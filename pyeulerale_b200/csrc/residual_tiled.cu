@@ -1,4 +1,6 @@
-// Tiled FP64 residual kernel: R(Ma, U, X, V) for packed instances (eb_compute_odes).
+// Tiled FP64 residual kernel: R(Ma, U, X, V) for packed instances (eb_compute_odes), and the
+// same kernel in one-component dual numbers for the matrix-free forward tangent
+// (eb_apply_odes_tangent).
 //
 // One CTA computes a tile of kTM x kTN cells (radial x angular) of one instance:
 //  1. it stages the tile's states with a two-cell halo (the reach of the nine-point cross
@@ -19,6 +21,12 @@
 //     cell then writes -(F_b + F_f + F_i + F_o) / area (f90:370-436).
 // Results agree with the reference to the rounding of the reordered arithmetic (<= 1e-12
 // relative); every branch (boundary cases, max_c tolerance) follows the reference.
+//
+// The kernel is a template on its scalar type T. T = double is the residual. T = Dual<double,
+// 1> is the tangent along a complex direction (dU, dX, dV, dMa): the CTAs of grid slice z = h
+// carry part h (0: real, 1: imaginary) of the direction as the dual component, with abs_c /
+// max_c (f90:97-120) taking their branches from the values as the reference's complex step
+// does.
 
 #include "common.cuh"
 
@@ -33,74 +41,99 @@ constexpr int kStaged = kSR * kSC;
 constexpr int kVR = kTM + 1, kVC = kTN + 1;   // staged vertices
 constexpr int kVerts = kVR * kVC;
 
+using D1 = Dual<double, 1>;
+
+template <class T>
 struct TileSmem {
-  double rho[kStaged], j1[kStaged], j2[kStaged], e[kStaged];
-  double p[kStaged], ir[kStaged], cs[kStaged];
-  double s_ang[kTM * (kTN + 2)];   // angular sensor centred on (r, c), c in [-1, kTN]
-  double s_rad[(kTM + 2) * kTN];   // radial sensor centred on (r, c), r in [-1, kTM]
-  double x[kVerts], z[kVerts], vx[kVerts], vz[kVerts];
-  double ff[4][kTN][kTM];          // flux through face f of each cell (from its f neighbour's face)
-  double fo[4][kTN][kTM];          // flux through face o of each cell (from its o neighbour's face)
+  T rho[kStaged], j1[kStaged], j2[kStaged], e[kStaged];
+  T p[kStaged], ir[kStaged], cs[kStaged];
+  T s_ang[kTM * (kTN + 2)];   // angular sensor centred on (r, c), c in [-1, kTN]
+  T s_rad[(kTM + 2) * kTN];   // radial sensor centred on (r, c), r in [-1, kTM]
+  T x[kVerts], z[kVerts], vx[kVerts], vz[kVerts];
+  T ff[4][kTN][kTM];          // flux through face f of each cell (from its f neighbour's face)
+  T fo[4][kTN][kTM];          // flux through face o of each cell (from its o neighbour's face)
 };
 
 __device__ __forceinline__ int sidx(int r, int c) { return (c + 2) * kSR + (r + 2); }
 __device__ __forceinline__ int vidx(int r, int c) { return c * kVR + r; }
 
+// a * b + c: one fused multiply-add for plain doubles, the dual product and sum otherwise.
+template <class A, class B, class C>
+__device__ __forceinline__ promote_t<A, promote_t<B, C>> fmad(const A& a, const B& b,
+                                                             const C& c) {
+  if constexpr (std::is_same<A, double>::value && std::is_same<B, double>::value &&
+                std::is_same<C, double>::value)
+    return fma(a, b, c);
+  else
+    return a * b + c;
+}
+
+template <class T>
 struct St {  // a state with its derived quantities
-  double rho, j1, j2, e, p, ir, cs;
+  T rho, j1, j2, e, p, ir, cs;
 };
 
-__device__ __forceinline__ St derive(double rho, double j1, double j2, double e) {
-  St s;
+template <class T>
+__device__ __forceinline__ St<T> derive(const T& rho, const T& j1, const T& j2, const T& e) {
+  St<T> s;
   s.rho = rho;
   s.j1 = j1;
   s.j2 = j2;
   s.e = e;
   s.ir = 1.0 / rho;
   s.p = kGm1 * (e - (j1 * j1 + j2 * j2) * s.ir * 0.5);
-  s.cs = sqrt(kGamma * s.p * s.ir);
+  s.cs = sqrt_(kGamma * s.p * s.ir);
   return s;
 }
 
-__device__ __forceinline__ St staged(const TileSmem& S, int i) {
-  return St{S.rho[i], S.j1[i], S.j2[i], S.e[i], S.p[i], S.ir[i], S.cs[i]};
+template <class T>
+__device__ __forceinline__ St<T> staged(const TileSmem<T>& S, int i) {
+  return St<T>{S.rho[i], S.j1[i], S.j2[i], S.e[i], S.p[i], S.ir[i], S.cs[i]};
 }
 
-__device__ __forceinline__ double sensor(double pa, double pb, double pc) {
-  return fabs(pa - 2.0 * pb + pc) / (pa + 2.0 * pb + pc);
+template <class T>
+__device__ __forceinline__ T sensor(const T& pa, const T& pb, const T& pc) {
+  return abs_c(pa - 2.0 * pb + pc) / (pa + 2.0 * pb + pc);
 }
 
-__device__ __forceinline__ double max_cd(double x, double y) {
-  return (x > y + 1e-8) ? x : y;
+// max_c(0, c) (f90:111-120 with x = 0): 0 only if 0 > Re c + 1e-8.
+template <class T>
+__device__ __forceinline__ T max_c0(const T& c) {
+  return (0.0 > value(c) + 1e-8) ? lift<T>(0.0) : c;
 }
 
 // Wall ghost (make_wall_ghost_state, f90:231-240) of state s for face normal n, grid velocity g.
-__device__ __forceinline__ St wall_ghost_st(const St& s, double nx, double nz, double gx,
-                                            double gz) {
-  const double proj = nx * (s.j1 - gx * s.rho) + nz * (s.j2 - gz * s.rho);
-  const double nn = nx * nx + nz * nz;
-  return derive(s.rho, s.j1 - 2.0 * nx * proj / nn, s.j2 - 2.0 * nz * proj / nn, s.e);
+template <class T>
+__device__ __forceinline__ St<T> wall_ghost_st(const St<T>& s, const T& nx, const T& nz,
+                                               const T& gx, const T& gz) {
+  const T proj = nx * (s.j1 - gx * s.rho) + nz * (s.j2 - gz * s.rho);
+  const T nn = nx * nx + nz * nz;
+  return derive<T>(s.rho, s.j1 - 2.0 * nx * proj / nn, s.j2 - 2.0 * nz * proj / nn, s.e);
 }
 
 // Far-field ghost (make_farfield_ghost_state, f90:269-274): 2 U_inf - U.
-__device__ __forceinline__ St farfield_ghost_st(const St& s, const Instance& in) {
-  const double speed = in.mach * sqrt(kGamma);
-  const double f1 = speed * in.cos_aoa, f2 = speed * in.sin_aoa;
-  const double fe = 1.0 / kGm1 + speed * speed / 2.0;
-  return derive(2.0 - s.rho, 2.0 * f1 - s.j1, 2.0 * f2 - s.j2, 2.0 * fe - s.e);
+template <class T>
+__device__ __forceinline__ St<T> farfield_ghost_st(const St<T>& s, const T& mach,
+                                                   const Instance& in) {
+  const T speed = mach * sqrt_(kGamma);
+  const T f1 = speed * in.cos_aoa, f2 = speed * in.sin_aoa;
+  const T fe = 1.0 / kGm1 + speed * speed / 2.0;
+  return derive<T>(2.0 - s.rho, 2.0 * f1 - s.j1, 2.0 * f2 - s.j2, 2.0 * fe - s.e);
 }
 
+template <class T>
 struct Flux {
-  double f[4];
+  T f[4];
 };
 
 // Central part + ALE term of make_face_flux (f90:197, 219) for l, r through normal (nx, nz)
 // with grid-velocity flux vn = g.n.
-__device__ __forceinline__ Flux central(const St& l, const St& r, double nx, double nz,
-                                       double vn) {
-  const double vl = (nx * l.j1 + nz * l.j2) * l.ir;
-  const double vr = (nx * r.j1 + nz * r.j2) * r.ir;
-  Flux F;
+template <class T>
+__device__ __forceinline__ Flux<T> central(const St<T>& l, const St<T>& r, const T& nx,
+                                           const T& nz, const T& vn) {
+  const T vl = (nx * l.j1 + nz * l.j2) * l.ir;
+  const T vr = (nx * r.j1 + nz * r.j2) * r.ir;
+  Flux<T> F;
   F.f[0] = (l.rho * vl + r.rho * vr) / 2.0 - (l.rho + r.rho) / 2.0 * vn;
   F.f[1] = ((l.j1 * vl + nx * l.p) + (r.j1 * vr + nx * r.p)) / 2.0 - (l.j1 + r.j1) / 2.0 * vn;
   F.f[2] = ((l.j2 * vl + nz * l.p) + (r.j2 * vr + nz * r.p)) / 2.0 - (l.j2 + r.j2) / 2.0 * vn;
@@ -109,23 +142,24 @@ __device__ __forceinline__ Flux central(const St& l, const St& r, double nx, dou
 }
 
 // make_face_flux with JST dissipation (f90:189-220); s1, s2 are the sensors centred on l and r.
-__device__ __forceinline__ Flux jst(const St& ll, const St& l, const St& r, const St& rr,
-                                   double nx, double nz, double len, double vn, double s1,
-                                   double s2, const Instance& in) {
-  const double vl = (nx * l.j1 + nz * l.j2) * l.ir;
-  const double vr = (nx * r.j1 + nz * r.j2) * r.ir;
-  const double lam = max_cd(fabs(vl) + l.cs * len, fabs(vr) + r.cs * len);
-  const double coef2 = in.k2 * max_cd(s1, s2) * lam;
-  const double c4 = in.k4 * lam - in.c4 * coef2;
-  const double coef4 = (0.0 > c4 + 1e-8) ? 0.0 : c4;
-  Flux F;
-  const double lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
-  const double llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
-  const double fl[4] = {l.rho * vl, l.j1 * vl + nx * l.p, l.j2 * vl + nz * l.p, (l.e + l.p) * vl};
-  const double fr[4] = {r.rho * vr, r.j1 * vr + nx * r.p, r.j2 * vr + nz * r.p, (r.e + r.p) * vr};
+template <class T>
+__device__ __forceinline__ Flux<T> jst(const St<T>& ll, const St<T>& l, const St<T>& r,
+                                       const St<T>& rr, const T& nx, const T& nz, const T& len,
+                                       const T& vn, const T& s1, const T& s2,
+                                       const Instance& in) {
+  const T vl = (nx * l.j1 + nz * l.j2) * l.ir;
+  const T vr = (nx * r.j1 + nz * r.j2) * r.ir;
+  const T lam = max_c(abs_c(vl) + l.cs * len, abs_c(vr) + r.cs * len);
+  const T coef2 = in.k2 * max_c(s1, s2) * lam;
+  const T coef4 = max_c0(in.k4 * lam - in.c4 * coef2);
+  Flux<T> F;
+  const T lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
+  const T llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
+  const T fl[4] = {l.rho * vl, l.j1 * vl + nx * l.p, l.j2 * vl + nz * l.p, (l.e + l.p) * vl};
+  const T fr[4] = {r.rho * vr, r.j1 * vr + nx * r.p, r.j2 * vr + nz * r.p, (r.e + r.p) * vr};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    double c = (fl[k] + fr[k]) / 2.0;
+    T c = (fl[k] + fr[k]) / 2.0;
     c = c - (coef2 * (rv[k] - lv[k]) - coef4 * (rrv[k] - 3.0 * rv[k] + 3.0 * lv[k] - llv[k]));
     F.f[k] = c - (lv[k] + rv[k]) / 2.0 * vn;
   }
@@ -139,39 +173,45 @@ __device__ __forceinline__ Flux jst(const St& ll, const St& l, const St& r, cons
 // orientation as the reference takes them. The shared parts are formed once: the central flux
 // minus the grid-velocity flux as (F(l) + F(r)) . n / 2 - (l + r) vn / 2 with the face-relative
 // normal velocities vl - vn and vr - vn, and the third difference in F's orientation.
-__device__ __forceinline__ void jst_pair(const St& ll, const St& l, const St& r, const St& rr,
-                                         double nx, double nz, double len, double vn, double sl,
-                                         double sr, const Instance& in, Flux& F, Flux& Fp) {
-  const double vl = (nx * l.j1 + nz * l.j2) * l.ir;
-  const double vr = (nx * r.j1 + nz * r.j2) * r.ir;
-  const double al = fabs(vl) + l.cs * len, ar = fabs(vr) + r.cs * len;
-  const double lam = max_cd(al, ar), lamp = max_cd(ar, al);
-  const double coef2 = in.k2 * max_cd(sl, sr) * lam;
-  const double coef2p = in.k2 * max_cd(sr, sl) * lamp;
-  const double c4 = in.k4 * lam - in.c4 * coef2;
-  const double c4p = in.k4 * lamp - in.c4 * coef2p;
-  const double coef4 = (0.0 > c4 + 1e-8) ? 0.0 : c4;
-  const double coef4p = (0.0 > c4p + 1e-8) ? 0.0 : c4p;
-  const double wl = vl - vn, wr = vr - vn, ps = l.p + r.p;
-  const double ca[4] = {0.5 * fma(l.rho, wl, r.rho * wr),
-                        0.5 * fma(l.j1, wl, fma(r.j1, wr, nx * ps)),
-                        0.5 * fma(l.j2, wl, fma(r.j2, wr, nz * ps)),
-                        0.5 * fma(l.e, wl, fma(r.e, wr, fma(l.p, vl, r.p * vr)))};
-  const double lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
-  const double llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
+template <class T>
+__device__ __forceinline__ void jst_pair(const St<T>& ll, const St<T>& l, const St<T>& r,
+                                         const St<T>& rr, const T& nx, const T& nz,
+                                         const T& len, const T& vn, const T& sl, const T& sr,
+                                         const Instance& in, Flux<T>& F, Flux<T>& Fp) {
+  const T vl = (nx * l.j1 + nz * l.j2) * l.ir;
+  const T vr = (nx * r.j1 + nz * r.j2) * r.ir;
+  // F' sees the normal velocities -vr, -vl: abs_c takes its derivative's sign from the value
+  // with zeros as positive, so at a zero velocity the two orientations' derivatives differ
+  // (the values, and plain-double results, do not)
+  const T al = abs_c(vl) + l.cs * len, ar = abs_c(vr) + r.cs * len;
+  const T alp = abs_c(-vl) + l.cs * len, arp = abs_c(-vr) + r.cs * len;
+  const T lam = max_c(al, ar), lamp = max_c(arp, alp);
+  const T coef2 = in.k2 * max_c(sl, sr) * lam;
+  const T coef2p = in.k2 * max_c(sr, sl) * lamp;
+  const T coef4 = max_c0(in.k4 * lam - in.c4 * coef2);
+  const T coef4p = max_c0(in.k4 * lamp - in.c4 * coef2p);
+  const T wl = vl - vn, wr = vr - vn, ps = l.p + r.p;
+  const T ca[4] = {0.5 * fmad(l.rho, wl, r.rho * wr),
+                   0.5 * fmad(l.j1, wl, fmad(r.j1, wr, nx * ps)),
+                   0.5 * fmad(l.j2, wl, fmad(r.j2, wr, nz * ps)),
+                   0.5 * fmad(l.e, wl, fmad(r.e, wr, fmad(l.p, vl, r.p * vr)))};
+  const T lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
+  const T llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const double d1 = rv[k] - lv[k];
-    const double d3 = fma(3.0, lv[k], fma(-3.0, rv[k], rrv[k])) - llv[k];
-    F.f[k] = fma(coef4, d3, fma(-coef2, d1, ca[k]));
-    Fp.f[k] = fma(-coef4p, d3, fma(coef2p, d1, -ca[k]));
+    const T d1 = rv[k] - lv[k];
+    const T d3 = fmad(3.0, lv[k], fmad(-3.0, rv[k], rrv[k])) - llv[k];
+    F.f[k] = fmad(coef4, d3, fmad(-coef2, d1, ca[k]));
+    Fp.f[k] = fmad(-coef4p, d3, fmad(coef2p, d1, -ca[k]));
   }
 }
 
 // Phases 2-4 of a tile whose states (with derived quantities) and vertices are staged in S:
-// sensors, faces, and the residual of the tile's cells. Every thread of the CTA calls it.
-__device__ __forceinline__ void tile_compute(TileSmem& S, const Instance& in, int m0, int n0,
-                                             double* R) {
+// sensors, faces, and the residual (or its tangent part) of the tile's cells. Every thread of
+// the CTA calls it.
+template <class T>
+__device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in, const T& mach,
+                                             int m0, int n0, double* R, double* dR, int h) {
   const int M = in.M, N = in.N;
   const int tid = threadIdx.x;
   // 2. sensors centred on each needed state
@@ -182,16 +222,16 @@ __device__ __forceinline__ void tile_compute(TileSmem& S, const Instance& in, in
   for (int e = tid; e < (kTM + 2) * kTN; e += kThreads) {
     const int r = e % (kTM + 2) - 1, c = e / (kTM + 2);
     const int m = m0 + r;
-    double s = 0.0;
+    T s = lift<T>(0.0);
     if (m == 0) {  // inner neighbour: the wall ghost of this wall cell (face o, flag 1)
-      const double nx = S.z[vidx(r, c + 1)] - S.z[vidx(r, c)];
-      const double nz = S.x[vidx(r, c)] - S.x[vidx(r, c + 1)];
-      const double gx = (S.vx[vidx(r, c)] + S.vx[vidx(r, c + 1)]) / 2.0;
-      const double gz = (S.vz[vidx(r, c)] + S.vz[vidx(r, c + 1)]) / 2.0;
-      const St gh = wall_ghost_st(staged(S, sidx(r, c)), nx, nz, gx, gz);
+      const T nx = S.z[vidx(r, c + 1)] - S.z[vidx(r, c)];
+      const T nz = S.x[vidx(r, c)] - S.x[vidx(r, c + 1)];
+      const T gx = (S.vx[vidx(r, c)] + S.vx[vidx(r, c + 1)]) / 2.0;
+      const T gz = (S.vz[vidx(r, c)] + S.vz[vidx(r, c + 1)]) / 2.0;
+      const St<T> gh = wall_ghost_st(staged(S, sidx(r, c)), nx, nz, gx, gz);
       s = sensor(gh.p, S.p[sidx(r, c)], S.p[sidx(r + 1, c)]);
     } else if (m == M - 1) {  // outer neighbour: the far-field ghost (face i, flag 5)
-      const St gh = farfield_ghost_st(staged(S, sidx(r, c)), in);
+      const St<T> gh = farfield_ghost_st(staged(S, sidx(r, c)), mach, in);
       s = sensor(gh.p, S.p[sidx(r, c)], S.p[sidx(r - 1, c)]);
     } else if (m > 0 && m < M - 1) {
       s = sensor(S.p[sidx(r - 1, c)], S.p[sidx(r, c)], S.p[sidx(r + 1, c)]);
@@ -208,16 +248,18 @@ __device__ __forceinline__ void tile_compute(TileSmem& S, const Instance& in, in
   const int r = tid % kTM, c = tid / kTM;
   const int m = m0 + r, n = n0 + c;
   const bool own = m < M && n < N;
-  Flux Fb{}, Fi{};
+  Flux<T> Fb, Fi;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) Fb.f[k] = Fi.f[k] = lift<T>(0.0);
   auto exists = [&](int rr, int cc) { return rr >= 0 && cc >= 0 && m0 + rr < M && n0 + cc < N; };
-  auto angular_face = [&](int fr, int fc, bool want_b, bool want_f, Flux& Fb_out) {
+  auto angular_face = [&](int fr, int fc, bool want_b, bool want_f, Flux<T>& Fb_out) {
     // l = (fr, fc), r = (fr, fc - 1): face b of (fr, fc) and face f of (fr, fc - 1)
-    const double nbx = S.z[vidx(fr, fc)] - S.z[vidx(fr + 1, fc)];
-    const double nbz = S.x[vidx(fr + 1, fc)] - S.x[vidx(fr, fc)];
-    const double vn = (S.vx[vidx(fr + 1, fc)] + S.vx[vidx(fr, fc)]) / 2.0 * nbx +
-                      (S.vz[vidx(fr + 1, fc)] + S.vz[vidx(fr, fc)]) / 2.0 * nbz;
-    const double len = sqrt(nbx * nbx + nbz * nbz);
-    Flux F, Fp;
+    const T nbx = S.z[vidx(fr, fc)] - S.z[vidx(fr + 1, fc)];
+    const T nbz = S.x[vidx(fr + 1, fc)] - S.x[vidx(fr, fc)];
+    const T vn = (S.vx[vidx(fr + 1, fc)] + S.vx[vidx(fr, fc)]) / 2.0 * nbx +
+                 (S.vz[vidx(fr + 1, fc)] + S.vz[vidx(fr, fc)]) / 2.0 * nbz;
+    const T len = sqrt_(nbx * nbx + nbz * nbz);
+    Flux<T> F, Fp;
     jst_pair(staged(S, sidx(fr, fc + 1)), staged(S, sidx(fr, fc)), staged(S, sidx(fr, fc - 1)),
              staged(S, sidx(fr, fc - 2)), nbx, nbz, len, vn, S.s_ang[fc * kTM + fr + kTM],
              S.s_ang[(fc - 1) * kTM + fr + kTM], in, F, Fp);
@@ -226,46 +268,48 @@ __device__ __forceinline__ void tile_compute(TileSmem& S, const Instance& in, in
 #pragma unroll
       for (int k = 0; k < 4; ++k) S.ff[k][fc - 1][fr] = Fp.f[k];
   };
-  auto radial_face = [&](int fr, int fc, bool want_i, bool want_o, Flux& Fi_out) {
+  auto radial_face = [&](int fr, int fc, bool want_i, bool want_o, Flux<T>& Fi_out) {
     // l = (fr, fc), r = (fr - 1, fc): face i of (fr, fc) and face o of (fr - 1, fc)
     const int fm = m0 + fr;
-    const double nix = S.z[vidx(fr, fc + 1)] - S.z[vidx(fr, fc)];
-    const double niz = S.x[vidx(fr, fc)] - S.x[vidx(fr, fc + 1)];
-    const double gx = (S.vx[vidx(fr, fc)] + S.vx[vidx(fr, fc + 1)]) / 2.0;
-    const double gz = (S.vz[vidx(fr, fc)] + S.vz[vidx(fr, fc + 1)]) / 2.0;
-    const double vn = gx * nix + gz * niz;
-    Flux F{}, Fp{};
+    const T nix = S.z[vidx(fr, fc + 1)] - S.z[vidx(fr, fc)];
+    const T niz = S.x[vidx(fr, fc)] - S.x[vidx(fr, fc + 1)];
+    const T gx = (S.vx[vidx(fr, fc)] + S.vx[vidx(fr, fc + 1)]) / 2.0;
+    const T gz = (S.vz[vidx(fr, fc)] + S.vz[vidx(fr, fc + 1)]) / 2.0;
+    const T vn = gx * nix + gz * niz;
+    Flux<T> F, Fp;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) F.f[k] = Fp.f[k] = lift<T>(0.0);
     if (fm == 0) {  // wall face of cell 0 (flag 1): central flux with the wall ghost
-      const St C = staged(S, sidx(fr, fc));
+      const St<T> C = staged(S, sidx(fr, fc));
       F = central(C, wall_ghost_st(C, nix, niz, gx, gz), nix, niz, vn);
     } else if (fm == M) {  // far-field face of cell M-1 (flag 5): central flux with the ghost
-      const St C = staged(S, sidx(fr - 1, fc));
-      Fp = central(C, farfield_ghost_st(C, in), -nix, -niz, -vn);
+      const St<T> C = staged(S, sidx(fr - 1, fc));
+      Fp = central(C, farfield_ghost_st(C, mach, in), -nix, -niz, -vn);
     } else {
-      const double len = sqrt(nix * nix + niz * niz);
-      const St L = staged(S, sidx(fr, fc)), R = staged(S, sidx(fr - 1, fc));
-      const double sl = S.s_rad[fc * (kTM + 2) + fr + 1], sr = S.s_rad[fc * (kTM + 2) + fr];
+      const T len = sqrt_(nix * nix + niz * niz);
+      const St<T> L = staged(S, sidx(fr, fc)), Rs = staged(S, sidx(fr - 1, fc));
+      const T sl = S.s_rad[fc * (kTM + 2) + fr + 1], sr = S.s_rad[fc * (kTM + 2) + fr];
       if (fm == 1) {
         // face i of cell 1 (flag 2): central; face o of cell 0 (flag 1): JST whose outer
         // neighbour is the wall ghost of cell 0
-        F = central(L, R, nix, niz, vn);
+        F = central(L, Rs, nix, niz, vn);
         if (want_o) {
-          const double wx = S.z[vidx(fr - 1, fc + 1)] - S.z[vidx(fr - 1, fc)];
-          const double wz = S.x[vidx(fr - 1, fc)] - S.x[vidx(fr - 1, fc + 1)];
-          const double wgx = (S.vx[vidx(fr - 1, fc)] + S.vx[vidx(fr - 1, fc + 1)]) / 2.0;
-          const double wgz = (S.vz[vidx(fr - 1, fc)] + S.vz[vidx(fr - 1, fc + 1)]) / 2.0;
-          Fp = jst(wall_ghost_st(R, wx, wz, wgx, wgz), R, L, staged(S, sidx(fr + 1, fc)), -nix,
+          const T wx = S.z[vidx(fr - 1, fc + 1)] - S.z[vidx(fr - 1, fc)];
+          const T wz = S.x[vidx(fr - 1, fc)] - S.x[vidx(fr - 1, fc + 1)];
+          const T wgx = (S.vx[vidx(fr - 1, fc)] + S.vx[vidx(fr - 1, fc + 1)]) / 2.0;
+          const T wgz = (S.vz[vidx(fr - 1, fc)] + S.vz[vidx(fr - 1, fc + 1)]) / 2.0;
+          Fp = jst(wall_ghost_st(Rs, wx, wz, wgx, wgz), Rs, L, staged(S, sidx(fr + 1, fc)), -nix,
                    -niz, len, -vn, sr, sl, in);
         }
       } else if (fm == M - 1) {
         // face i of cell M-1 (flag 5): JST whose outer neighbour is the far-field ghost;
         // face o of cell M-2 (flag 4): central
-        F = jst(farfield_ghost_st(L, in), L, R, staged(S, sidx(fr - 2, fc)), nix, niz, len, vn, sl,
-                sr, in);
-        Fp = central(R, L, -nix, -niz, -vn);
+        F = jst(farfield_ghost_st(L, mach, in), L, Rs, staged(S, sidx(fr - 2, fc)), nix, niz,
+                len, vn, sl, sr, in);
+        Fp = central(Rs, L, -nix, -niz, -vn);
       } else {
-        jst_pair(staged(S, sidx(fr + 1, fc)), L, R, staged(S, sidx(fr - 2, fc)), nix, niz, len, vn,
-                 sl, sr, in, F, Fp);
+        jst_pair(staged(S, sidx(fr + 1, fc)), L, Rs, staged(S, sidx(fr - 2, fc)), nix, niz, len,
+                 vn, sl, sr, in, F, Fp);
       }
     }
     if (want_i) Fi_out = F;
@@ -277,39 +321,70 @@ __device__ __forceinline__ void tile_compute(TileSmem& S, const Instance& in, in
   if (m <= M && n < N) radial_face(r, c, own, exists(r - 1, c), Fi);
   if (tid < kTM) {
     if (exists(tid, kTN - 1)) {
-      Flux unused;
+      Flux<T> unused;
       angular_face(tid, kTN, false, true, unused);
     }
   } else if (tid < kTM + kTN) {
     if (exists(kTM - 1, tid - kTM)) {
-      Flux unused;
+      Flux<T> unused;
       radial_face(kTM, tid - kTM, false, true, unused);
     }
   }
   __syncthreads();
   if (!own) return;
-  const double bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
-  const double fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
-  const double fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
-  const double box = S.x[vidx(r + 1, c)], boz = S.z[vidx(r + 1, c)];
-  const double area = fabs((fox - bix) * (boz - fiz) - (foz - biz) * (box - fix)) / 2.0;
-  const double ia = 1.0 / area;
-  double res[4];
+  const T bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
+  const T fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
+  const T fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
+  const T box = S.x[vidx(r + 1, c)], boz = S.z[vidx(r + 1, c)];
+  const T area = abs_c((fox - bix) * (boz - fiz) - (foz - biz) * (box - fix)) / 2.0;
+  const T ia = 1.0 / area;
+  T res[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) res[k] = -(((Fb.f[k] + S.ff[k][c][r]) + Fi.f[k]) + S.fo[k][c][r]) * ia;
-  double* out = R + 4 * (in.cell_offset + m + (int64_t)M * n);
-  reinterpret_cast<double2*>(out)[0] = make_double2(res[0], res[1]);
-  reinterpret_cast<double2*>(out)[1] = make_double2(res[2], res[3]);
+  const int64_t g = in.cell_offset + m + (int64_t)M * n;
+  if constexpr (std::is_same<T, double>::value) {
+    double* out = R + 4 * g;
+    reinterpret_cast<double2*>(out)[0] = make_double2(res[0], res[1]);
+    reinterpret_cast<double2*>(out)[1] = make_double2(res[2], res[3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dR[8 * g + 2 * k + h] = res[k].d[0];
+    if (R && h == 0) {
+      double* out = R + 4 * g;
+      reinterpret_cast<double2*>(out)[0] = make_double2(res[0].v, res[1].v);
+      reinterpret_cast<double2*>(out)[1] = make_double2(res[2].v, res[3].v);
+    }
+  }
 }
 
-// Three CTAs per SM (80 registers, with a few spills): on the 256-instance 129x129 batch this
-// runs 11 % faster than two CTAs at 120 registers and 4 % faster than four at 64.
-__global__ void __launch_bounds__(kThreads, 3)
-k_residual_tiled(Table t, const double* X, const double* V, const double* U, double* R) {
+// Scalar of type T from a value and (for the dual) part h of an interleaved complex tangent.
+template <class T>
+__device__ __forceinline__ T with_part(double v, const double* d, int64_t at, int h) {
+  if constexpr (std::is_same<T, double>::value) {
+    return v;
+  } else {
+    T r;
+    r.v = v;
+    r.d[0] = d ? __ldg(d + at + h) : 0.0;
+    return r;
+  }
+}
+
+// Residual: three CTAs per SM (80 registers, with a few spills); on the 256-instance 129x129
+// batch this runs 11 % faster than two CTAs at 120 registers and 4 % faster than four at 64.
+// Tangent (twice the shared memory): two CTAs per SM.
+template <class T>
+constexpr int kMinBlocks = std::is_same<T, double>::value ? 3 : 2;
+
+template <class T>
+__global__ void __launch_bounds__(kThreads, kMinBlocks<T>)
+k_residual_tiled(Table t, const double* X, const double* V, const double* U, const double* dX,
+                 const double* dV, const double* dU, const double* dMa, double* R, double* dR) {
   extern __shared__ __align__(16) unsigned char tile_smem[];
-  TileSmem& S = *reinterpret_cast<TileSmem*>(tile_smem);
+  TileSmem<T>& S = *reinterpret_cast<TileSmem<T>*>(tile_smem);
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;
   const int M = in.M, N = in.N;
+  const int h = blockIdx.z;  // part of the tangent direction (dual kernel only)
   const int tiles_m = (M + kTM - 1) / kTM;
   const int tiles = tiles_m * ((N + kTN - 1) / kTN);
   if ((int)blockIdx.x >= tiles) return;
@@ -317,6 +392,10 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
   const double* Ui = U + 4 * in.cell_offset;
   const double* Xi = X + 2 * in.vert_offset;
   const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
+  const double* dUi = dU ? dU + 8 * in.cell_offset : nullptr;
+  const double* dXi = dX ? dX + 4 * in.vert_offset : nullptr;
+  const double* dVi = dV ? dV + 4 * in.vert_offset : nullptr;
+  const T mach = with_part<T>(in.mach, dMa, 2 * (int64_t)blockIdx.y, h);
   const int tid = threadIdx.x;
 
   // 1. stage states (cross-shaped halo) and derived quantities, vertices and grid velocities.
@@ -325,6 +404,7 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
   // its loads are in flight together instead of one round after another.
   static_assert(kStaged <= 2 * kThreads && kVerts <= 2 * kThreads, "two staging rounds");
   double2 sa[2], sb[2], xv[2], vv[2];
+  int64_t sj[2], vj[2];
   bool sval[2];
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
@@ -335,22 +415,25 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
     sval[k] = e < kStaged && !corner && m >= 0 && m < M;
     sa[k] = make_double2(1.0, 0.0);
     sb[k] = make_double2(0.0, 1.0);
+    sj[k] = 0;
     if (sval[k]) {
       int n = n0 + c;  // periodic in the angular index: n0 + c lies in [-2, N + kTN + 1]
       while (n < 0) n += N;
       while (n >= N) n -= N;
-      const double* q = Ui + 4 * (m + (int64_t)M * n);
+      sj[k] = m + (int64_t)M * n;
+      const double* q = Ui + 4 * sj[k];
       sa[k] = __ldg(reinterpret_cast<const double2*>(q));
       sb[k] = __ldg(reinterpret_cast<const double2*>(q + 2));
     }
     const int ev = tid + k * kThreads;
     xv[k] = make_double2(0.0, 0.0);
     vv[k] = make_double2(0.0, 0.0);
+    vj[k] = 0;
     if (ev < kVerts) {
       const int vm = min(m0 + ev % kVR, M), vn = min(n0 + ev / kVR, N);
-      const int64_t v = vm + (int64_t)(M + 1) * vn;
-      xv[k] = __ldg(reinterpret_cast<const double2*>(Xi + 2 * v));
-      if (Vi) vv[k] = __ldg(reinterpret_cast<const double2*>(Vi + 2 * v));
+      vj[k] = vm + (int64_t)(M + 1) * vn;
+      xv[k] = __ldg(reinterpret_cast<const double2*>(Xi + 2 * vj[k]));
+      if (Vi) vv[k] = __ldg(reinterpret_cast<const double2*>(Vi + 2 * vj[k]));
     }
   }
 #pragma unroll
@@ -358,35 +441,52 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, dou
     const int e = tid + k * kThreads;
     if (e < kStaged) {
       if (sval[k]) {
-        const St st = derive(sa[k].x, sa[k].y, sb[k].x, sb[k].y);
+        const double* dq = dUi ? dUi + 8 * sj[k] : nullptr;
+        const St<T> st = derive<T>(with_part<T>(sa[k].x, dq, 0, h), with_part<T>(sa[k].y, dq, 2, h),
+                                   with_part<T>(sb[k].x, dq, 4, h), with_part<T>(sb[k].y, dq, 6, h));
         S.rho[e] = st.rho; S.j1[e] = st.j1; S.j2[e] = st.j2; S.e[e] = st.e;
         S.p[e] = st.p; S.ir[e] = st.ir; S.cs[e] = st.cs;
       } else {  // outside the grid or an unused corner: finite placeholders
-        S.rho[e] = 1.0; S.j1[e] = 0.0; S.j2[e] = 0.0; S.e[e] = 1.0;
-        S.p[e] = 1.0; S.ir[e] = 1.0; S.cs[e] = 1.0;
+        S.rho[e] = lift<T>(1.0); S.j1[e] = lift<T>(0.0); S.j2[e] = lift<T>(0.0);
+        S.e[e] = lift<T>(1.0); S.p[e] = lift<T>(1.0); S.ir[e] = lift<T>(1.0);
+        S.cs[e] = lift<T>(1.0);
       }
     }
     if (e < kVerts) {
-      S.x[e] = xv[k].x;
-      S.z[e] = xv[k].y;
-      S.vx[e] = vv[k].x;
-      S.vz[e] = vv[k].y;
+      S.x[e] = with_part<T>(xv[k].x, dXi, 4 * vj[k], h);
+      S.z[e] = with_part<T>(xv[k].y, dXi, 4 * vj[k] + 2, h);
+      S.vx[e] = with_part<T>(vv[k].x, dVi, 4 * vj[k], h);
+      S.vz[e] = with_part<T>(vv[k].y, dVi, 4 * vj[k] + 2, h);
     }
   }
   __syncthreads();
 
-  tile_compute(S, in, m0, n0, R);
+  tile_compute<T>(S, in, mach, m0, n0, R, dR, h);
 }
 
 int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
                           double* R, cudaStream_t stream, int max_tiles) {
   const Table t = make_table(b);
   dim3 grid(max_tiles, b->n_inst);
-  if (cudaFuncSetAttribute(k_residual_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(TileSmem)) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_residual_tiled<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(TileSmem<double>)) != cudaSuccess)
     return check_launch("compute_odes attribute");
-  k_residual_tiled<<<grid, kThreads, sizeof(TileSmem), stream>>>(t, X, V, U, R);
+  k_residual_tiled<double><<<grid, kThreads, sizeof(TileSmem<double>), stream>>>(
+      t, X, V, U, nullptr, nullptr, nullptr, nullptr, R, nullptr);
   return check_launch("compute_odes");
+}
+
+int launch_tangent_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
+                         const double* dU, const double* dX, const double* dV, const double* dMa,
+                         double* dR, double* R, cudaStream_t stream, int max_tiles) {
+  const Table t = make_table(b);
+  dim3 grid(max_tiles, b->n_inst, 2);
+  if (cudaFuncSetAttribute(k_residual_tiled<D1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(TileSmem<D1>)) != cudaSuccess)
+    return check_launch("apply_odes_tangent attribute");
+  k_residual_tiled<D1><<<grid, kThreads, sizeof(TileSmem<D1>), stream>>>(t, X, V, U, dX, dV, dU,
+                                                                         dMa, R, dR);
+  return check_launch("apply_odes_tangent");
 }
 
 int residual_tiles(int M, int N) { return ((M + kTM - 1) / kTM) * ((N + kTN - 1) / kTN); }
