@@ -214,12 +214,17 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
                                              int m0, int n0, double* R, double* dR, int h) {
   const int M = in.M, N = in.N;
   const int tid = threadIdx.x;
-  // 2. sensors centred on each needed state
-  for (int e = tid; e < kTM * (kTN + 2); e += kThreads) {
+  // 2. sensors centred on each needed state: every thread evaluates one angular and one radial
+  // sensor, and the kAngX + kRadX left over go to warps 2-4, so that no warp evaluates more
+  // than three (the phase ends at a barrier: its slowest warp sets its time)
+  constexpr int kAng = kTM * (kTN + 2), kRad = (kTM + 2) * kTN;
+  constexpr int kAngX = kAng - kThreads, kRadX = kRad - kThreads, kX0 = 64;
+  static_assert(kAngX >= 0 && kRadX >= 0 && kX0 + kAngX + kRadX <= kThreads, "sensor split");
+  auto angular_sensor = [&](int e) {
     const int r = e % kTM, c = e / kTM - 1;
     S.s_ang[e] = sensor(S.p[sidx(r, c - 1)], S.p[sidx(r, c)], S.p[sidx(r, c + 1)]);
-  }
-  for (int e = tid; e < (kTM + 2) * kTN; e += kThreads) {
+  };
+  auto radial_sensor = [&](int e) {
     const int r = e % (kTM + 2) - 1, c = e / (kTM + 2);
     const int m = m0 + r;
     T s = lift<T>(0.0);
@@ -237,7 +242,12 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
       s = sensor(S.p[sidx(r - 1, c)], S.p[sidx(r, c)], S.p[sidx(r + 1, c)]);
     }
     S.s_rad[e] = s;
-  }
+  };
+  angular_sensor(tid);
+  radial_sensor(tid);
+  if (tid >= kX0 && tid < kX0 + kAngX) angular_sensor(kThreads + tid - kX0);
+  else if (tid >= kX0 + kAngX && tid < kX0 + kAngX + kRadX)
+    radial_sensor(kThreads + tid - kX0 - kAngX);
   __syncthreads();
 
   // 3. faces. Thread (r, c) evaluates the angular face between cells (r, c-1) and (r, c) and the
@@ -401,18 +411,22 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, con
   // 1. stage states (cross-shaped halo) and derived quantities, vertices and grid velocities.
   // A thread first issues all of its global loads (at most two staged states and two vertex
   // pairs: kStaged = 432 and kVerts = 297 are below 2 * kThreads), then derives and stores, so
-  // its loads are in flight together instead of one round after another.
+  // its loads are in flight together instead of one round after another. The second-round
+  // states go to the highest threads and the second-round vertices to the lowest, so that no
+  // warp derives a second state and also stages a second vertex.
   static_assert(kStaged <= 2 * kThreads && kVerts <= 2 * kThreads, "two staging rounds");
+  auto state_item = [&](int k) { return k == 0 ? tid : tid + kStaged - kThreads; };
+  auto state_valid = [&](int k, int e) { return (k == 0 || e >= kThreads) && e < kStaged; };
   double2 sa[2], sb[2], xv[2], vv[2];
   int64_t sj[2], vj[2];
   bool sval[2];
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
-    const int e = tid + k * kThreads;
+    const int e = state_item(k);
     const int r = e % kSR - 2, c = e / kSR - 2;
     const bool corner = (r < 0 || r >= kTM) && (c < 0 || c >= kTN);
     const int m = m0 + r;
-    sval[k] = e < kStaged && !corner && m >= 0 && m < M;
+    sval[k] = state_valid(k, e) && !corner && m >= 0 && m < M;
     sa[k] = make_double2(1.0, 0.0);
     sb[k] = make_double2(0.0, 1.0);
     sj[k] = 0;
@@ -438,8 +452,8 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, con
   }
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
-    const int e = tid + k * kThreads;
-    if (e < kStaged) {
+    const int e = state_item(k);
+    if (state_valid(k, e)) {
       if (sval[k]) {
         const double* dq = dUi ? dUi + 8 * sj[k] : nullptr;
         const St<T> st = derive<T>(with_part<T>(sa[k].x, dq, 0, h), with_part<T>(sa[k].y, dq, 2, h),
@@ -452,11 +466,12 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, con
         S.cs[e] = lift<T>(1.0);
       }
     }
-    if (e < kVerts) {
-      S.x[e] = with_part<T>(xv[k].x, dXi, 4 * vj[k], h);
-      S.z[e] = with_part<T>(xv[k].y, dXi, 4 * vj[k] + 2, h);
-      S.vx[e] = with_part<T>(vv[k].x, dVi, 4 * vj[k], h);
-      S.vz[e] = with_part<T>(vv[k].y, dVi, 4 * vj[k] + 2, h);
+    const int ev = tid + k * kThreads;
+    if (ev < kVerts) {
+      S.x[ev] = with_part<T>(xv[k].x, dXi, 4 * vj[k], h);
+      S.z[ev] = with_part<T>(xv[k].y, dXi, 4 * vj[k] + 2, h);
+      S.vx[ev] = with_part<T>(vv[k].x, dVi, 4 * vj[k], h);
+      S.vz[ev] = with_part<T>(vv[k].y, dVi, 4 * vj[k] + 2, h);
     }
   }
   __syncthreads();
