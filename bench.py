@@ -275,6 +275,79 @@ def cpu_resolvent_rate(X, V, U, mach: float, shift: complex) -> dict:
                       "core.py:512-565"}
 
 
+def cpu_linear_rates(X, V, U, mach: float) -> dict:
+    """The reference's own linearisation procedures on the host, in its single thread (the
+    oracle restatement of src/spatial_discretization.f90): the complex-step d(odes)/d(states)
+    Jacobian (f90:666-750), the four forward and the four reverse products with the stored
+    Jacobians (f90:604-650, 825-918, 1005-1072) of one 128x128 instance, and the matrix-vector
+    product of the CSR matrix that _assemble_csr builds (core.py:512-531) under scipy."""
+    from scipy.sparse import bsr_array
+
+    from oracle.shim import SpatialDiscretizationModule
+
+    M, N = U.shape[1], U.shape[2]
+    disc = SpatialDiscretizationModule()
+    disc.aoa[...] = FLOW["aoa_deg"]
+    Xc, Vc, Uc = (np.asfortranarray(np.asarray(a, dtype=complex)) for a in (X, V, U))
+    J_u = np.zeros((4, 4, M, N, 9), order="F")
+    J_x = np.zeros((4, 2, M, N, 4), order="F")
+    J_v = np.zeros((4, 2, M, N, 4), order="F")
+    J_m = np.zeros((4, 1, M, N), order="F")
+
+    def per_call(fn, budget=0.5):
+        fn()
+        n, t0 = 0, time.perf_counter()
+        while True:
+            fn()
+            n += 1
+            t = time.perf_counter() - t0
+            if t >= budget:
+                return t / n
+
+    t_jac = per_call(lambda: disc.compute_odes_wrt_states(mach, Xc, Vc, Uc, J_u), 1.0)
+    disc.compute_odes_wrt_vertices(mach, Xc, Vc, Uc, J_x)
+    disc.compute_odes_wrt_velocities(mach, Xc, Vc, Uc, J_v)
+    disc.compute_odes_wrt_mach(mach, Xc, Vc, Uc, J_m)
+    rng = np.random.default_rng(9)
+
+    def crand(shape):
+        return np.asfortranarray(rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+
+    cells, verts = (4, M, N), (2, M + 1, N + 1)
+    w, gU, gX, gV, gM = crand(cells), crand(cells), crand(verts), crand(verts), crand((1,))
+
+    def vjp():
+        disc.apply_odes_wrt_states_rev(J_u, w, gU)
+        disc.apply_odes_wrt_vertices_rev(J_x, w, gX)
+        disc.apply_odes_wrt_vertices_rev(J_v, w, gV)
+        disc.apply_odes_wrt_mach_rev(J_m, w, gM)
+
+    dU, dXv, dVv, dm = crand(cells), crand(verts), crand(verts), crand((1,))
+    jR = [crand(cells) for _ in range(4)]
+
+    def jvp():
+        disc.apply_odes_wrt_states_fwd(J_u, dU, jR[0])
+        disc.apply_odes_wrt_vertices_fwd(J_x, dXv, jR[1])
+        disc.apply_odes_wrt_vertices_fwd(J_v, dVv, jR[2])
+        disc.apply_odes_wrt_mach_fwd(J_m, dm, jR[3])
+
+    t_vjp, t_jvp = per_call(vjp), per_call(jvp)
+    nnzb = (9 * M - 6) * N
+    data = np.empty((4, 4, nnzb), order="F")
+    idx = np.empty(nnzb, dtype=np.intc)
+    ptr = np.empty(M * N + 1, dtype=np.intc)
+    disc.convert_odes_wrt_states(J_u, data, idx, ptr)
+    A = bsr_array((np.moveaxis(data, -1, 0), idx - 1, ptr - 1), dtype=complex).tocsr()
+    x = crand(4 * M * N)
+    t_spmv = per_call(lambda: A @ x)
+    return {"jacobian_states": {"value": M * N / t_jac, "unit": "cells/s"},
+            "vjp": {"value": 1.0 / t_vjp, "unit": "VJP/s (four reverse products, one instance)"},
+            "jvp": {"value": 1.0 / t_jvp, "unit": "JVP/s (four forward products, one instance)"},
+            "bsr_spmv": {"value": 1.0 / t_spmv, "unit": "SpMV/s (scipy CSR, complex x)"},
+            "cores": 1, "kind": "port", "cpu": cpu_model(),
+            "sample": f"one {M}x{N}-cell instance, each procedure repeated for >= 0.5 s"}
+
+
 # ---- B200 arm -------------------------------------------------------------------------------
 
 def read_traffic() -> float | None:
@@ -437,7 +510,7 @@ def run_b200(args) -> None:
     # matrix-free forward tangent (complex dU, dX, dV, dMa in one stencil pass) of every
     # instance, and the shifted BSR SpMV (A - s I) x cycled over the BSR forms of
     # LINEAR_SPMV_INSTANCES instances (more bytes than L2 holds, so every pass reads HBM)
-    linear = None
+    linear = cpu_lin = None
     if "linear" in parts:
         def per_call(fn, n):
             for _ in range(args.warmup):
@@ -542,6 +615,12 @@ def run_b200(args) -> None:
                          "issue": f"the {n_mat} calls captured in one CUDA graph on "
                                   f"{SPMV_STREAMS} streams, replayed"},
             "peak_gbs": peak}
+        if rank == 0 and not args.no_cpu_baseline:
+            cpu_lin = cpu_linear_rates(X, V, Us[0], FLOW["mach"])
+            linear["cpu_reference_method"] = cpu_lin
+            for key in ("jacobian_states", "jvp", "bsr_spmv"):
+                linear[key]["vs_cpu_reference_method"] = \
+                    linear[key]["value"] / cpu_lin[key]["value"]
         del J_u, tU, tX, tV, tR, mats, sx, sy, spmv_graph, side
 
     # resolvent: the frequency response of the steady state (PTC from free stream), 64 shifts
@@ -555,6 +634,7 @@ def run_b200(args) -> None:
         sd = SpatialDiscretization(X, mach_number=FLOW["mach"], angle_of_attack=FLOW["aoa_deg"],
                                    coefficient_length=GRID["chord"],
                                    coefficient_center=FLOW["center"])
+        sd_rings, sd_cols = sd.num_radial, sd.num_angular
         t0 = time.perf_counter()
         hist = drivers.ptc(sd, rtol=1e-10, max_iter=200)
         t_ptc = time.perf_counter() - t0
@@ -593,6 +673,10 @@ def run_b200(args) -> None:
                "shifts": len(ks), "shift_group": group, "seconds": t_batched,
                "plain": {"value": plain_rate, "shifts": len(ks_plain), "seconds": t_plain},
                "batched_vs_plain": batched_rate / plain_rate,
+               "achieved_tflops": len(ks) * sd_rings * 4 * (4 * sd_cols) ** 3 * 8 / t_batched / 1e12,
+               "flops": "4 (4N)^3 complex multiply-adds (8 flops) per ring and shift: the "
+                        "Gauss-Jordan inversion and the three Schur / L products of the "
+                        "factorisation, over the whole batched time",
                "max_rel_diff_batched_vs_plain": agree,
                "adjoint_gradient_rel_diff": float(np.max(np.abs(grad_b - grad_p))
                                                   / np.max(np.abs(grad_p))),
@@ -699,7 +783,10 @@ def run_b200(args) -> None:
         "clocks": clk,
         "vjp": None if vjp_rate is None else {
             "value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
-            "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4},
+            "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4,
+            "cpu_reference_method": None if cpu_lin is None else cpu_lin["vjp"],
+            "vs_cpu_reference_method": None if cpu_lin is None
+            else vjp_rate / cpu_lin["vjp"]["value"]},
         "linear": linear,
         "resolvent": res,
         "uneven": uneven,
