@@ -60,7 +60,7 @@ PROFILE_SUMMARY = ROOT / "profiles" / "residual_tiled_naca0004_129x129.md"
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--instances", type=int, default=256, help="instances per GPU")

@@ -23,8 +23,8 @@
 // relative); every branch (boundary cases, max_c tolerance) follows the reference.
 //
 // The kernel is a template on its scalar type T. T = double is the residual. T = Dual<double,
-// 1> is the tangent along a complex direction (dU, dX, dV, dMa): the CTAs of grid slice z = h
-// carry part h (0: real, 1: imaginary) of the direction as the dual component, with abs_c /
+// 1> is the tangent along a complex direction (dU, dX, dV, dMa): CTA 2 t + h of a tile t
+// carries part h (0: real, 1: imaginary) of the direction as the dual component, with abs_c /
 // max_c (f90:97-120) taking their branches from the values as the reference's complex step
 // does.
 
@@ -394,11 +394,15 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, con
   TileSmem<T>& S = *reinterpret_cast<TileSmem<T>*>(tile_smem);
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;
   const int M = in.M, N = in.N;
-  const int h = blockIdx.z;  // part of the tangent direction (dual kernel only)
+  // the dual kernel's two parts of a tile are neighbouring CTAs (x = 2 tile + part), so the
+  // second finds the tile's inputs in L2 and completes the output sectors the first began
+  constexpr bool kDual = !std::is_same<T, double>::value;
+  const int h = kDual ? (int)(blockIdx.x & 1) : 0;
+  const int tile = kDual ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
   const int tiles_m = (M + kTM - 1) / kTM;
   const int tiles = tiles_m * ((N + kTN - 1) / kTN);
-  if ((int)blockIdx.x >= tiles) return;
-  const int m0 = (blockIdx.x % tiles_m) * kTM, n0 = (blockIdx.x / tiles_m) * kTN;
+  if (tile >= tiles) return;
+  const int m0 = (tile % tiles_m) * kTM, n0 = (tile / tiles_m) * kTN;
   const double* Ui = U + 4 * in.cell_offset;
   const double* Xi = X + 2 * in.vert_offset;
   const double* Vi = V ? V + 2 * in.vert_offset : nullptr;
@@ -495,7 +499,7 @@ int launch_tangent_tiled(const eb_batch* b, const double* X, const double* V, co
                          const double* dU, const double* dX, const double* dV, const double* dMa,
                          double* dR, double* R, cudaStream_t stream, int max_tiles) {
   const Table t = make_table(b);
-  dim3 grid(max_tiles, b->n_inst, 2);
+  dim3 grid(2 * max_tiles, b->n_inst);
   if (cudaFuncSetAttribute(k_residual_tiled<D1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sizeof(TileSmem<D1>)) != cudaSuccess)
     return check_launch("apply_odes_tangent attribute");
