@@ -16,6 +16,9 @@
  *    d(odes)/d(states) (4, 4, M, N, 9), d(odes)/d(vertices|velocities) (4, 2, M, N, 4),
  *    d(odes)/d(mach) (4, 1, M, N), forces (2, N), d(forces)/d(states) (2, 4, N),
  *    d(forces)/d(vertices) (2, 2, N, 2). Complex arrays are interleaved (re, im) doubles.
+ *  - Every array pointer must be 16-byte aligned (the kernels move states, complex values and
+ *    coordinate pairs as 16-byte vectors); a misaligned array is rejected with EB_ERR_ARG
+ *    before anything is launched.
  *  - The states, vertices and velocities are real here: the reference stores them as
  *    complex128 only to run its complex-step differentiation, and its public API exposes
  *    their real parts (core.py:159-211).

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <initializer_list>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -224,10 +225,24 @@ __device__ __forceinline__ void stc(double* p, C2 c) {
   *reinterpret_cast<double2*>(p) = make_double2(c.re, c.im);
 }
 
+// Arrays are read and written as 16-byte vectors (4-component states, complex values, pairs of
+// coordinates): every array argument must be 16-byte aligned, and a misaligned one is rejected
+// with EB_ERR_ARG before any launch (null pointers pass).
+inline int aligned16(std::initializer_list<const void*> ptrs) {
+  for (const void* q : ptrs)
+    if (reinterpret_cast<uintptr_t>(q) & 15) return fail(EB_ERR_ARG, "arrays must be 16-byte aligned");
+  return EB_OK;
+}
 
 }  // namespace eb
 
 #define EB_STREAM(s) reinterpret_cast<cudaStream_t>(s)
+#define EB_ALIGNED(...)                              \
+  do {                                               \
+    int _rc = eb::aligned16({__VA_ARGS__});          \
+    if (_rc != EB_OK) return _rc;                    \
+  } while (0)
+
 #define EB_VALIDATE(b)            \
   do {                            \
     int _rc = eb::validate(b);    \

@@ -303,7 +303,10 @@ __global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, int64_t n_c
     C2 acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double* blk = Jc + slot_stride * k;
+      // the 4x2 block (64 contiguous bytes) in four 16-byte loads
+      const double2* b2 = reinterpret_cast<const double2*>(Jc + slot_stride * k);
+      const double2 q0 = __ldg(b2), q1 = __ldg(b2 + 1), q2 = __ldg(b2 + 2), q3 = __ldg(b2 + 3);
+      const double blk[8] = {q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y};
       const C2 a = ldc(xi + 4 * v[k]), b = ldc(xi + 4 * v[k] + 2);
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
@@ -376,8 +379,11 @@ __global__ void k_apply_mach_fwd(Table t, int64_t n_cells, const double* J, cons
       idx = lo;
     }
     const C2 d = ldc(dm + 2 * idx);
+    const double2 j01 = __ldg(reinterpret_cast<const double2*>(J + 4 * g));
+    const double2 j23 = __ldg(reinterpret_cast<const double2*>(J + 4 * g + 2));
+    const double jv[4] = {j01.x, j01.y, j23.x, j23.y};
 #pragma unroll
-    for (int r = 0; r < 4; ++r) stc(y + 8 * g + 2 * r, C2{J[4 * g + r] * d.re, J[4 * g + r] * d.im});
+    for (int r = 0; r < 4; ++r) stc(y + 8 * g + 2 * r, C2{jv[r] * d.re, jv[r] * d.im});
   }
 }
 
@@ -660,6 +666,7 @@ const char* eb_version(void) { return "euler_b200 1.0 (sm_100a, FP64)"; }
 
 int eb_set_free_stream_state(const eb_batch* b, double* U, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(U);
   if (!U) return fail(EB_ERR_ARG, "null states");
   const Table t = make_table(b);
   k_free_stream<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, U);
@@ -669,6 +676,7 @@ int eb_set_free_stream_state(const eb_batch* b, double* U, void* stream) {
 int eb_compute_odes(const eb_batch* b, const double* X, const double* V, const double* U,
                     double* R, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, R);
   if (!X || !U || !R) return fail(EB_ERR_ARG, "null array");
   int dim = b->max_dim;
   if (b->n_inst == 1 && b->d_table == nullptr) dim = std::max(b->single.M, b->single.N);
@@ -681,6 +689,7 @@ int eb_compute_odes(const eb_batch* b, const double* X, const double* V, const d
 int eb_compute_odes_untiled(const eb_batch* b, const double* X, const double* V, const double* U,
                             double* R, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, R);
   if (!X || !U || !R) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_residual<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U, R);
@@ -690,6 +699,7 @@ int eb_compute_odes_untiled(const eb_batch* b, const double* X, const double* V,
 int eb_compute_forces(const eb_batch* b, const double* X, const double* U, double* F,
                       double* coef, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, U, F);
   if (!X || !U || !F) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_forces<<<b->n_inst, 256, 0, EB_STREAM(stream)>>>(t, X, U, F, coef);
@@ -699,6 +709,7 @@ int eb_compute_forces(const eb_batch* b, const double* X, const double* U, doubl
 int eb_compute_pressure_coefficients(const eb_batch* b, const double* U, double* cp,
                                      void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(U);
   if (!U || !cp) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_pressure_coef<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, U, cp);
@@ -709,6 +720,7 @@ int eb_apply_pressure_coefficients_wrt_states_fwd(const eb_batch* b, const doubl
                                                   const double* d_states, double* d_cp,
                                                   void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(U, d_states);
   if (!U || !d_states || !d_cp) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_pressure_coef_fwd<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, U,
@@ -719,6 +731,7 @@ int eb_apply_pressure_coefficients_wrt_states_fwd(const eb_batch* b, const doubl
 int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double* d_mach,
                                double* d_odes, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_mach, d_odes);
   if (!J || !d_mach || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_mach_fwd<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J,
@@ -729,6 +742,7 @@ int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double*
 int eb_apply_odes_wrt_mach_rev(const eb_batch* b, const double* J, const double* d_odes,
                                double* d_mach, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_odes, d_mach);
   if (!J || !d_mach || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_mach_rev<<<b->n_inst, 512, 0, EB_STREAM(stream)>>>(t, J, d_odes, d_mach);
@@ -738,6 +752,7 @@ int eb_apply_odes_wrt_mach_rev(const eb_batch* b, const double* J, const double*
 int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const double* d_states,
                                  double* d_odes, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_states, d_odes);
   if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_states_fwd4<<<grid_for(4 * b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
@@ -748,6 +763,7 @@ int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const doubl
 int eb_apply_odes_wrt_states_rev(const eb_batch* b, const double* J, const double* d_odes,
                                  double* d_states, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_odes, d_states);
   if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_states_rev4<<<grid_for(4 * b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
@@ -758,6 +774,7 @@ int eb_apply_odes_wrt_states_rev(const eb_batch* b, const double* J, const doubl
 int eb_apply_odes_wrt_vertices_fwd(const eb_batch* b, const double* J,
                                    const double* d_vertices, double* d_odes, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_vertices, d_odes);
   if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_vertices_fwd<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
@@ -768,6 +785,7 @@ int eb_apply_odes_wrt_vertices_fwd(const eb_batch* b, const double* J,
 int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const double* d_odes,
                                    double* d_vertices, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_odes, d_vertices);
   if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_vertices_rev<<<grid_for(2 * b->n_verts, 256), 256, 0, EB_STREAM(stream)>>>(
@@ -778,6 +796,7 @@ int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const dou
 int eb_apply_forces_wrt_states_fwd(const eb_batch* b, const double* J, const double* d_states,
                                    double* d_forces, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_states, d_forces);
   if (!J || !d_states || !d_forces) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_forces_states_fwd<<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(
@@ -788,6 +807,7 @@ int eb_apply_forces_wrt_states_fwd(const eb_batch* b, const double* J, const dou
 int eb_apply_forces_wrt_states_rev(const eb_batch* b, const double* J, const double* d_forces,
                                    double* d_states, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_forces, d_states);
   if (!J || !d_states || !d_forces) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_forces_states_rev<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
@@ -798,6 +818,7 @@ int eb_apply_forces_wrt_states_rev(const eb_batch* b, const double* J, const dou
 int eb_apply_forces_wrt_vertices_fwd(const eb_batch* b, const double* J,
                                      const double* d_vertices, double* d_forces, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_vertices, d_forces);
   if (!J || !d_vertices || !d_forces) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_forces_vertices_fwd<<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(
@@ -808,6 +829,7 @@ int eb_apply_forces_wrt_vertices_fwd(const eb_batch* b, const double* J,
 int eb_apply_forces_wrt_vertices_rev(const eb_batch* b, const double* J,
                                      const double* d_forces, double* d_vertices, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, d_forces, d_vertices);
   if (!J || !d_vertices || !d_forces) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_apply_forces_vertices_rev<<<grid_for(b->n_verts, 256), 256, 0, EB_STREAM(stream)>>>(
@@ -819,6 +841,7 @@ int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, c
                           const double* dU, const double* dX, const double* dV,
                           const double* dMa, double* dR, double* R, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, dU, dX, dV, dMa, dR, R);
   if (!X || !U || !dR) return fail(EB_ERR_ARG, "null array");
   int dim = b->max_dim;
   if (b->n_inst == 1 && b->d_table == nullptr) dim = std::max(b->single.M, b->single.N);
@@ -830,6 +853,7 @@ int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, c
 int eb_convert_odes_wrt_states(const eb_batch* b, const double* J, double* data,
                                int32_t* indices, int32_t* index_pointers, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(J, data);
   if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "convert takes a single instance");
   if (!J || !data || !indices || !index_pointers) return fail(EB_ERR_ARG, "null array");
   const int M = b->single.M, N = b->single.N;

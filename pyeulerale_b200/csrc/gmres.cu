@@ -601,6 +601,9 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
                    const int32_t* sys_inst, const double* shifts, int adjoint,
                    const double* rhs, double* x, const eb_gmres_options* opt, void* workspace,
                    int64_t workspace_bytes, eb_gmres_info* info, void* stream) {
+  if ((reinterpret_cast<uintptr_t>(J) | reinterpret_cast<uintptr_t>(rhs) |
+       reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(workspace)) & 15)
+    return fail(EB_ERR_ARG, "gmres: arrays must be 16-byte aligned");
   int rc = validate(b);
   if (rc != EB_OK) return rc;
   if (!J || !rhs || !x || !opt || !workspace || !info || !shifts || n_sys < 1)
@@ -793,6 +796,9 @@ extern "C" int eb_gmres_solve_noalloc(const eb_batch* b, const eb_instance* host
                                       double* x, const eb_gmres_options* opt,
                                       eb_gmres_info* info, void* stream) {
   if (!b || !opt || n_sys < 1) return fail(EB_ERR_ARG, "gmres_noalloc: null argument");
+  if ((reinterpret_cast<uintptr_t>(J) | reinterpret_cast<uintptr_t>(rhs) |
+       reinterpret_cast<uintptr_t>(x)) & 15)
+    return fail(EB_ERR_ARG, "gmres_noalloc: arrays must be 16-byte aligned");
   const int64_t need = eb_gmres_workspace_bytes(b, host_table, n_sys, sys_inst, opt->restart);
   if (need < 0) return fail(EB_ERR_ARG, "gmres_noalloc: invalid systems");
   if (need > (int64_t)kStaticScratchBytes) {

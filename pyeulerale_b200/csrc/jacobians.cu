@@ -10,6 +10,7 @@ extern "C" {
 int eb_compute_odes_wrt_mach(const eb_batch* b, const double* X, const double* V,
                              const double* U, double* J, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_jac_mach<double, kDirNone><<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
@@ -20,6 +21,7 @@ int eb_compute_odes_wrt_mach(const eb_batch* b, const double* X, const double* V
 int eb_compute_odes_wrt_states(const eb_batch* b, const double* X, const double* V,
                                const double* U, double* J, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_jac_states<double, kDirNone><<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
@@ -30,6 +32,7 @@ int eb_compute_odes_wrt_states(const eb_batch* b, const double* X, const double*
 int eb_compute_odes_wrt_vertices(const eb_batch* b, const double* X, const double* V,
                                  const double* U, double* J, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_jac_vertexlike<double, kDirNone, false>
@@ -41,6 +44,7 @@ int eb_compute_odes_wrt_vertices(const eb_batch* b, const double* X, const doubl
 int eb_compute_odes_wrt_velocities(const eb_batch* b, const double* X, const double* V,
                                    const double* U, double* J, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_jac_vertexlike<double, kDirNone, true>
@@ -52,6 +56,7 @@ int eb_compute_odes_wrt_velocities(const eb_batch* b, const double* X, const dou
 int eb_compute_forces_wrt_states(const eb_batch* b, const double* X, const double* U,
                                  double* J, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_jac_forces_states<double, kDirNone><<<grid_for(b->n_wall, 128), 128, 0, EB_STREAM(stream)>>>(
@@ -62,6 +67,7 @@ int eb_compute_forces_wrt_states(const eb_batch* b, const double* X, const doubl
 int eb_compute_forces_wrt_vertices(const eb_batch* b, const double* X, const double* U,
                                    double* J, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   k_jac_forces_vertices<double, kDirNone>

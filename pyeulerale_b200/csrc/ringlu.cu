@@ -1016,8 +1016,11 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
   int rc = check_group(b, n_shifts, workspace, workspace_stride, L);
   if (rc != EB_OK) return rc;
   if (!J || !shifts || !rhs || !x) return fail(EB_ERR_ARG, "ringlu: null argument");
-  for (int s = 0; s < n_shifts; ++s)
+  for (int s = 0; s < n_shifts; ++s) {
     if (!J[s] || !rhs[s] || !x[s]) return fail(EB_ERR_ARG, "ringlu: null argument");
+    if ((reinterpret_cast<uintptr_t>(rhs[s]) | reinterpret_cast<uintptr_t>(x[s])) & 15)
+      return fail(EB_ERR_ARG, "ringlu: rhs and x must be 16-byte aligned");
+  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cublasHandle_t h = nullptr;
   if ((rc = blas_handle(st, h)) != EB_OK) return rc;

@@ -29,6 +29,7 @@ int eb_odes_wrt_mach_dir(const eb_batch* b, const double* X, const double* V, co
                          int dir_kind, const double* d, double* J_re, double* J_im,
                          void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   EB_DIR_DISPATCH(k_jac_mach, b->n_cells, t, b->n_cells, X, V, U, d, nullptr, J_re, J_im);
@@ -39,6 +40,7 @@ int eb_odes_wrt_states_dir(const eb_batch* b, const double* X, const double* V,
                            const double* U, int dir_kind, const double* d, double* J_re,
                            double* J_im, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   EB_DIR_DISPATCH(k_jac_states, b->n_cells, t, b->n_cells, X, V, U, d, nullptr, J_re, J_im);
@@ -49,6 +51,7 @@ int eb_odes_wrt_vertices_dir(const eb_batch* b, const double* X, const double* V
                              const double* U, int dir_kind, const double* d, double* J_re,
                              double* J_im, void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, V, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
   const int g = grid_for(b->n_cells, 128);
@@ -76,6 +79,7 @@ int eb_forces_wrt_states_dir(const eb_batch* b, const double* X, const double* U
                              int dir_kind, const double* d, double* J_re, double* J_im,
                              void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   if (dir_kind != kDirStates && dir_kind != kDirVertices)
     return fail(EB_ERR_ARG, "forces depend on states and vertices only");
@@ -93,6 +97,7 @@ int eb_forces_wrt_vertices_dir(const eb_batch* b, const double* X, const double*
                                int dir_kind, const double* d, double* J_re, double* J_im,
                                void* stream) {
   EB_VALIDATE(b);
+  EB_ALIGNED(X, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   if (dir_kind != kDirStates && dir_kind != kDirVertices)
     return fail(EB_ERR_ARG, "forces depend on states and vertices only");

@@ -36,6 +36,25 @@ def test_library_exports_every_declared_symbol():
     assert declared <= bound, declared - bound
 
 
+@pytest.mark.parametrize("entry,n_arrays", [("eb_compute_odes", 4),
+                                            ("eb_apply_odes_wrt_states_rev", 3),
+                                            ("eb_apply_odes_wrt_vertices_fwd", 3),
+                                            ("eb_compute_odes_wrt_states", 4)])
+def test_misaligned_arrays_rejected_before_any_launch(entry, n_arrays):
+    """Arrays are accessed as 16-byte vectors: an array 8 bytes off a 16-byte boundary is an
+    argument error returned by the host-side checks (the fake addresses are never touched)."""
+    from pyeulerale_b200.build import build_library
+
+    build_library()
+    batch = _lib.single_batch(_lib.make_instance(8, 9, 0.5, 1.25))
+    good, bad = 0x7F0000000000, 0x7F0000000008
+    args = [good] * n_arrays
+    args[-1] = bad
+    with pytest.raises(_lib.EulerB200Error, match="16-byte aligned") as err:
+        _lib.call(entry, ctypes.byref(batch), *args, None)
+    assert err.value.code == -1
+
+
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Instance) == 104
     assert _lib.Instance.wall_offset.offset == 24
