@@ -12,10 +12,10 @@ One timed "step" is one residual evaluation R(Ma, U, X, V) of the whole batch (o
 The JSON line reports cell-residual evaluations per second (``value``), and beside it the VJP
 rate (full set of reverse products per instance: d/dU, d/dX, d/dV, d/dMa), the linearisation
 rates (the d(odes)/d(states) Jacobian, the matrix-free tangent, the forward products, the
-shifted BSR SpMV) and the resolvent rate: the pitch frequency response (64 shifts) plus the
-adjoint lift gradient of the PTC steady state of one instance, solved to 1e-10 relative
-residual, with the shifts factored together (batched) and one at a time through the drop-in
-class (plain).
+shifted BSR SpMV), the 13 second-order inner-product gradients and the resolvent rate: the
+pitch frequency response (64 shifts) plus the adjoint lift gradient of the PTC steady state of
+one instance, solved to 1e-10 relative residual, with the shifts factored together (batched)
+and one at a time through the drop-in class (plain).
 
 ``--impl reference`` times the CPU restatement of the reference (complex arithmetic, all host
 threads) on a bounded sample of the same workload. Under torchrun every rank processes its own
@@ -68,9 +68,9 @@ def parse_args():
                    help="frequency-response shifts timed one at a time (plain path)")
     p.add_argument("--batched-shifts", type=int, default=64,
                    help="frequency-response shifts timed through the batched driver")
-    p.add_argument("--parts", default="residual,vjp,linear,resolvent,uneven",
+    p.add_argument("--parts", default="residual,vjp,linear,second_order,resolvent,uneven",
                    help="comma-separated parts to run besides the residual "
-                        "(vjp, linear, resolvent, uneven)")
+                        "(vjp, linear, second_order, resolvent, uneven)")
     p.add_argument("--uneven-instances", type=int, default=48)
     p.add_argument("--uneven-sizes", default="65,129",
                    help="grid point counts (n x n O-grids) the uneven instances draw from")
@@ -348,6 +348,39 @@ def cpu_linear_rates(X, V, U, mach: float) -> dict:
             "sample": f"one {M}x{N}-cell instance, each procedure repeated for >= 0.5 s"}
 
 
+def cpu_second_order_rate(X, V, U, mach: float) -> dict:
+    """The reference's second-order method on the host for one routine,
+    compute_odes_wrt_states_inner_product_wrt_states (core.py:761-802): central differences of
+    complex-step Jacobians, four d(odes)/d(states) builds (real and imaginary part of the
+    direction, plus and minus the step) and four reverse products, with the oracle restatement
+    of the Fortran procedures."""
+    from oracle.shim import SpatialDiscretizationModule
+
+    M, N = U.shape[1], U.shape[2]
+    disc = SpatialDiscretizationModule()
+    disc.aoa[...] = FLOW["aoa_deg"]
+    Xc, Vc, Uc = (np.asfortranarray(np.asarray(a, dtype=complex)) for a in (X, V, U))
+    rng = np.random.default_rng(13)
+    d_states = np.asfortranarray(rng.standard_normal((4, M, N)) + 1j * rng.standard_normal((4, M, N)))
+    d_odes = np.asfortranarray(rng.standard_normal((4, M, N)) + 1j * rng.standard_normal((4, M, N)))
+    t0 = time.perf_counter()
+    grad = np.zeros((4, M, N), dtype=complex, order="F")
+    vjp = np.zeros((4, M, N), dtype=complex, order="F")
+    Jp = np.zeros((4, 4, M, N, 9), order="F")
+    step = 1e-6 * (1.0 + np.linalg.norm(Uc)) ** 0.5 / np.linalg.norm(d_states)
+    for sign in (1.0, -1.0):
+        for part, factor in ((np.real, 1.0), (np.imag, 1j)):
+            disc.compute_odes_wrt_states(mach, Xc, Vc, Uc + sign * step * part(d_states), Jp)
+            disc.apply_odes_wrt_states_rev(Jp, d_odes.conj(), vjp)
+            grad += sign * factor * vjp
+    grad = grad / 2.0 / step
+    t = time.perf_counter() - t0
+    return {"value": 1.0 / t, "unit": "routine calls/s (one 128x128 instance)", "cores": 1,
+            "kind": "port", "cpu": cpu_model(),
+            "sample": f"compute_odes_wrt_states_inner_product_wrt_states once in {t:.2f} s "
+                      "(four complex-step Jacobian builds and reverse products, core.py:761-802)"}
+
+
 # ---- B200 arm -------------------------------------------------------------------------------
 
 def read_traffic() -> float | None:
@@ -623,6 +656,62 @@ def run_b200(args) -> None:
                     linear[key]["value"] / cpu_lin[key]["value"]
         del J_u, tU, tX, tV, tR, mats, sx, sy, spmv_graph, side
 
+    # second order: the 13 inner-product gradients of the drop-in class (core.py:718-1275) on
+    # one 128x128 instance, host arrays in and out as the reference's API has them (each call
+    # builds one directional Jacobian on the device in nested duals and applies its reverse
+    # product); beside it the reference's finite-difference method for one of them on the host
+    second = None
+    if "second_order" in parts:
+        from pyeulerale_b200 import SpatialDiscretization
+
+        sd2 = SpatialDiscretization(X, mach_number=FLOW["mach"], angle_of_attack=FLOW["aoa_deg"],
+                                    coefficient_length=GRID["chord"],
+                                    coefficient_center=FLOW["center"])
+        sd2.states[...] = Us[0]
+        M2, N2 = sd2.num_radial, sd2.num_angular
+        srng = np.random.default_rng(31 + rank)
+
+        def crand(shape):
+            return np.asfortranarray(srng.standard_normal(shape)
+                                     + 1j * srng.standard_normal(shape))
+
+        w, dS = crand((4, M2, N2)), crand((4, M2, N2))
+        dXs, dVs, dF = crand((2, M2 + 1, N2 + 1)), crand((2, M2 + 1, N2 + 1)), crand((2, N2))
+        routines = [
+            lambda: sd2.compute_odes_wrt_states_inner_product_wrt_mach(w, dS),
+            lambda: sd2.compute_odes_wrt_states_inner_product_wrt_states(w, dS),
+            lambda: sd2.compute_odes_wrt_states_inner_product_wrt_vertices(w, dS),
+            lambda: sd2.compute_odes_wrt_vertices_inner_product_wrt_mach(w, dXs),
+            lambda: sd2.compute_odes_wrt_vertices_inner_product_wrt_states(w, dXs),
+            lambda: sd2.compute_odes_wrt_vertices_inner_product_wrt_vertices(w, dXs),
+            lambda: sd2.compute_odes_wrt_velocities_inner_product_wrt_mach(w, dVs),
+            lambda: sd2.compute_odes_wrt_velocities_inner_product_wrt_states(w, dVs),
+            lambda: sd2.compute_odes_wrt_velocities_inner_product_wrt_vertices(w, dVs),
+            lambda: sd2.compute_forces_wrt_states_inner_product_wrt_states(dF, dS),
+            lambda: sd2.compute_forces_wrt_states_inner_product_wrt_vertices(dF, dS),
+            lambda: sd2.compute_forces_wrt_vertices_inner_product_wrt_states(dF, dXs),
+            lambda: sd2.compute_forces_wrt_vertices_inner_product_wrt_vertices(dF, dXs),
+        ]
+        for fn in routines:
+            fn()
+        barrier()
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            for fn in routines:
+                fn()
+        barrier()
+        t_so = max_over_ranks(time.perf_counter() - t0)
+        second = {"value": world * reps * len(routines) / t_so,
+                  "unit": "second-order routine calls/s (drop-in class, host arrays, one "
+                          "128x128 instance per call)",
+                  "routines": len(routines), "calls": reps * len(routines), "seconds": t_so}
+        if rank == 0 and not args.no_cpu_baseline:
+            second["cpu_reference_method"] = cpu_second_order_rate(X, V, Us[0], FLOW["mach"])
+            second["vs_cpu_reference_method"] = \
+                (second["value"] / world) / second["cpu_reference_method"]["value"]
+        del sd2
+
     # resolvent: the frequency response of the steady state (PTC from free stream), 64 shifts
     # s = i k V / (c / 2), k log-spaced on [0.01, 10], plus the adjoint lift gradient; batched
     # (shift_group shifts per factorisation call) against one shift at a time through the
@@ -788,6 +877,7 @@ def run_b200(args) -> None:
             "vs_cpu_reference_method": None if cpu_lin is None
             else vjp_rate / cpu_lin["vjp"]["value"]},
         "linear": linear,
+        "second_order": second,
         "resolvent": res,
         "uneven": uneven,
     }
