@@ -220,6 +220,15 @@ __device__ __forceinline__ T* at(char* ws0, int64_t stride, size_t off) {
 // also yields their candidates for the next step. The staging buffers alternate between steps,
 // so one barrier per step suffices. Records the pivot row of each step in perm and flags a zero
 // or non-finite pivot in info[0].
+// Maximum of a 64-bit key over the warp as two 32-bit warp reductions: the high words, then
+// the low words of the lanes that hold the maximal high word (the exact 64-bit maximum).
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long key) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned H = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned L = __reduce_max_sync(0xffffffffu, hi == H ? lo : 0u);
+  return ((unsigned long long)H << 32) | L;
+}
+
 constexpr int kPanelThreads = 512;
 constexpr int kMaxK = 1024;
 template <int NB, int ROWS>
@@ -228,6 +237,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
                size_t off_perm, size_t off_info) {
   constexpr int kWarps = kPanelThreads / 32;
   __shared__ cuDoubleComplex cand[2][kWarps][NB];
+  __shared__ cuDoubleComplex cand_inv[2][kWarps];  // 1 / (the candidate's pivot value)
   __shared__ unsigned long long cand_key[2][kWarps];
   __shared__ unsigned char chosen[kMaxK];
   const cuDoubleComplex* in = at<cuDoubleComplex>(ws0, stride, off_in);
@@ -275,11 +285,18 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
                       (unsigned long long)(kMaxK - 1 - bi))
                    : 0ull;
     const unsigned long long mine = key;
+    // the reciprocal of this thread's candidate pivot, formed while the arg-max runs (the
+    // winner stages it with its row, which takes the division off the step's critical path)
+    cuDoubleComplex cinv = make_cuDoubleComplex(0.0, 0.0);
+    if (bi < kMaxK) {
+      cuDoubleComplex c0 = a[0][0];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long ok = __shfl_xor_sync(0xffffffffu, key, o);
-      key = ok > key ? ok : key;
+      for (int r = 1; r < ROWS; ++r)
+        if (bi == tid + r * kPanelThreads) c0 = a[r][0];
+      const double d = 1.0 / (c0.x * c0.x + c0.y * c0.y);
+      cinv = make_cuDoubleComplex(c0.x * d, -c0.y * d);
     }
+    key = warp_max_u64(key);
     if (key != 0ull && mine == key) {  // this thread owns the warp's best row: stage it
       const int wi = kMaxK - 1 - (int)(key & 0x3FFull);
 #pragma unroll
@@ -288,15 +305,11 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
 #pragma unroll
           for (int k = 0; k < NB; ++k) cand[par][warp][k] = a[r][k];
         }
+      cand_inv[par][warp] = cinv;
     }
     if (lane == 0) cand_key[par][warp] = key;
     __syncthreads();
-    unsigned long long kb = lane < kWarps ? cand_key[par][lane] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long ok = __shfl_xor_sync(0xffffffffu, kb, o);
-      kb = ok > kb ? ok : kb;
-    }
+    const unsigned long long kb = warp_max_u64(lane < kWarps ? cand_key[par][lane] : 0ull);
     const int p = kMaxK - 1 - (int)(kb & 0x3FFull);
     const int w = (p % kPanelThreads) / 32;  // the warp of the thread that owns row p
     const double v = __longlong_as_double((long long)(kb & ~0x3FFull));
@@ -312,9 +325,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1)
     // next one a[.][1]; after the elimination the row rotates by one more column, so after NB
     // steps it is back in order. The staged pivot row is rotated the same way.
     const cuDoubleComplex* prow = cand[par][w];
-    const cuDoubleComplex ap = prow[0];
-    const double d = 1.0 / (ap.x * ap.x + ap.y * ap.y);
-    const cuDoubleComplex inv = make_cuDoubleComplex(ap.x * d, -ap.y * d);
+    const cuDoubleComplex inv = cand_inv[par][w];
     best = -1.0;
     bi = kMaxK;
 #pragma unroll
