@@ -279,8 +279,9 @@ def cpu_linear_rates(X, V, U, mach: float) -> dict:
     """The reference's own linearisation procedures on the host, in its single thread (the
     oracle restatement of src/spatial_discretization.f90): the complex-step d(odes)/d(states)
     Jacobian (f90:666-750), the four forward and the four reverse products with the stored
-    Jacobians (f90:604-650, 825-918, 1005-1072) of one 128x128 instance, and the matrix-vector
-    product of the CSR matrix that _assemble_csr builds (core.py:512-531) under scipy."""
+    Jacobians (f90:604-650, 825-918, 1005-1072) of one 128x128 instance, its BSR conversion
+    (f90:765-814), and the matrix-vector product of the CSR matrix that _assemble_csr builds
+    (core.py:512-531) under scipy."""
     from scipy.sparse import bsr_array
 
     from oracle.shim import SpatialDiscretizationModule
@@ -336,13 +337,16 @@ def cpu_linear_rates(X, V, U, mach: float) -> dict:
     data = np.empty((4, 4, nnzb), order="F")
     idx = np.empty(nnzb, dtype=np.intc)
     ptr = np.empty(M * N + 1, dtype=np.intc)
-    disc.convert_odes_wrt_states(J_u, data, idx, ptr)
+    t_conv = per_call(lambda: disc.convert_odes_wrt_states(J_u, data, idx, ptr))
     A = bsr_array((np.moveaxis(data, -1, 0), idx - 1, ptr - 1), dtype=complex).tocsr()
     x = crand(4 * M * N)
     t_spmv = per_call(lambda: A @ x)
     return {"jacobian_states": {"value": M * N / t_jac, "unit": "cells/s"},
             "vjp": {"value": 1.0 / t_vjp, "unit": "VJP/s (four reverse products, one instance)"},
             "jvp": {"value": 1.0 / t_jvp, "unit": "JVP/s (four forward products, one instance)"},
+            "bsr_conversion": {"value": 1.0 / t_conv,
+                               "unit": "conversions/s (the oracle's O(nnz) restatement; the "
+                                       "reference's Fortran loop is O((MN)^2), f90:765-814)"},
             "bsr_spmv": {"value": 1.0 / t_spmv, "unit": "SpMV/s (scipy CSR, complex x)"},
             "cores": 1, "kind": "port", "cpu": cpu_model(),
             "sample": f"one {M}x{N}-cell instance, each procedure repeated for >= 0.5 s"}
@@ -597,6 +601,9 @@ def run_b200(args) -> None:
             one.call("eb_convert_odes_wrt_states", J_u[144 * inst.cell_offsets[i]:], data, idx,
                      ptr, stream=sp)
             mats.append((data, idx, ptr))
+        data0, idx0, ptr0 = mats[0]
+        t_conv = per_call(lambda: one.call("eb_convert_odes_wrt_states", J_u, data0, idx0, ptr0,
+                                           stream=sp), max(5, args.steps // 4))
         sx = torch.randn(8 * rows * n_mat, generator=gen, **f64)
         sy = torch.empty(8 * rows * n_mat, **f64)
 
@@ -641,6 +648,11 @@ def run_b200(args) -> None:
                     "unit": "JVP/s (dR/dU, dR/dX, dR/dV, dR/dMa forward products per instance)",
                     "achieved_gbs": BYTES_PER_CELL_JVP * cells / t_jvp / 1e9,
                     "bytes_per_cell": BYTES_PER_CELL_JVP, "launches_per_jvp_batch": 4},
+            "bsr_conversion": {"value": world / t_conv,
+                               "unit": "conversions/s (one 128x128 instance: 146,688 blocks, "
+                                       "1-based indices as the reference emits them)",
+                               "achieved_gbs": (1152 * rows + nnzb * (128 + 4)
+                                                + (rows + 1) * 4) / t_conv / 1e9},
             "bsr_spmv": {"value": world / t_spmv, "unit": "SpMV/s (one 128x128 instance)",
                          "achieved_gbs": spmv_bytes / t_spmv / 1e9,
                          "bytes_per_spmv": spmv_bytes, "nnzb": nnzb,
@@ -651,7 +663,7 @@ def run_b200(args) -> None:
         if rank == 0 and not args.no_cpu_baseline:
             cpu_lin = cpu_linear_rates(X, V, Us[0], FLOW["mach"])
             linear["cpu_reference_method"] = cpu_lin
-            for key in ("jacobian_states", "jvp", "bsr_spmv"):
+            for key in ("jacobian_states", "jvp", "bsr_conversion", "bsr_spmv"):
                 linear[key]["vs_cpu_reference_method"] = \
                     linear[key]["value"] / cpu_lin[key]["value"]
         del J_u, tU, tX, tV, tR, mats, sx, sy, spmv_graph, side

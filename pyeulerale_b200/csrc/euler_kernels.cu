@@ -538,12 +538,16 @@ __global__ void k_apply_forces_vertices_rev(Table t, int64_t n_verts, const doub
 // convert_odes_wrt_states, f90:765-814, one thread per block row. For N >= 5 and M >= 4 the
 // nine stencil columns of a row are distinct, so the row holds 5 + [m>=1] + [m>=2] +
 // [m<=M-2] + [m<=M-3] blocks, emitted in ascending column order with 1-based indices.
-__global__ void k_convert_bsr(int M, int N, const double* J, double* data, int32_t* indices,
-                              int32_t* indptr) {
+// Eight threads per block row: each finds the row's sorted columns (the same few register
+// operations in all eight) and copies its 16-byte pair of every block, so a block moves as one
+// coalesced 128-byte access; thread 0 of the row writes the indices and the row pointer.
+__global__ void __launch_bounds__(256) k_convert_bsr(int M, int N, const double* J, double* data,
+                                                     int32_t* indices, int32_t* indptr) {
   const int64_t rows = (int64_t)M * N;
   const int64_t line = 9 * (int64_t)M - 6;  // blocks per angular line
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
-       r += (int64_t)gridDim.x * blockDim.x) {
+  const int l = threadIdx.x & 7;
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3; r < rows;
+       r += ((int64_t)gridDim.x * blockDim.x) >> 3) {
     const int m = (int)(r % M), n = (int)(r / M);
     // blocks in the rows m' < m of this line
     int64_t before = 5 * (int64_t)m + (m > 1 ? m - 1 : 0) + (m > 2 ? m - 2 : 0) +
@@ -571,15 +575,15 @@ __global__ void k_convert_bsr(int M, int N, const double* J, double* data, int32
       col[b + 1] = c;
       slot[b + 1] = sl;
     }
-    indptr[r] = (int32_t)(ptr + 1);
-    if (r == rows - 1) indptr[rows] = (int32_t)(ptr + cnt + 1);
+    if (l == 0) {
+      indptr[r] = (int32_t)(ptr + 1);
+      if (r == rows - 1) indptr[rows] = (int32_t)(ptr + cnt + 1);
+    }
     const int64_t slot_stride = 16 * rows;
     for (int a = 0; a < cnt; ++a) {
-      const double* blk = J + slot_stride * slot[a] + 16 * r;
-      double* dst = data + 16 * (ptr + a);
-#pragma unroll
-      for (int e = 0; e < 16; ++e) dst[e] = blk[e];
-      indices[ptr + a] = (int32_t)(col[a] + 1);
+      const double2* blk = reinterpret_cast<const double2*>(J + slot_stride * slot[a] + 16 * r);
+      reinterpret_cast<double2*>(data + 16 * (ptr + a))[l] = __ldg(blk + l);
+      if (l == 0) indices[ptr + a] = (int32_t)(col[a] + 1);
     }
   }
 }
@@ -857,7 +861,7 @@ int eb_convert_odes_wrt_states(const eb_batch* b, const double* J, double* data,
   if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "convert takes a single instance");
   if (!J || !data || !indices || !index_pointers) return fail(EB_ERR_ARG, "null array");
   const int M = b->single.M, N = b->single.N;
-  k_convert_bsr<<<grid_for((int64_t)M * N, 128), 128, 0, EB_STREAM(stream)>>>(
+  k_convert_bsr<<<grid_for(8 * (int64_t)M * N, 256), 256, 0, EB_STREAM(stream)>>>(
       M, N, J, data, indices, index_pointers);
   return check_launch("convert_odes_wrt_states");
 }

@@ -45,7 +45,7 @@ def test_cpu_reference_methods_run_on_a_small_grid():
 
     X, V, U = small_case()
     lin = bench.cpu_linear_rates(X, V, U, 0.5)
-    for key in ("jacobian_states", "vjp", "jvp", "bsr_spmv"):
+    for key in ("jacobian_states", "vjp", "jvp", "bsr_conversion", "bsr_spmv"):
         assert lin[key]["value"] > 0, key
     assert lin["cores"] == 1 and lin["kind"] == "port"
     so = bench.cpu_second_order_rate(X, V, U, 0.5)
