@@ -66,7 +66,9 @@ struct Handle {
   cudaEvent_t start = nullptr;
 };
 
-constexpr int kLanes = 2;
+// Lane 0: the caller's stream; 1: the second half of a multi-shift call; 2 and 3: the side
+// streams on which the Gauss-Jordan block updates of lanes 0 and 1 run ahead of the next block.
+constexpr int kLanes = 4;
 thread_local Handle g_handle[kLanes];
 
 int blas_handle(cudaStream_t st, cublasHandle_t& out, int lane = 0) {
@@ -105,9 +107,10 @@ inline int panel_width(int K) {
 
 // Width of the Gauss-Jordan column blocks whose trailing update is one ZGEMM (when it divides
 // K and a stream's group has at least kGjBlockMinShifts shifts; otherwise every panel updates
-// the whole block itself). On the 129x129 grid (K = 512) the blocked form takes 0.180 instead
-// of 0.200 ms per ring and shift with 16 shifts per group, breaks even at 4 and is 13 % slower
-// with one shift, whose thin ZGEMMs do not fill the GPU.
+// the whole block itself). On the 129x129 grid (K = 512) the blocked form takes 0.175 instead
+// of 0.200 ms per ring and shift with 16 shifts per group (0.180 without the look-ahead of
+// invert_ring), breaks even at 4 and stays 8 % slower with one shift even with the look-ahead:
+// the single shift's thin ZGEMMs and extra launches cost more than its streaming passes.
 constexpr int kGjBlock = 64;
 constexpr int kGjBlockMinShifts = 8;
 
@@ -712,7 +715,7 @@ void gj_pass_any(const Group& g, int nb, int rows, int j0, int c_lo, int c_hi, s
 // the panels of a block update only the block's columns (an even number of passes, so the
 // block ends in D_m), and the rest of D_m takes the block's combined rank-kGjBlock update as
 // strided-batched ZGEMMs (tensor-core DMMA) instead of kGjBlock / nb streaming passes.
-int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
+int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int side_lane) {
   const Layout& L = g.L;
   const int K = L.K, nb = panel_width(K), rows = (K + kPanelThreads - 1) / kPanelThreads;
   const size_t buf[2] = {g.boff(L.off_D, m), L.off_T};
@@ -722,28 +725,47 @@ int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
     for (int p = 0; p < passes; ++p)
       gj_pass_any(g, nb, rows, p * nb, 0, K, buf[p & 1], buf[(p + 1) & 1], st);
   } else {
+    // Look-ahead: the block's update of the next block's columns runs on st, right before the
+    // next block's panels; its update of every other column runs on the side stream, under
+    // those panels. st waits for the side stream before it moves the next pivot rows (which
+    // reads and zeroes rows of those columns and overwrites R) and at the end.
+    cublasHandle_t hs = nullptr;
+    int rc = blas_handle(st, hs, side_lane);
+    if (rc != EB_OK) return rc;
+    Handle& side = g_handle[side_lane];
     const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
     const int64_t es = g.es();
     cuDoubleComplex* W = g.blk(L.off_D, m);
     cuDoubleComplex* Rp = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_Rp);
+    auto update = [&](cublasHandle_t hh, int c_lo, int c_hi, int b0) {
+      if (c_hi <= c_lo) return EB_OK;
+      return blas_ok(cublasZgemmStridedBatched(hh, CUBLAS_OP_N, CUBLAS_OP_N, K, c_hi - c_lo,
+                                               kGjBlock, &one, W + (size_t)K * b0, K, es,
+                                               Rp + (size_t)kGjBlock * c_lo, kGjBlock, es, &one,
+                                               W + (size_t)K * c_lo, K, es, g.S),
+                     "ringlu: gemm Gauss-Jordan block update");
+    };
+    bool side_busy = false;
     for (int b0 = 0; b0 < K; b0 += kGjBlock) {
       for (int q = 0; q < kGjBlock / nb; ++q)
         gj_pass_any(g, nb, rows, b0 + q * nb, b0, b0 + kGjBlock, buf[q & 1], buf[(q + 1) & 1], st);
       if (K == kGjBlock) break;
+      if (side_busy && cudaStreamWaitEvent(st, side.done, 0) != cudaSuccess)
+        return check_launch("ringlu side join");
       k_gj_take_pivot_rows<<<dim3(K, g.S), 64, 0, st>>>(K, b0, kGjBlock, g.base, g.stride, buf[0],
                                                         L.off_Rp, L.off_perm, L.off_info);
-      const int ranges[2][2] = {{0, b0}, {b0 + kGjBlock, K}};
-      for (const auto& rg : ranges) {
-        const int n_cols = rg[1] - rg[0];
-        if (n_cols <= 0) continue;
-        int rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, n_cols, kGjBlock,
-                                                   &one, W + (size_t)K * b0, K, es,
-                                                   Rp + (size_t)kGjBlock * rg[0], kGjBlock, es,
-                                                   &one, W + (size_t)K * rg[0], K, es, g.S),
-                         "ringlu: gemm Gauss-Jordan block update");
-        if (rc != EB_OK) return rc;
-      }
+      const int n0 = b0 + kGjBlock, n1 = std::min(K, b0 + 2 * kGjBlock);  // the next block
+      if ((rc = update(h, n0, n1, b0)) != EB_OK) return rc;
+      if (cudaEventRecord(side.start, st) != cudaSuccess ||
+          cudaStreamWaitEvent(side.stream, side.start, 0) != cudaSuccess)
+        return check_launch("ringlu side fork");
+      if ((rc = update(hs, 0, b0, b0)) != EB_OK) return rc;
+      if ((rc = update(hs, n1, K, b0)) != EB_OK) return rc;
+      if (cudaEventRecord(side.done, side.stream) != cudaSuccess) return check_launch("ringlu side");
+      side_busy = true;
     }
+    if (side_busy && cudaStreamWaitEvent(st, side.done, 0) != cudaSuccess)
+      return check_launch("ringlu side join");
   }
   const size_t W = blocked ? buf[0] : buf[passes & 1];
   const size_t other = blocked ? buf[1] : buf[(passes + 1) & 1];
@@ -757,14 +779,14 @@ int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
 }
 
 // One ring of the block elimination for every shift of the group.
-int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st) {
+int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int side_lane) {
   const Layout& L = g.L;
   const int M = L.M, K = L.K, N = L.N;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
   const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
   const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
   const int64_t es = g.es();
-  int rc = invert_ring(g, h, m, st);
+  int rc = invert_ring(g, h, m, st, side_lane);
   if (rc != EB_OK) return rc;
   if (m + 1 < M) {
     // T = L1[m+1] = B1'[m+1] Dinv_m;  D[m+1] -= T C1'[m]
@@ -886,7 +908,7 @@ int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
   if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
   if (n_shifts == 1) {
     for (int m = 0; m < M; ++m)
-      if ((rc = factor_ring(g, h, m, st)) != EB_OK) return rc;
+      if ((rc = factor_ring(g, h, m, st, 2)) != EB_OK) return rc;
     return EB_OK;
   }
   // Two halves of the shifts on two streams, ring by ring: one half's latency-bound
@@ -900,8 +922,8 @@ int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
   cudaEventRecord(lane.start, st);
   cudaStreamWaitEvent(lane.stream, lane.start, 0);
   for (int m = 0; m < M; ++m) {
-    if ((rc = factor_ring(g1, h, m, st)) != EB_OK) return rc;
-    if ((rc = factor_ring(g2, h2, m, lane.stream)) != EB_OK) return rc;
+    if ((rc = factor_ring(g1, h, m, st, 2)) != EB_OK) return rc;
+    if ((rc = factor_ring(g2, h2, m, lane.stream, 3)) != EB_OK) return rc;
   }
   cudaEventRecord(lane.done, lane.stream);
   cudaStreamWaitEvent(st, lane.done, 0);
