@@ -11,7 +11,8 @@ from helpers import Gpu, crandn, make_case, oracle_eval, rel_err
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129", "min4x5"]
+CASES = ["ref8x9", "naca0012_33", "naca0012_33_moving", "naca0004_129", "naca0004_33_sym",
+         "min4x5"]
 
 # Tolerances: residual / forces differ from the reference arithmetic by summation order and
 # the real-vs-complex evaluation only; Jacobians are exact dual-number derivatives compared
