@@ -61,6 +61,24 @@ int validate(const eb_batch* b) {
   return EB_OK;
 }
 
+// Grid of a per-instance kernel: y = instance (no search of the instance table per thread), x
+// covers the largest instance's items (`per_item` threads for each of its cells, or vertices),
+// capped so that the whole grid stays within a few waves of 148 SMs. A batch of several
+// instances needs max_dim (the largest M or N) and at most 65535 instances.
+int per_instance_grid(const eb_batch* b, bool vertices, int per_item, int threads, dim3& grid) {
+  int64_t M = b->single.M, N = b->single.N;
+  if (b->n_inst > 1 || b->d_table) {
+    if (b->max_dim < 5) return fail(EB_ERR_ARG, "batch max_dim must be the largest M or N");
+    if (b->n_inst > 65535) return fail(EB_ERR_ARG, "at most 65535 instances per batch");
+    M = N = b->max_dim;
+  }
+  const int64_t items = vertices ? (M + 1) * (N + 1) : M * N;
+  int64_t x = (per_item * items + threads - 1) / threads;
+  const int64_t cap = std::max<int64_t>(1, (int64_t)148 * 64 * 8 / b->n_inst);
+  grid = dim3((unsigned)std::max<int64_t>(1, std::min(x, cap)), (unsigned)b->n_inst);
+  return EB_OK;
+}
+
 // ---- kernels -----------------------------------------------------------------------------
 
 __global__ void k_free_stream(Table t, int64_t n_cells, double* U) {
@@ -196,16 +214,17 @@ __global__ void __launch_bounds__(256) k_apply_states_fwd4(Table t, int64_t n_ce
                                                            const double* J, const double* x,
                                                            double* y) {
   const int i = threadIdx.x & 3;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int M = in.M, N = in.N;
+  const int64_t cells = (int64_t)M * N;
   const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t wq = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wq * 8 < n_cells;
+  for (int64_t wq = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wq * 8 < cells;
        wq += n_warps) {
-    const int64_t g = 8 * wq + ((threadIdx.x & 31) >> 2);
-    const bool live = g < n_cells;
+    const int64_t local = 8 * wq + ((threadIdx.x & 31) >> 2);
+    const bool live = local < cells;
+    const int64_t g = in.cell_offset + local;
     double ar[4] = {0.0, 0.0, 0.0, 0.0}, ai[4] = {0.0, 0.0, 0.0, 0.0};
     if (live) {
-      const Instance in = t.cell(g);
-      const int M = in.M, N = in.N;
-      const int64_t local = g - in.cell_offset;
       const int m = (int)(local % M), n = (int)(local / M);
       const int64_t slot_stride = 16 * (int64_t)M * N;
       const double* Jc = J + 144 * in.cell_offset + 16 * local + 4 * i;
@@ -250,13 +269,14 @@ __global__ void __launch_bounds__(256) k_apply_states_fwd4(Table t, int64_t n_ce
 __global__ void __launch_bounds__(256) k_apply_states_rev4(Table t, int64_t n_cells,
                                                            const double* J, const double* w,
                                                            double* y) {
-  for (int64_t gq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gq < 4 * n_cells;
-       gq += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t g = gq >> 2;
-    const int i = (int)(gq & 3);
-    const Instance in = t.cell(g);
-    const int M = in.M, N = in.N;
-    const int64_t local = g - in.cell_offset;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int M = in.M, N = in.N;
+  const int64_t cells = (int64_t)M * N;
+  for (int64_t lq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lq < 4 * cells;
+       lq += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t local = lq >> 2;
+    const int64_t g = in.cell_offset + local;
+    const int i = (int)(lq & 3);
     const int m = (int)(local % M), n = (int)(local / M);
     const int64_t slot_stride = 16 * (int64_t)M * N;
     const double* Ji = J + 144 * in.cell_offset;
@@ -289,11 +309,12 @@ __global__ void __launch_bounds__(256) k_apply_states_rev4(Table t, int64_t n_ce
 __global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, int64_t n_cells,
                                                             const double* J, const double* x,
                                                             double* y) {
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    const Instance in = t.cell(g);
-    const int M = in.M, N = in.N;
-    const int64_t local = g - in.cell_offset;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int M = in.M, N = in.N;
+  const int64_t cells = (int64_t)M * N;
+  for (int64_t local = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; local < cells;
+       local += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = in.cell_offset + local;
     const int m = (int)(local % M), n = (int)(local / M);
     const int64_t slot_stride = 8 * (int64_t)M * N;
     const double* Jc = J + 32 * in.cell_offset + 8 * local;
@@ -326,13 +347,14 @@ __global__ void __launch_bounds__(256) k_apply_vertices_rev(Table t, int64_t n_v
                                                             double* y) {
   // Two threads per vertex: thread d computes component d from column d of each 4x2 block
   // (32 contiguous bytes), which keeps the registers per thread low and many loads in flight.
-  for (int64_t gq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gq < 2 * n_verts;
-       gq += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t g = gq >> 1;
-    const int d = (int)(gq & 1);
-    const Instance in = t.vert(g);
-    const int M = in.M, N = in.N;
-    const int64_t local = g - in.vert_offset;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int M = in.M, N = in.N;
+  const int64_t verts = (int64_t)(M + 1) * (N + 1);
+  for (int64_t lq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; lq < 2 * verts;
+       lq += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t local = lq >> 1;
+    const int64_t g = in.vert_offset + local;
+    const int d = (int)(lq & 1);
     const int m = (int)(local % (M + 1)), n = (int)(local / (M + 1));
     const int64_t slot_stride = 8 * (int64_t)M * N;
     const double* Ji = J + 32 * in.cell_offset;
@@ -367,18 +389,12 @@ __global__ void __launch_bounds__(256) k_apply_vertices_rev(Table t, int64_t n_v
 // apply_odes_wrt_mach_fwd, f90:604-621.
 __global__ void k_apply_mach_fwd(Table t, int64_t n_cells, const double* J, const double* dm,
                                  double* y) {
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    int idx = 0;
-    if (t.dev) {
-      int lo = 0, hi = t.n - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (t.dev[mid].cell_offset <= g) lo = mid; else hi = mid - 1;
-      }
-      idx = lo;
-    }
-    const C2 d = ldc(dm + 2 * idx);
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const C2 d = ldc(dm + 2 * blockIdx.y);
+  const int64_t cells = (int64_t)in.M * in.N;
+  for (int64_t local = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; local < cells;
+       local += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = in.cell_offset + local;
     const double2 j01 = __ldg(reinterpret_cast<const double2*>(J + 4 * g));
     const double2 j23 = __ldg(reinterpret_cast<const double2*>(J + 4 * g + 2));
     const double jv[4] = {j01.x, j01.y, j23.x, j23.y};
@@ -738,8 +754,9 @@ int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double*
   EB_ALIGNED(J, d_mach, d_odes);
   if (!J || !d_mach || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_mach_fwd<<<grid_for(b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J,
-                                                                              d_mach, d_odes);
+  dim3 grid;
+  if (int rc = per_instance_grid(b, false, 1, 256, grid)) return rc;
+  k_apply_mach_fwd<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_mach, d_odes);
   return check_launch("apply_odes_wrt_mach_fwd");
 }
 
@@ -759,8 +776,9 @@ int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const doubl
   EB_ALIGNED(J, d_states, d_odes);
   if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_states_fwd4<<<grid_for(4 * b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
-      t, b->n_cells, J, d_states, d_odes);
+  dim3 grid;
+  if (int rc = per_instance_grid(b, false, 4, 256, grid)) return rc;
+  k_apply_states_fwd4<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_states, d_odes);
   return check_launch("apply_odes_wrt_states_fwd");
 }
 
@@ -770,8 +788,9 @@ int eb_apply_odes_wrt_states_rev(const eb_batch* b, const double* J, const doubl
   EB_ALIGNED(J, d_odes, d_states);
   if (!J || !d_states || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_states_rev4<<<grid_for(4 * b->n_cells, 256), 256, 0, EB_STREAM(stream)>>>(
-      t, b->n_cells, J, d_odes, d_states);
+  dim3 grid;
+  if (int rc = per_instance_grid(b, false, 4, 256, grid)) return rc;
+  k_apply_states_rev4<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_odes, d_states);
   return check_launch("apply_odes_wrt_states_rev");
 }
 
@@ -781,8 +800,10 @@ int eb_apply_odes_wrt_vertices_fwd(const eb_batch* b, const double* J,
   EB_ALIGNED(J, d_vertices, d_odes);
   if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_vertices_fwd<<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
-      t, b->n_cells, J, d_vertices, d_odes);
+  dim3 grid;
+  if (int rc = per_instance_grid(b, false, 1, 128, grid)) return rc;
+  k_apply_vertices_fwd<<<grid, 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_vertices,
+                                                           d_odes);
   return check_launch("apply_odes_wrt_vertices_fwd");
 }
 
@@ -792,8 +813,10 @@ int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const dou
   EB_ALIGNED(J, d_odes, d_vertices);
   if (!J || !d_vertices || !d_odes) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_apply_vertices_rev<<<grid_for(2 * b->n_verts, 256), 256, 0, EB_STREAM(stream)>>>(
-      t, b->n_verts, J, d_odes, d_vertices);
+  dim3 grid;
+  if (int rc = per_instance_grid(b, true, 2, 256, grid)) return rc;
+  k_apply_vertices_rev<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_verts, J, d_odes,
+                                                           d_vertices);
   return check_launch("apply_odes_wrt_vertices_rev");
 }
 
