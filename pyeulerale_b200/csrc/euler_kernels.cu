@@ -210,9 +210,8 @@ __global__ void __launch_bounds__(256) k_forces(Table t, const double* X, const 
 // the slots before the columns are added (the reference sums each block's product row by row),
 // a reordering at the rounding level. The loop runs per warp so that every lane reaches the
 // shuffles.
-__global__ void __launch_bounds__(256) k_apply_states_fwd4(Table t, int64_t n_cells,
-                                                           const double* J, const double* x,
-                                                           double* y) {
+__global__ void __launch_bounds__(256) k_apply_states_fwd4(Table t, const double* J,
+                                                           const double* x, double* y) {
   const int i = threadIdx.x & 3;
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
   const int M = in.M, N = in.N;
@@ -266,9 +265,8 @@ __global__ void __launch_bounds__(256) k_apply_states_fwd4(Table t, int64_t n_ce
 // contiguous bytes; the four threads of a state read the block's 128 bytes together). Few
 // registers per thread let many warps keep DRAM loads in flight (one thread per state, with
 // the whole block in registers, reached 64 % of the HBM copy bandwidth, this 84 %).
-__global__ void __launch_bounds__(256) k_apply_states_rev4(Table t, int64_t n_cells,
-                                                           const double* J, const double* w,
-                                                           double* y) {
+__global__ void __launch_bounds__(256) k_apply_states_rev4(Table t, const double* J,
+                                                           const double* w, double* y) {
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
   const int M = in.M, N = in.N;
   const int64_t cells = (int64_t)M * N;
@@ -306,9 +304,8 @@ __global__ void __launch_bounds__(256) k_apply_states_rev4(Table t, int64_t n_ce
 }
 
 // apply_odes_wrt_vertices_fwd, f90:1005-1032.
-__global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, int64_t n_cells,
-                                                            const double* J, const double* x,
-                                                            double* y) {
+__global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, const double* J,
+                                                            const double* x, double* y) {
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
   const int M = in.M, N = in.N;
   const int64_t cells = (int64_t)M * N;
@@ -342,9 +339,8 @@ __global__ void __launch_bounds__(128) k_apply_vertices_fwd(Table t, int64_t n_c
 
 // apply_odes_wrt_vertices_rev, f90:1044-1072, gathered per vertex (no wrap: the closing
 // vertex column n = N is distinct from n = 0, as in the reference).
-__global__ void __launch_bounds__(256) k_apply_vertices_rev(Table t, int64_t n_verts,
-                                                            const double* J, const double* w,
-                                                            double* y) {
+__global__ void __launch_bounds__(256) k_apply_vertices_rev(Table t, const double* J,
+                                                            const double* w, double* y) {
   // Two threads per vertex: thread d computes component d from column d of each 4x2 block
   // (32 contiguous bytes), which keeps the registers per thread low and many loads in flight.
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
@@ -387,8 +383,7 @@ __global__ void __launch_bounds__(256) k_apply_vertices_rev(Table t, int64_t n_v
 }
 
 // apply_odes_wrt_mach_fwd, f90:604-621.
-__global__ void k_apply_mach_fwd(Table t, int64_t n_cells, const double* J, const double* dm,
-                                 double* y) {
+__global__ void k_apply_mach_fwd(Table t, const double* J, const double* dm, double* y) {
   const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
   const C2 d = ldc(dm + 2 * blockIdx.y);
   const int64_t cells = (int64_t)in.M * in.N;
@@ -756,7 +751,7 @@ int eb_apply_odes_wrt_mach_fwd(const eb_batch* b, const double* J, const double*
   const Table t = make_table(b);
   dim3 grid;
   if (int rc = per_instance_grid(b, false, 1, 256, grid)) return rc;
-  k_apply_mach_fwd<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_mach, d_odes);
+  k_apply_mach_fwd<<<grid, 256, 0, EB_STREAM(stream)>>>(t, J, d_mach, d_odes);
   return check_launch("apply_odes_wrt_mach_fwd");
 }
 
@@ -778,7 +773,7 @@ int eb_apply_odes_wrt_states_fwd(const eb_batch* b, const double* J, const doubl
   const Table t = make_table(b);
   dim3 grid;
   if (int rc = per_instance_grid(b, false, 4, 256, grid)) return rc;
-  k_apply_states_fwd4<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_states, d_odes);
+  k_apply_states_fwd4<<<grid, 256, 0, EB_STREAM(stream)>>>(t, J, d_states, d_odes);
   return check_launch("apply_odes_wrt_states_fwd");
 }
 
@@ -790,7 +785,7 @@ int eb_apply_odes_wrt_states_rev(const eb_batch* b, const double* J, const doubl
   const Table t = make_table(b);
   dim3 grid;
   if (int rc = per_instance_grid(b, false, 4, 256, grid)) return rc;
-  k_apply_states_rev4<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_odes, d_states);
+  k_apply_states_rev4<<<grid, 256, 0, EB_STREAM(stream)>>>(t, J, d_odes, d_states);
   return check_launch("apply_odes_wrt_states_rev");
 }
 
@@ -802,8 +797,7 @@ int eb_apply_odes_wrt_vertices_fwd(const eb_batch* b, const double* J,
   const Table t = make_table(b);
   dim3 grid;
   if (int rc = per_instance_grid(b, false, 1, 128, grid)) return rc;
-  k_apply_vertices_fwd<<<grid, 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, J, d_vertices,
-                                                           d_odes);
+  k_apply_vertices_fwd<<<grid, 128, 0, EB_STREAM(stream)>>>(t, J, d_vertices, d_odes);
   return check_launch("apply_odes_wrt_vertices_fwd");
 }
 
@@ -815,8 +809,7 @@ int eb_apply_odes_wrt_vertices_rev(const eb_batch* b, const double* J, const dou
   const Table t = make_table(b);
   dim3 grid;
   if (int rc = per_instance_grid(b, true, 2, 256, grid)) return rc;
-  k_apply_vertices_rev<<<grid, 256, 0, EB_STREAM(stream)>>>(t, b->n_verts, J, d_odes,
-                                                           d_vertices);
+  k_apply_vertices_rev<<<grid, 256, 0, EB_STREAM(stream)>>>(t, J, d_odes, d_vertices);
   return check_launch("apply_odes_wrt_vertices_rev");
 }
 
