@@ -86,6 +86,24 @@ def test_apply_products(evaluated, oracle):
 def test_tangent_kernel(evaluated):
     """Matrix-free forward tangent == sum of the Jacobian products (complex direction)."""
     name, case, gpu, g, o = evaluated
+    check_tangent(name, gpu, o)
+
+
+@pytest.mark.parametrize("name", ["naca0004_33_sym", "naca0012_33"])
+def test_tangent_at_exact_free_stream(cuda, oracle, golden_grids, name):
+    """At an exact free stream many sensor numerators cancel to exactly zero and abs_c takes
+    its derivative sign from a zero (positive, as the reference's complex step does): the
+    tangent of the tiled dual kernel matches the complex-step Jacobian products there too."""
+    from pyeulerale_b200 import grid as G
+
+    case = make_case(name, golden_grids)
+    M, N = case["U"].shape[1], case["U"].shape[2]
+    case["U"] = G.perturbed_states(M, N, case["mach"], case["aoa"], 0.0,
+                                   np.random.default_rng(0))
+    check_tangent(name + "_free_stream", Gpu(cuda, case), oracle_eval(oracle, case))
+
+
+def check_tangent(name, gpu, o):
     M, N = gpu.M, gpu.N
     rng = np.random.default_rng(5)
     dU = crandn(rng, (4, M, N))
