@@ -64,7 +64,9 @@ typedef struct eb_instance {
 } eb_instance;
 
 /* A set of instances. For a single grid set n_inst = 1, d_table = NULL and fill `single`;
- * otherwise d_table is a DEVICE array of n_inst instances sorted by cell_offset. */
+ * otherwise d_table is a DEVICE array of n_inst (at most 65535) instances sorted by
+ * cell_offset, and max_dim must hold the largest M or N: the per-instance kernels run one grid
+ * row per instance sized by it (EB_ERR_ARG otherwise). */
 typedef struct eb_batch {
   const eb_instance* d_table;
   int32_t n_inst;
