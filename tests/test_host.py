@@ -55,6 +55,23 @@ def test_misaligned_arrays_rejected_before_any_launch(entry, n_arrays):
     assert err.value.code == -1
 
 
+@pytest.mark.parametrize("entry", ["eb_apply_odes_wrt_states_rev", "eb_apply_odes_wrt_states_fwd",
+                                   "eb_apply_odes_wrt_vertices_rev", "eb_apply_odes_wrt_mach_fwd"])
+def test_batch_without_max_dim_rejected_before_any_launch(entry):
+    """The per-instance product kernels size their grid rows by max_dim: a batch of several
+    instances without it is an argument error returned by the host-side checks (the fake table
+    and array addresses are never touched)."""
+    from pyeulerale_b200.build import build_library
+
+    build_library()
+    batch = _lib.single_batch(_lib.make_instance(8, 9, 0.5, 1.25))
+    batch.n_inst, batch.d_table, batch.max_dim = 2, 0x7F0000000000, 0
+    with pytest.raises(_lib.EulerB200Error, match="max_dim") as err:
+        _lib.call(entry, ctypes.byref(batch), 0x7F0000001000, 0x7F0000002000, 0x7F0000003000,
+                  None)
+    assert err.value.code == -1
+
+
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Instance) == 104
     assert _lib.Instance.wall_offset.offset == 24
