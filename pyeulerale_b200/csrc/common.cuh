@@ -19,6 +19,8 @@ namespace eb {
 int fail(int code, const char* msg);
 int check_launch(const char* what);
 int validate(const eb_batch* b);
+// Grid of a per-instance kernel (y = instance; defined in euler_kernels.cu).
+int per_instance_grid(const eb_batch* b, bool vertices, int per_item, int threads, dim3& grid);
 
 
 static_assert(sizeof(Instance) == sizeof(eb_instance), "instance layout mismatch");

@@ -45,10 +45,10 @@ __global__ void __launch_bounds__(128) k_jac_states(Table t, int64_t n_cells, co
   using TX = std::conditional_t<Dir == kDirVertices, B, double>;
   using TV = std::conditional_t<Dir == kDirVelocities, B, double>;
   using R = Dual<B, 4>;
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    const Instance in = t.cell(g);
-    const int64_t local = g - in.cell_offset;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int64_t cells = (int64_t)in.M * in.N;
+  for (int64_t local = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; local < cells;
+       local += (int64_t)gridDim.x * blockDim.x) {
     Plain p;
     load_plain(in, local, X, V, U, p);
     Direction dir;
@@ -101,10 +101,10 @@ __global__ void __launch_bounds__(128) k_jac_vertexlike(Table t, int64_t n_cells
   // the seeded variable is Dual<B, 2>; the other geometry variable keeps its base type
   using TX = std::conditional_t<Velo, TXb, Dual<B, 2>>;
   using TV = std::conditional_t<Velo, Dual<B, 2>, TVb>;
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    const Instance in = t.cell(g);
-    const int64_t local = g - in.cell_offset;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int64_t cells = (int64_t)in.M * in.N;
+  for (int64_t local = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; local < cells;
+       local += (int64_t)gridDim.x * blockDim.x) {
     Plain p;
     load_plain(in, local, X, V, U, p);
     Direction dir;
@@ -164,10 +164,11 @@ __global__ void __launch_bounds__(128) k_jac_mach(Table t, int64_t n_cells, cons
   using TS = std::conditional_t<Dir == kDirStates, B, double>;
   using TX = std::conditional_t<Dir == kDirVertices, B, double>;
   using TV = std::conditional_t<Dir == kDirVelocities, B, double>;
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_cells;
-       g += (int64_t)gridDim.x * blockDim.x) {
-    const Instance in = t.cell(g);
-    const int64_t local = g - in.cell_offset;
+  const Instance in = t.dev ? t.dev[blockIdx.y] : t.single;  // grid y = instance
+  const int64_t cells = (int64_t)in.M * in.N;
+  for (int64_t local = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; local < cells;
+       local += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = in.cell_offset + local;
     const int m = (int)(local % in.M);
     if (m != in.M - 1) {
       for (int r = 0; r < 4; ++r) store_b<B>(lift<B>(0.0), 4 * g + r, J, Jre, Jim);

@@ -13,7 +13,9 @@ int eb_compute_odes_wrt_mach(const eb_batch* b, const double* X, const double* V
   EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_jac_mach<double, kDirNone><<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+  dim3 jgrid;
+  if (int rc = per_instance_grid(b, false, 1, 128, jgrid)) return rc;
+  k_jac_mach<double, kDirNone><<<jgrid, 128, 0, EB_STREAM(stream)>>>(
       t, b->n_cells, X, V, U, nullptr, J, nullptr, nullptr);
   return check_launch("compute_odes_wrt_mach");
 }
@@ -24,7 +26,9 @@ int eb_compute_odes_wrt_states(const eb_batch* b, const double* X, const double*
   EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  k_jac_states<double, kDirNone><<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(
+  dim3 jgrid;
+  if (int rc = per_instance_grid(b, false, 1, 128, jgrid)) return rc;
+  k_jac_states<double, kDirNone><<<jgrid, 128, 0, EB_STREAM(stream)>>>(
       t, b->n_cells, X, V, U, nullptr, J, nullptr, nullptr);
   return check_launch("compute_odes_wrt_states");
 }
@@ -35,8 +39,10 @@ int eb_compute_odes_wrt_vertices(const eb_batch* b, const double* X, const doubl
   EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
+  dim3 jgrid;
+  if (int rc = per_instance_grid(b, false, 1, 128, jgrid)) return rc;
   k_jac_vertexlike<double, kDirNone, false>
-      <<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
+      <<<jgrid, 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
                                                                   nullptr, J, nullptr, nullptr);
   return check_launch("compute_odes_wrt_vertices");
 }
@@ -47,8 +53,10 @@ int eb_compute_odes_wrt_velocities(const eb_batch* b, const double* X, const dou
   EB_ALIGNED(X, V, U, J);
   if (!X || !U || !J) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
+  dim3 jgrid;
+  if (int rc = per_instance_grid(b, false, 1, 128, jgrid)) return rc;
   k_jac_vertexlike<double, kDirNone, true>
-      <<<grid_for(b->n_cells, 128), 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
+      <<<jgrid, 128, 0, EB_STREAM(stream)>>>(t, b->n_cells, X, V, U,
                                                                   nullptr, J, nullptr, nullptr);
   return check_launch("compute_odes_wrt_velocities");
 }

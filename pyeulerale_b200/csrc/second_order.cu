@@ -9,16 +9,16 @@ using namespace eb;
 
 extern "C" {
 
-#define EB_DIR_DISPATCH(KERNEL, N_ITEMS, ...)                                               \
+#define EB_DIR_DISPATCH(KERNEL, ...)                                                        \
   switch (dir_kind) {                                                                       \
     case kDirStates:                                                                        \
-      KERNEL<D2, kDirStates><<<grid_for(N_ITEMS, 128), 128, 0, EB_STREAM(stream)>>>(__VA_ARGS__); \
+      KERNEL<D2, kDirStates><<<jgrid, 128, 0, EB_STREAM(stream)>>>(__VA_ARGS__); \
       break;                                                                                \
     case kDirVertices:                                                                      \
-      KERNEL<D2, kDirVertices><<<grid_for(N_ITEMS, 128), 128, 0, EB_STREAM(stream)>>>(__VA_ARGS__); \
+      KERNEL<D2, kDirVertices><<<jgrid, 128, 0, EB_STREAM(stream)>>>(__VA_ARGS__); \
       break;                                                                                \
     case kDirVelocities:                                                                    \
-      KERNEL<D2, kDirVelocities><<<grid_for(N_ITEMS, 128), 128, 0, EB_STREAM(stream)>>>(__VA_ARGS__); \
+      KERNEL<D2, kDirVelocities><<<jgrid, 128, 0, EB_STREAM(stream)>>>(__VA_ARGS__); \
       break;                                                                                \
     default:                                                                                \
       return fail(EB_ERR_ARG, "dir_kind must be 0 (states), 1 (vertices) or 2 (velocities)"); \
@@ -32,7 +32,9 @@ int eb_odes_wrt_mach_dir(const eb_batch* b, const double* X, const double* V, co
   EB_ALIGNED(X, V, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  EB_DIR_DISPATCH(k_jac_mach, b->n_cells, t, b->n_cells, X, V, U, d, nullptr, J_re, J_im);
+  dim3 jgrid;
+  if (int rc = per_instance_grid(b, false, 1, 128, jgrid)) return rc;
+  EB_DIR_DISPATCH(k_jac_mach, t, b->n_cells, X, V, U, d, nullptr, J_re, J_im);
   return check_launch("odes_wrt_mach_dir");
 }
 
@@ -43,7 +45,9 @@ int eb_odes_wrt_states_dir(const eb_batch* b, const double* X, const double* V,
   EB_ALIGNED(X, V, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  EB_DIR_DISPATCH(k_jac_states, b->n_cells, t, b->n_cells, X, V, U, d, nullptr, J_re, J_im);
+  dim3 jgrid;
+  if (int rc = per_instance_grid(b, false, 1, 128, jgrid)) return rc;
+  EB_DIR_DISPATCH(k_jac_states, t, b->n_cells, X, V, U, d, nullptr, J_re, J_im);
   return check_launch("odes_wrt_states_dir");
 }
 
@@ -54,7 +58,8 @@ int eb_odes_wrt_vertices_dir(const eb_batch* b, const double* X, const double* V
   EB_ALIGNED(X, V, U, d, J_re, J_im);
   if (!X || !U || !d || !J_re || !J_im) return fail(EB_ERR_ARG, "null array");
   const Table t = make_table(b);
-  const int g = grid_for(b->n_cells, 128);
+  dim3 g;
+  if (int rc = per_instance_grid(b, false, 1, 128, g)) return rc;
   cudaStream_t s = EB_STREAM(stream);
   switch (dir_kind) {
     case kDirStates:
