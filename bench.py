@@ -87,7 +87,59 @@ def parse_args():
                    help="shifts factored concurrently (one workspace of ~2.7 GB each)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline budget")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--dry-run", action="store_true",
+                   help="rank plumbing only (gloo on the CPU, no GPU work): every rank joins, "
+                        "times an empty region, and rank 0 prints the JSON line")
     return p.parse_args()
+
+
+def launch_ranks(args) -> int | None:
+    """Starts one rank per GPU when ``--gpus N`` (N > 1) is given outside a torchrun launch.
+
+    Re-executes this script under ``torch.distributed.run`` (one node, N processes, rendezvous
+    on 127.0.0.1) and returns its exit code; returns None when this process already is a rank
+    (WORLD_SIZE set) or when one GPU is asked for.
+    """
+    if args.gpus <= 1 or "WORLD_SIZE" in os.environ:
+        return None
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
+def run_dry(args) -> None:
+    """The multi-rank skeleton of the B200 arm without a GPU: gloo process group, barrier,
+    max over ranks of a timed empty region, one JSON line from rank 0."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from pyeulerale_b200.batch import max_over_ranks
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but {world} ranks were started")
+    t0 = time.perf_counter()
+    if world > 1:
+        dist.barrier()
+    t = max_over_ranks(time.perf_counter() - t0)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "n_gpus": world,
+                          "dry_run": True, "max_rank_seconds": t,
+                          "config": {"instances_per_gpu": args.instances,
+                                     "parallelism": f"replicas x{world}"}}), flush=True)
 
 
 # ---- workload -------------------------------------------------------------------------------
@@ -408,6 +460,8 @@ def run_b200(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but {world} ranks were started")
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
@@ -871,6 +925,10 @@ def run_b200(args) -> None:
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": None if traffic_cell is None else traffic_cell * cells,
+                     "traffic_source": None if traffic_cell is None else
+                     f"ncu capture summarised in profiles/{PROFILE_SUMMARY.name} (DRAM bytes "
+                     "per cell of the same kernel, scaled to this launch's cells), not "
+                     "measured in this run",
                      "algorithmic_bytes_per_launch": BYTES_PER_CELL_RESIDUAL * cells,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "cpu_baseline": cpu,
@@ -900,6 +958,12 @@ def main() -> None:
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    rc = launch_ranks(args)
+    if rc is not None:
+        sys.exit(rc)
+    if args.dry_run:
+        run_dry(args)
     else:
         run_b200(args)
 

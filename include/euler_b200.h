@@ -217,7 +217,10 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
  * workspace is a 48 MiB array in the library's device memory, held by every GPU that loads the
  * library until the process exits; systems needing more (eb_gmres_workspace_bytes) are
  * rejected with EB_ERR_ARG. The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture. All calls share
+ * (cudaGetSymbolAddress); under CUDA's lazy module loading (the default) that lookup is also
+ * when the device commits the 48 MiB, so the first call is itself a device allocation: make it
+ * once at start-up, on each device, before the loop that may not allocate and before any
+ * stream capture. Later calls allocate nothing. All calls share
  * the array: calls that overlap on the GPU (other streams, other host threads) race and must be
  * serialised by the caller. No counterpart in the reference (its solver allocates on every
  * call, core.py:512-599). */

@@ -9,8 +9,9 @@ the GPU through the C ABI (``include/euler_b200.h``):
 
 * residual, forces and all Jacobians are forward-mode dual-number kernels (no complex step);
 * Jacobian products are stencil gathers on the device-resident Jacobians;
-* the resolvent ``(dR/dU - shift I)^-1`` is a complex GMRES with a block-Jacobi
-  preconditioner on the device (the reference factorises with SuperLU on every call);
+* the resolvent ``(dR/dU - shift I)^-1`` is a direct block LU over the grid's radial rings on
+  the device, refined to the solve tolerance (the reference factorises with SuperLU on every
+  call); complex GMRES with a block-Jacobi preconditioner is the alternative solver;
 * the 13 second-order routines are exact directional derivatives of the Jacobians (nested
   duals) instead of the reference's central differences of complex-step Jacobians, so they
   agree with the reference to its finite-difference truncation error.
@@ -461,7 +462,7 @@ class SpatialDiscretization:
 
     def solve_odes_wrt_states_fwd(self, d_odes: np.ndarray, shift: float | complex = 0.,
                                   d_states: np.ndarray | None = None) -> np.ndarray:
-        """``(dR/dU - shift Id)^-1 . dR`` by device GMRES (core.py:533-565)."""
+        """``(dR/dU - shift Id)^-1 . dR`` on the device (core.py:533-565)."""
         self._check_array(d_odes, self._odes.shape, dtype=d_odes.dtype)
         result_dtype = np.promote_types(type(shift), d_odes.dtype)
         if d_states is None:
@@ -475,7 +476,7 @@ class SpatialDiscretization:
 
     def solve_odes_wrt_states_adj(self, d_states: np.ndarray, shift: float | complex = 0.,
                                   d_odes: np.ndarray | None = None) -> np.ndarray:
-        """``(dR/dU - shift Id)^-H . dU`` by device GMRES (core.py:567-599)."""
+        """``(dR/dU - shift Id)^-H . dU`` on the device (core.py:567-599)."""
         self._check_array(d_states, self._odes.shape, dtype=d_states.dtype)
         result_dtype = np.promote_types(type(shift), d_states.dtype)
         if d_odes is None:

@@ -610,7 +610,8 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
     return fail(EB_ERR_ARG, "gmres: null argument");
   if (b->n_inst > 1 && !host_table) return fail(EB_ERR_ARG, "gmres: batch needs host_table");
   const int m = opt->restart;
-  if (m < 1 || opt->max_iterations < 1 || !(opt->tol > 0)) return fail(EB_ERR_ARG, "gmres: bad options");
+  if (m < 1 || opt->max_iterations < 1 || opt->check_every < 1 || !(opt->tol > 0))
+    return fail(EB_ERR_ARG, "gmres: bad options (restart, max_iterations and check_every >= 1, tol > 0)");
   std::vector<Sys> sys;
   int64_t n_cells, n_chunks;
   if (!build_systems(b, host_table, n_sys, sys_inst, shifts, adjoint, sys, n_cells, n_chunks))
@@ -799,6 +800,8 @@ extern "C" int eb_gmres_solve_noalloc(const eb_batch* b, const eb_instance* host
   if ((reinterpret_cast<uintptr_t>(J) | reinterpret_cast<uintptr_t>(rhs) |
        reinterpret_cast<uintptr_t>(x)) & 15)
     return fail(EB_ERR_ARG, "gmres_noalloc: arrays must be 16-byte aligned");
+  if (opt->restart < 1 || opt->max_iterations < 1 || opt->check_every < 1 || !(opt->tol > 0))
+    return fail(EB_ERR_ARG, "gmres_noalloc: bad options (restart, max_iterations and check_every >= 1, tol > 0)");
   const int64_t need = eb_gmres_workspace_bytes(b, host_table, n_sys, sys_inst, opt->restart);
   if (need < 0) return fail(EB_ERR_ARG, "gmres_noalloc: invalid systems");
   if (need > (int64_t)kStaticScratchBytes) {

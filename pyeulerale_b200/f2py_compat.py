@@ -6,7 +6,7 @@ module offers an object with the same 20 procedures (f90:68-87), the same callin
 (array sizes taken from the arrays, results written in place into the caller's Fortran-ordered
 arrays, complex128 fields and float64 Jacobians) and the same four module variables as writable
 0-d arrays (``aoa``, ``jst_k2``, ``jst_k4``, ``jst_c4``; f90:63-66). Binding it in place of the
-Fortran extension runs the reference's own ``core.py`` on the B200 (INTEGRATION.md).
+Fortran extension runs the reference's own ``core.py`` on the B200.
 
 Every call copies its host inputs to the device, launches the kernel through the C ABI and
 copies the result back. The complex fields' imaginary parts are not used: the reference stores

@@ -1,9 +1,8 @@
 """Generates the committed golden fixtures from the PyEulerALE reference checkout.
 
-Run in a checkout that has the reference sources (``PYEULERALE_REFERENCE``, default
-``/root/reference``):
+Run with ``PYEULERALE_REFERENCE`` naming a checkout of the reference sources:
 
-    python tests/golden/make_golden.py
+    PYEULERALE_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 It writes, next to this script:
 
@@ -81,7 +80,9 @@ def _reference_function(path: Path, name: str):
     return namespace[name]
 
 
-def main(root: Path = DEFAULT_REFERENCE) -> None:
+def main(root: Path | None = DEFAULT_REFERENCE) -> None:
+    if root is None:
+        raise SystemExit("set PYEULERALE_REFERENCE to a checkout of the reference sources")
     grids = {}
     for key, rel in GRIDS.items():
         pts = np.loadtxt(root / rel, dtype=int, skiprows=1, max_rows=1)

@@ -54,3 +54,31 @@ def test_cpu_reference_methods_run_on_a_small_grid():
     assert res["value"] > 0 and "relative residual" in res["sample"]
     rel = float(res["sample"].split("relative residual ")[1].split(")")[0])
     assert rel < 1e-8
+
+
+def test_gpus_flag_starts_that_many_ranks():
+    """``bench.py --gpus 2`` outside torchrun starts two ranks (here in the gloo dry run, which
+    runs the launcher, the rank check, the barrier and the max over ranks without a GPU) and
+    prints one JSON line whose n_gpus is 2."""
+    import os
+
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--dry-run",
+                          "--steps", "3", "--warmup", "3"], cwd=ROOT, capture_output=True,
+                         text=True, timeout=300, check=True, env=env).stdout
+    lines = [json.loads(s) for s in out.strip().splitlines() if s.startswith("{")]
+    assert len(lines) == 1, out
+    assert lines[0]["n_gpus"] == 2 and lines[0]["dry_run"] is True
+    assert lines[0]["config"]["parallelism"] == "replicas x2"
+
+
+def test_rank_count_mismatch_fails_loudly():
+    """A rank whose WORLD_SIZE disagrees with --gpus stops before any timing."""
+    import os
+
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    proc = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--dry-run"],
+                          cwd=ROOT, capture_output=True, text=True, timeout=120, env=env)
+    assert proc.returncode != 0
+    assert "2 but 1 ranks" in proc.stderr

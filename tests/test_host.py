@@ -122,3 +122,36 @@ def test_dropin_requires_cuda(golden_grids):
 
     with pytest.raises(RuntimeError, match="CUDA"):
         SpatialDiscretization(golden_grids["naca0012_8x9"])
+
+
+@pytest.mark.parametrize("field,value", [("check_every", 0), ("restart", 0),
+                                         ("max_iterations", 0), ("tol", 0.0)])
+def test_gmres_bad_options_rejected_before_any_launch(field, value):
+    """GMRES options out of range (check_every = 0 would divide by zero on the host) are an
+    argument error returned before any launch, for both GMRES entry points (the fake device
+    addresses are never touched)."""
+    from pyeulerale_b200 import solver
+    from pyeulerale_b200.build import build_library
+
+    build_library()
+    lib = solver._bind()
+    batch = _lib.single_batch(_lib.make_instance(8, 9, 0.5, 1.25))
+    opts = solver.GmresOptions(1e-10, 30, 100, 10, 0)
+    setattr(opts, field, value)
+    infos = (solver.GmresInfo * 1)()
+    shifts = np.array([1.0, 0.0])
+    fake = 0x7F0000000000
+    rc = lib.eb_gmres_solve(ctypes.byref(batch), None, fake, 1, None, shifts.ctypes.data, 0,
+                            fake, fake, ctypes.byref(opts), fake, 1 << 30, infos, None)
+    assert rc == _lib.EB_ERR_ARG
+    assert "bad options" in lib.eb_last_error().decode()
+    lib.eb_gmres_solve_noalloc.restype = ctypes.c_int
+    lib.eb_gmres_solve_noalloc.argtypes = [
+        ctypes.POINTER(_lib.Batch), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.POINTER(solver.GmresOptions), ctypes.POINTER(solver.GmresInfo), ctypes.c_void_p]
+    rc = lib.eb_gmres_solve_noalloc(ctypes.byref(batch), None, fake, 1, None,
+                                    shifts.ctypes.data, 0, fake, fake, ctypes.byref(opts),
+                                    infos, None)
+    assert rc == _lib.EB_ERR_ARG
+    assert "bad options" in lib.eb_last_error().decode()

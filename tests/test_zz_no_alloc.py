@@ -4,7 +4,8 @@ Callers that cannot allocate device memory (their memory belongs to another runt
 their loop may not allocate once running) use the entry point whose workspace is the library's
 fixed 48 MiB device array. Two calls in a row must give the same solutions as the allocating
 entry point: the array keeps the previous call's contents, so anything left over must not leak
-into the next solve. This file is collected last so that a failure here cannot hide others.
+into the next solve. After its first call on a device, a call must leave the device's free
+memory unchanged. This file is collected last so that a failure here cannot hide others.
 """
 
 from __future__ import annotations
@@ -36,6 +37,44 @@ def test_noalloc_matches_allocating_solver_twice(cuda, golden_grids):
                                                  sys_inst=[0] * len(shifts), x=x)
         assert info.max_rel_residual <= 1e-10
         assert rel_err(got.cpu().numpy(), ref.cpu().numpy()) <= 1e-10, (info, info_ref)
+
+
+def test_noalloc_two_instances_allocates_nothing(cuda, golden_grids):
+    """A batch of two instances of different size (systems mapped by sys_inst, sizes from the
+    host table): the same solutions as the allocating entry point on two calls in a row, and
+    the second call leaves the device's free memory and torch's allocation unchanged."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200 import solver
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    rng = np.random.default_rng(31)
+    grids = [golden_grids["naca0012_8x9"], G.naca_ogrid(13, 17, 0.08, 1.0, 15.0, 0.02)]
+    specs = [InstanceSpec(grids[0], 0.5, 1.25), InstanceSpec(grids[1], 0.4, -1.0)]
+    inst = InstanceSet(specs)
+    states = [G.perturbed_states(s.M, s.N, s.mach, s.aoa_deg, 0.01, rng) for s in specs]
+    dX = cuda.from_numpy(inst.pack_vertices()).cuda()
+    dV = cuda.zeros_like(dX)
+    dU = cuda.from_numpy(inst.pack_cells(states)).cuda()
+    J = cuda.zeros(144 * inst.n_cells, dtype=cuda.float64, device="cuda")
+    inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J)
+    sys_inst = [1, 0, 1]
+    shifts = [0.4 + 0.3j, 1.5, 1.0j]
+    sizes = [8 * specs[i].M * specs[i].N for i in sys_inst]
+    rhs = cuda.from_numpy(rng.standard_normal(sum(sizes))).cuda()
+    kw = dict(sys_inst=sys_inst, host_table=inst.host_table)
+    ref, _ = solver.solve_shifted(inst.batch, J, rhs, shifts, **kw)
+    x = cuda.full_like(rhs, np.nan)
+    solver.solve_shifted_noalloc(inst.batch, J, rhs, shifts, x=x, **kw)  # first call: set-up
+    cuda.cuda.synchronize()
+    free0, alloc0 = cuda.cuda.mem_get_info()[0], cuda.cuda.memory_allocated()
+    x.fill_(np.nan)
+    got, info = solver.solve_shifted_noalloc(inst.batch, J, rhs, shifts, x=x, **kw)
+    cuda.cuda.synchronize()
+    assert cuda.cuda.mem_get_info()[0] == free0
+    assert cuda.cuda.memory_allocated() == alloc0
+    assert got.data_ptr() == x.data_ptr()
+    assert info.max_rel_residual <= 1e-10
+    assert rel_err(got.cpu().numpy(), ref.cpu().numpy()) <= 1e-10, info
 
 
 def test_noalloc_rejects_oversized_systems(cuda):
