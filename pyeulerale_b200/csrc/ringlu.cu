@@ -15,6 +15,9 @@
 // (primes: blocks already updated by earlier rings). B2 and C2 are never updated, so they stay
 // block diagonal and the products with them are block-row / block-column scalings instead of
 // dense GEMMs: a ring costs one inversion and three dense complex GEMMs of order K.
+// Storage per ring: Dinv_m, L1[m] and C1'[m] as dense super-blocks, B2 and C2 as their N real
+// 4 x 4 diagonal blocks. L2[m+2] is only needed while ring m is eliminated (one scratch block):
+// the solves apply it as B2[m+2] (Dinv_m y), one dense product with the stored inverse.
 // This replaces the reference's SuperLU factorisation (src/py_euler_ale/core.py:512-599) and is
 // the robust path for shifts near zero, where Krylov methods with local preconditioners
 // stagnate. One factorisation serves both the forward solve and the Hermitian-adjoint solve
@@ -116,10 +119,11 @@ constexpr int kGjBlockMinShifts = 8;
 
 struct Layout {
   int M, N, K;
-  size_t blk;  // bytes of one K x K complex block
-  size_t off_D, off_L1, off_L2, off_C1, off_C2, off_T, off_Rp, off_perm, off_info, off_acc,
-      off_shift;
-  size_t off_y, off_x, off_r;
+  size_t blk;   // bytes of one K x K complex block
+  size_t bdr;   // bytes of one ring's block diagonal (N real 4 x 4 blocks)
+  size_t off_D, off_L1, off_C1, off_B2, off_C2, off_T, off_L2, off_Rp, off_perm, off_info,
+      off_acc, off_shift;
+  size_t off_y, off_x, off_r, off_w;
   size_t total;
 };
 
@@ -135,12 +139,14 @@ Layout plan(int M, int N) {
     o = align_up(o + bytes);
     return at;
   };
+  L.bdr = sizeof(double) * 16 * (size_t)N;
   L.off_D = take(L.blk * M);
   L.off_L1 = take(L.blk * M);
-  L.off_L2 = take(L.blk * M);
   L.off_C1 = take(L.blk * M);
-  L.off_C2 = take(L.blk * M);
+  L.off_B2 = take(L.bdr * M);
+  L.off_C2 = take(L.bdr * M);
   L.off_T = take(L.blk);
+  L.off_L2 = take(L.blk);
   L.off_Rp = take(sizeof(cuDoubleComplex) * (size_t)kGjBlock * L.K);
   L.off_perm = take(sizeof(int) * (size_t)L.K);
   L.off_info = take(sizeof(int) * 4);
@@ -150,15 +156,17 @@ Layout plan(int M, int N) {
   L.off_y = take(vec);
   L.off_x = take(vec);
   L.off_r = take(vec);
+  L.off_w = take(vec);
   L.total = o;
   return L;
 }
 
 // Scatters the 4x4 blocks of the nine-slot Jacobian into the ring super-blocks
-// (column-major K x K) and subtracts the shift on the diagonal.
+// (column-major K x K) and subtracts the shift on the diagonal; the ii / oo blocks (B2, C2)
+// go to the rings' block diagonals (ring m, cell n: 16 doubles at 16 (m N + n), column-major).
 __global__ void k_assemble(int M, int N, const double* J, const double* shift,
-                           cuDoubleComplex* D, cuDoubleComplex* B1, cuDoubleComplex* B2,
-                           cuDoubleComplex* C1, cuDoubleComplex* C2) {
+                           cuDoubleComplex* D, cuDoubleComplex* B1, double* B2,
+                           cuDoubleComplex* C1, double* C2) {
   const double sr = shift[0], si = shift[1];
   const int64_t cells = (int64_t)M * N;
   const int K = 4 * N;
@@ -171,13 +179,16 @@ __global__ void k_assemble(int M, int N, const double* J, const double* shift,
     const int m = (int)(c % M), n = (int)(c / M);
     if (!slot_active(s, m, M)) continue;
     const double* J16 = J + slot_stride * s + 16 * c;
+    if (s == kII || s == kOO) {
+      double* bd = (s == kII ? B2 : C2) + 16 * ((int64_t)m * N + n);
+      for (int e = 0; e < 16; ++e) bd[e] = J16[e];
+      continue;
+    }
     const int nn = wrap(n + slot_dn(s), N);
     cuDoubleComplex* T;
     switch (s) {
       case kI: T = B1 + blk * m; break;
-      case kII: T = B2 + blk * m; break;
       case kO: T = C1 + blk * m; break;
-      case kOO: T = C2 + blk * m; break;
       default: T = D + blk * m; break;
     }
     for (int i = 0; i < 4; ++i)
@@ -501,19 +512,17 @@ __global__ void __launch_bounds__(256) k_gj_permute(int K, char* ws0, int64_t st
   }
 }
 
-// Block-diagonal left product in place: X <- Bd X, where X (at off_X) holds the block-diagonal
-// Bd in its 4 x 4 diagonal blocks on entry and Y = Bd Src is written over it (Src at off_S).
+// Block-diagonal left product: X = Bd S, Bd the N real 4 x 4 blocks at off_bd (one ring's
+// block diagonal), S the K x K block at off_S, X the K x K block at off_X.
 // Grid: N row blocks x shifts.
-__global__ void __launch_bounds__(256) k_bd_left(int K, char* ws0, int64_t stride, size_t off_X,
-                                                 size_t off_S) {
-  __shared__ cuDoubleComplex bd[4][4];
-  cuDoubleComplex* X = at<cuDoubleComplex>(ws0, stride, off_X);
+__global__ void __launch_bounds__(256) k_bd_left(int K, char* ws0, int64_t stride, size_t off_bd,
+                                                 size_t off_S, size_t off_X) {
+  __shared__ double bd[16];
+  const double* B = at<const double>(ws0, stride, off_bd);
   const cuDoubleComplex* S = at<cuDoubleComplex>(ws0, stride, off_S);
+  cuDoubleComplex* X = at<cuDoubleComplex>(ws0, stride, off_X);
   const int n = blockIdx.x;
-  if (threadIdx.x < 16) {
-    const int r = threadIdx.x & 3, q = threadIdx.x >> 2;
-    bd[r][q] = X[(size_t)K * (4 * n + q) + 4 * n + r];
-  }
+  if (threadIdx.x < 16) bd[threadIdx.x] = B[16 * n + threadIdx.x];
   __syncthreads();
   for (int c = threadIdx.x; c < K; c += blockDim.x) {
     const cuDoubleComplex* s = S + (size_t)K * c + 4 * n;
@@ -521,29 +530,24 @@ __global__ void __launch_bounds__(256) k_bd_left(int K, char* ws0, int64_t strid
     cuDoubleComplex* x = X + (size_t)K * c + 4 * n;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      cuDoubleComplex acc = cmul(bd[r][0], s0);
-      acc = cfma(bd[r][1], s1, acc);
-      acc = cfma(bd[r][2], s2, acc);
-      acc = cfma(bd[r][3], s3, acc);
-      x[r] = acc;
+      const double b0 = bd[r], b1 = bd[r + 4], b2 = bd[r + 8], b3 = bd[r + 12];
+      x[r] = make_cuDoubleComplex(fma(b3, s3.x, fma(b2, s2.x, fma(b1, s1.x, b0 * s0.x))),
+                                  fma(b3, s3.y, fma(b2, s2.y, fma(b1, s1.y, b0 * s0.y))));
     }
   }
 }
 
 // Block-diagonal right products: Y -= X Bd for two (X, Y) pairs selected by blockIdx.z, Bd the
-// 4 x 4 diagonal blocks stored in the K x K block at off_B. Grid: N column blocks x shifts x 2.
-__global__ void __launch_bounds__(256) k_bd_right(int K, char* ws0, int64_t stride, size_t off_B,
+// N real 4 x 4 blocks at off_bd. Grid: N column blocks x shifts x 2.
+__global__ void __launch_bounds__(256) k_bd_right(int K, char* ws0, int64_t stride, size_t off_bd,
                                                   size_t off_X0, size_t off_Y0, size_t off_X1,
                                                   size_t off_Y1) {
-  __shared__ cuDoubleComplex bd[4][4];
-  const cuDoubleComplex* B = at<cuDoubleComplex>(ws0, stride, off_B);
+  __shared__ double bd[16];
+  const double* B = at<const double>(ws0, stride, off_bd);
   const cuDoubleComplex* X = at<cuDoubleComplex>(ws0, stride, blockIdx.z ? off_X1 : off_X0);
   cuDoubleComplex* Y = at<cuDoubleComplex>(ws0, stride, blockIdx.z ? off_Y1 : off_Y0);
   const int n = blockIdx.x;
-  if (threadIdx.x < 16) {
-    const int q = threadIdx.x & 3, c = threadIdx.x >> 2;
-    bd[q][c] = B[(size_t)K * (4 * n + c) + 4 * n + q];
-  }
+  if (threadIdx.x < 16) bd[threadIdx.x] = B[16 * n + threadIdx.x];
   __syncthreads();
   for (int r = threadIdx.x; r < K; r += blockDim.x) {
     cuDoubleComplex x[4];
@@ -554,9 +558,37 @@ __global__ void __launch_bounds__(256) k_bd_right(int K, char* ws0, int64_t stri
       cuDoubleComplex* y = Y + (size_t)K * (4 * n + c) + r;
       cuDoubleComplex acc = *y;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc = cfms(x[q], bd[q][c], acc);
+      for (int q = 0; q < 4; ++q) {
+        const double b = bd[q + 4 * c];
+        acc.x = fma(-x[q].x, b, acc.x);
+        acc.y = fma(-x[q].y, b, acc.y);
+      }
       *y = acc;
     }
+  }
+}
+
+// Block-diagonal vector product of the solves: out -= Bd v (trans = 0) or out -= Bd^T v
+// (trans = 1; the blocks are real, so Bd^H = Bd^T), or out = -(...) when `assign` is set. Bd:
+// N real 4 x 4 blocks at off_bd; v, out: K complex at off_v, off_out. Grid: blocks x shifts.
+__global__ void __launch_bounds__(128) k_bd_vec(int N, char* ws0, int64_t stride, size_t off_bd,
+                                                size_t off_v, size_t off_out, int trans,
+                                                int assign) {
+  const double* B = at<const double>(ws0, stride, off_bd);
+  const cuDoubleComplex* v = at<cuDoubleComplex>(ws0, stride, off_v);
+  cuDoubleComplex* out = at<cuDoubleComplex>(ws0, stride, off_out);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 4 * N; e += gridDim.x * blockDim.x) {
+    const int n = e >> 2, r = e & 3;
+    const double* b = B + 16 * n;
+    const cuDoubleComplex* vn = v + 4 * n;
+    cuDoubleComplex acc = assign ? make_cuDoubleComplex(0.0, 0.0) : out[e];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double bi = trans ? b[i + 4 * r] : b[r + 4 * i];
+      acc.x = fma(-bi, vn[i].x, acc.x);
+      acc.y = fma(-bi, vn[i].y, acc.y);
+    }
+    out[e] = acc;
   }
 }
 
@@ -802,16 +834,17 @@ int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int si
       return rc;
   }
   if (m + 2 < M) {
-    // L2[m+2] = B2[m+2] Dinv_m;  B1'[m+2] -= L2[m+2] C1'[m]
-    k_bd_left<<<dim3(N, g.S), 256, 0, st>>>(K, g.base, g.stride, g.boff(L.off_L2, m + 2), g.boff(L.off_D, m));
+    // L2[m+2] = B2[m+2] Dinv_m (scratch);  B1'[m+2] -= L2[m+2] C1'[m]
+    k_bd_left<<<dim3(N, g.S), 256, 0, st>>>(K, g.base, g.stride, L.off_B2 + L.bdr * (m + 2),
+                                            g.boff(L.off_D, m), L.off_L2);
     if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone,
-                                                g.blk(L.off_L2, m + 2), K, es, g.blk(L.off_C1, m), K, es,
+                                                g.blk(L.off_L2, 0), K, es, g.blk(L.off_C1, m), K, es,
                                                 &one, g.blk(L.off_L1, m + 2), K, es, g.S),
                       "ringlu: gemm L1 update")) != EB_OK)
       return rc;
     // D[m+2] -= L2[m+2] C2[m];  C1'[m+1] -= L1[m+1] C2[m]
-    k_bd_right<<<dim3(N, g.S, 2), 256, 0, st>>>(K, g.base, g.stride, g.boff(L.off_C2, m),
-                                                g.boff(L.off_L2, m + 2), g.boff(L.off_D, m + 2),
+    k_bd_right<<<dim3(N, g.S, 2), 256, 0, st>>>(K, g.base, g.stride, L.off_C2 + L.bdr * m,
+                                                L.off_L2, g.boff(L.off_D, m + 2),
                                                 L.off_T, g.boff(L.off_C1, m + 1));
   }
   if (m + 1 < M &&
@@ -822,45 +855,60 @@ int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int si
 }
 
 // Ring-ordered triangular solves with the stored factors for every shift: y (ring layout)
-// holds the right-hand sides on entry; the solutions are left in x.
-int ring_solve(const Group& g, cublasHandle_t h, bool adjoint) {
+// holds the right-hand sides on entry; the solutions are left in x (w: scratch vectors).
+// A = Lt Ut with L2[m] = B2[m] Dinv_{m-2}, so the forward sweep keeps w[m] = Dinv_m y[m] of the
+// finished rings and subtracts B2[m] w[m-2]; the adjoint sweep applies L2[m+2]^H as
+// Dinv_m^H (B2[m+2]^T x[m+2]).
+int ring_solve(const Group& g, cublasHandle_t h, bool adjoint, cudaStream_t stream) {
   const Layout& L = g.L;
-  const int M = L.M, K = L.K;
+  const int M = L.M, K = L.K, N = L.N;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
   const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
   const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
   const int64_t es = g.es();
   cuDoubleComplex* y = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_y);
   cuDoubleComplex* x = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_x);
+  cuDoubleComplex* w = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_w);
   auto yv = [&](int m) { return y + (size_t)K * m; };
   auto xv = [&](int m) { return x + (size_t)K * m; };
+  auto wv = [&](int m) { return w + (size_t)K * m; };
+  const size_t vb = sizeof(cuDoubleComplex) * (size_t)K;  // bytes of one ring vector
   auto gemv = [&](cublasOperation_t op, const cuDoubleComplex* alpha, const cuDoubleComplex* A,
                   const cuDoubleComplex* v, const cuDoubleComplex* beta, cuDoubleComplex* out) {
     return cublasZgemvStridedBatched(h, op, K, K, alpha, A, K, es, v, 1, es, beta, out, 1, es, g.S);
+  };
+  const dim3 bdg((4 * N + 127) / 128, g.S);
+  // out -= Bd v (trans: Bd^T v), ring vectors given by workspace offsets; assign: out = -Bd v
+  auto bdvec = [&](size_t off_bd, size_t off_v, size_t off_out, int trans, int assign) {
+    k_bd_vec<<<bdg, 128, 0, stream>>>(N, g.base, g.stride, off_bd, off_v, off_out, trans, assign);
   };
   cublasStatus_t st = CUBLAS_STATUS_SUCCESS;
   auto run = [&](cublasStatus_t s) {
     if (s != CUBLAS_STATUS_SUCCESS) st = s;
   };
   if (!adjoint) {
-    for (int m = 1; m < M; ++m) {  // Lt z = b (in y)
-      run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_L1, m), yv(m - 1), &one, yv(m)));
-      if (m >= 2) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_L2, m), yv(m - 2), &one, yv(m)));
+    for (int m = 0; m < M; ++m) {  // Lt z = b (z in y), w[m] = Dinv_m z[m]
+      if (m >= 1) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_L1, m), yv(m - 1), &one, yv(m)));
+      if (m >= 2) bdvec(L.off_B2 + L.bdr * m, L.off_w + vb * (m - 2), L.off_y + vb * m, 0, 0);
+      if (m + 2 < M) run(gemv(CUBLAS_OP_N, &one, g.blk(L.off_D, m), yv(m), &zero, wv(m)));
     }
     for (int m = M - 1; m >= 0; --m) {  // Ut x = z
       if (m + 1 < M) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_C1, m), xv(m + 1), &one, yv(m)));
-      if (m + 2 < M) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_C2, m), xv(m + 2), &one, yv(m)));
+      if (m + 2 < M) bdvec(L.off_C2 + L.bdr * m, L.off_x + vb * (m + 2), L.off_y + vb * m, 0, 0);
       run(gemv(CUBLAS_OP_N, &one, g.blk(L.off_D, m), yv(m), &zero, xv(m)));
     }
   } else {
     for (int m = 0; m < M; ++m) {  // Ut^H z = b (z in x)
       if (m >= 1) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_C1, m - 1), xv(m - 1), &one, yv(m)));
-      if (m >= 2) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_C2, m - 2), xv(m - 2), &one, yv(m)));
+      if (m >= 2) bdvec(L.off_C2 + L.bdr * (m - 2), L.off_x + vb * (m - 2), L.off_y + vb * m, 1, 0);
       run(gemv(CUBLAS_OP_C, &one, g.blk(L.off_D, m), yv(m), &zero, xv(m)));
     }
     for (int m = M - 1; m >= 0; --m) {  // Lt^H x = z
       if (m + 1 < M) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_L1, m + 1), xv(m + 1), &one, xv(m)));
-      if (m + 2 < M) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_L2, m + 2), xv(m + 2), &one, xv(m)));
+      if (m + 2 < M) {  // x[m] -= Dinv_m^H (B2[m+2]^T x[m+2]), with w[m] = -B2[m+2]^T x[m+2]
+        bdvec(L.off_B2 + L.bdr * (m + 2), L.off_x + vb * (m + 2), L.off_w + vb * m, 1, 1);
+        run(gemv(CUBLAS_OP_C, &one, g.blk(L.off_D, m), wv(m), &one, xv(m)));
+      }
     }
   }
   if (st != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "ringlu: gemv failed");
@@ -897,13 +945,13 @@ int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
   if (rc != EB_OK) return rc;
   for (int s = 0; s < n_shifts; ++s) {
     char* w = g.base + (int64_t)s * g.stride;
-    cudaMemsetAsync(w, 0, L.off_T, st);  // the five block arrays
+    cudaMemsetAsync(w, 0, L.off_T, st);  // the stored super-blocks and block diagonals
     cudaMemsetAsync(w + L.off_info, 0, sizeof(int) * 4, st);
     k_assemble<<<grid_for((int64_t)M * N * 9, 256), 256, 0, st>>>(
         M, N, J[s], reinterpret_cast<const double*>(w + L.off_shift),
         reinterpret_cast<cuDoubleComplex*>(w + L.off_D), reinterpret_cast<cuDoubleComplex*>(w + L.off_L1),
-        reinterpret_cast<cuDoubleComplex*>(w + L.off_L2), reinterpret_cast<cuDoubleComplex*>(w + L.off_C1),
-        reinterpret_cast<cuDoubleComplex*>(w + L.off_C2));
+        reinterpret_cast<double*>(w + L.off_B2), reinterpret_cast<cuDoubleComplex*>(w + L.off_C1),
+        reinterpret_cast<double*>(w + L.off_C2));
   }
   if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
   if (n_shifts == 1) {
@@ -1068,7 +1116,7 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
     for (int s = 0; s < n_shifts; ++s)
       k_to_rings<<<gc, 128, 0, st>>>(M, N, it == 0 ? rhs[s] : reinterpret_cast<double*>(ws(s) + L.off_r),
                                      reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_y));
-    if ((rc = ring_solve(g, h, adjoint != 0)) != EB_OK) return rc;
+    if ((rc = ring_solve(g, h, adjoint != 0, st)) != EB_OK) return rc;
     for (int s = 0; s < n_shifts; ++s) {
       double* a = reinterpret_cast<double*>(ws(s) + L.off_acc);
       k_from_rings<<<gc, 128, 0, st>>>(M, N, reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_x), x[s],
