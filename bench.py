@@ -72,11 +72,12 @@ def parse_args():
                    help="comma-separated parts to run besides the residual "
                         "(vjp, linear, second_order, resolvent, uneven)")
     p.add_argument("--uneven-instances", type=int, default=48)
-    p.add_argument("--uneven-sizes", default="65,129",
-                   help="grid point counts (n x n O-grids) the uneven instances draw from")
+    p.add_argument("--uneven-sizes", default="65,129,257,513x257",
+                   help="O-grid point counts the uneven instances draw from: n (n x n) or "
+                        "RxA (R radial x A angular points)")
     p.add_argument("--uneven-iter", type=int, default=30, help="PTC iteration cap")
-    p.add_argument("--uneven-plain", type=int, default=3,
-                   help="instances timed one at a time for the comparison")
+    p.add_argument("--uneven-plain", type=int, default=1,
+                   help="instances of each size timed one at a time for the comparison")
     p.add_argument("--workspace-gb", type=float, default=80.0,
                    help="device memory for batched factorisations")
     p.add_argument("--profile-region", choices=["none", "residual", "batched"], default="none",
@@ -856,50 +857,78 @@ def run_b200(args) -> None:
         from pyeulerale_b200 import grid as G
 
         urng = np.random.default_rng(4 + rank)
-        sizes = [int(v) for v in args.uneven_sizes.split(",")]
-        uspecs = []
+        size_names = args.uneven_sizes.split(",")
+
+        def points(name):
+            r, _, a = name.partition("x")
+            return int(r), int(a or r)
+
+        uspecs, uclass = [], []
         for _ in range(args.uneven_instances):
-            n_pts = int(urng.choice(sizes))
+            name = size_names[int(urng.integers(len(size_names)))]
             tt = int(urng.choice([4, 6, 8, 10, 12]))
-            Xg = G.naca_ogrid(n_pts, n_pts, thickness=tt / 100, chord=1.0, far_radius=20.0,
+            rp, ap = points(name)
+            Xg = G.naca_ogrid(rp, ap, thickness=tt / 100, chord=1.0, far_radius=20.0,
                               first_spacing=0.01)
             uspecs.append(InstanceSpec(Xg, float(urng.uniform(0.3, 0.6)),
                                        float(urng.uniform(-2.0, 3.0)), 1.0, (0.25, 0.0)))
+            uclass.append(name)
         uinst = InstanceSet(uspecs)
+        ws_bytes = int(args.workspace_gb * (1 << 30))
         barrier()
         t0 = time.perf_counter()
         ures = drivers.ptc_batched(uinst, rtol=1e-10, max_iter=args.uneven_iter,
-                                   workspace_bytes=int(args.workspace_gb * (1 << 30)))
-        drivers.adjoint_lift_gradients_batched(uinst, ures,
-                                               workspace_bytes=int(args.workspace_gb * (1 << 30)))
+                                   workspace_bytes=ws_bytes)
+        drivers.adjoint_lift_gradients_batched(uinst, ures, workspace_bytes=ws_bytes)
         barrier()
         t_ub = max_over_ranks(time.perf_counter() - t0)
-        n_plain = min(args.uneven_plain, len(uspecs))
-        t0 = time.perf_counter()
-        for sp in uspecs[:n_plain]:
-            sd = SpatialDiscretization(sp.vertices, mach_number=sp.mach,
-                                       angle_of_attack=sp.aoa_deg, coefficient_length=sp.chord,
-                                       coefficient_center=sp.center)
-            hist = drivers.ptc(sd, rtol=1e-10, max_iter=args.uneven_iter)
-            if np.isfinite(hist.rel_norms[-1]):
-                try:
-                    drivers.adjoint_lift_gradient(sd)
-                except _lib.EulerB200Error:
-                    pass  # a singular adjoint system, as in the batched path
-            del sd
-        barrier()
-        t_up = max_over_ranks(time.perf_counter() - t0)
         conv = sum(1 for h in ures.rel_norms if h and h[-1] <= 1e-10)
+        iters = max(len(h) for h in ures.rel_norms)
+        del ures
+        torch.cuda.empty_cache()
+        # plain: the first `uneven_plain` instances of each size one at a time through the
+        # drop-in class; the plain time of the whole set is each size's mean time x its count
+        per_size = {}
+        for name in size_names:
+            members = [k for k, c in enumerate(uclass) if c == name][:args.uneven_plain]
+            if not members:
+                continue
+            barrier()
+            t0 = time.perf_counter()
+            for k in members:
+                sp = uspecs[k]
+                sd = SpatialDiscretization(sp.vertices, mach_number=sp.mach,
+                                           angle_of_attack=sp.aoa_deg,
+                                           coefficient_length=sp.chord,
+                                           coefficient_center=sp.center)
+                hist = drivers.ptc(sd, rtol=1e-10, max_iter=args.uneven_iter)
+                if np.isfinite(hist.rel_norms[-1]):
+                    try:
+                        drivers.adjoint_lift_gradient(sd)
+                    except _lib.EulerB200Error:
+                        pass  # a singular adjoint system, as in the batched path
+                del sd
+                torch.cuda.empty_cache()
+            barrier()
+            dt = max_over_ranks(time.perf_counter() - t0)
+            per_size[name] = {"count": uclass.count(name), "timed": len(members),
+                              "seconds_per_instance": dt / len(members)}
+        t_up = sum(v["count"] * v["seconds_per_instance"] for v in per_size.values())
+        n_set = sum(v["count"] for v in per_size.values())
         uneven = {"value": world * len(uspecs) / t_ub,
                   "unit": "instances/s (PTC to 1e-10 + adjoint lift gradient)",
-                  "workload": f"{len(uspecs)} NACA-00tt O-grids of sizes {sizes} (tt in 4..12, "
-                              "Ma in [0.3, 0.6], alpha in [-2, 3] deg), per GPU",
-                  "seconds": t_ub, "converged": conv,
-                  "iterations_max": max(len(h) for h in ures.rel_norms),
-                  "plain": {"value": world * n_plain / t_up, "instances": n_plain,
-                            "seconds": t_up},
-                  "batched_vs_plain": (len(uspecs) / t_ub) / (n_plain / t_up)}
-        del ures, uinst
+                  "workload": f"{len(uspecs)} NACA-00tt O-grids drawn from the sizes "
+                              f"{size_names} (tt in 4..12, Ma in [0.3, 0.6], alpha in [-2, 3] "
+                              "deg), per GPU",
+                  "sizes": [int(s) if s.isdigit() else s for s in size_names],
+                  "counts": {s: uclass.count(s) for s in size_names},
+                  "seconds": t_ub, "converged": conv, "iterations_max": iters,
+                  "plain": {"value": world * n_set / t_up, "per_size": per_size,
+                            "seconds_estimated": t_up,
+                            "method": "drop-in class, one instance at a time (PTC + adjoint); "
+                                      "the set's plain time = per-size time x count"},
+                  "batched_vs_plain": (len(uspecs) / t_ub) / (n_set / t_up)}
+        del uinst
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -81,3 +81,39 @@ def test_ptc_and_adjoint_batched_match_single(cuda):
         assert rel_err(states[k], s.states.real) <= 1e-9, k
         ref = drivers.adjoint_lift_gradient(s)
         assert rel_err(grads[k], ref) <= 1e-8, (k, rel_err(grads[k], ref))
+
+
+def test_ptc_batched_large_grids_match_single(cuda):
+    """The two largest grid sizes of the uneven workload, a 257x257 and a 513x257 O-grid
+    (12.9 GB and 25.8 GB of ring-LU factors each), through the batched PTC and adjoint: the same
+    histories, steady states and adjoint lift gradients as the drop-in one instance at a time."""
+    from pyeulerale_b200 import SpatialDiscretization, drivers
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    specs = [InstanceSpec(G.naca_ogrid(257, 257, 0.12, 1.0, 20.0, 0.01), 0.5, 1.25, 1.0,
+                          (0.25, 0.0)),
+             InstanceSpec(G.naca_ogrid(513, 257, 0.08, 1.0, 20.0, 0.01), 0.4, 1.0, 1.0,
+                          (0.25, 0.0))]
+    inst = InstanceSet(specs)
+    res = drivers.ptc_batched(inst, rtol=1e-10, max_iter=30, workspace_bytes=28 << 30)
+    grads = drivers.adjoint_lift_gradients_batched(inst, res, workspace_bytes=28 << 30)
+    states = inst.unpack_cells(res.states.cpu().numpy())
+    batched = res.rel_norms
+    del res
+    cuda.cuda.empty_cache()
+    for k, sp in enumerate(specs):
+        s = SpatialDiscretization(sp.vertices, mach_number=sp.mach, angle_of_attack=sp.aoa_deg,
+                                  coefficient_length=sp.chord, coefficient_center=sp.center)
+        hist = drivers.ptc(s, rtol=1e-10, max_iter=30)
+        assert batched[k][-1] <= 1e-10 and hist.rel_norms[-1] <= 1e-10, (k, batched[k],
+                                                                          hist.rel_norms)
+        assert abs(len(batched[k]) - hist.iterations) <= 1, (k, batched[k], hist.rel_norms)
+        early = [i for i, r in enumerate(hist.rel_norms) if r > 1e-7 and i < len(batched[k])]
+        assert np.allclose([batched[k][i] for i in early], [hist.rel_norms[i] for i in early],
+                           rtol=1e-6), k
+        assert rel_err(states[k], s.states.real) <= 1e-9, k
+        ref = drivers.adjoint_lift_gradient(s)
+        assert rel_err(grads[k], ref) <= 1e-8, (k, rel_err(grads[k], ref))
+        del s
+        cuda.cuda.empty_cache()
