@@ -29,6 +29,7 @@
 // does.
 
 #include "common.cuh"
+#include "tile_faces.cuh"
 
 namespace eb {
 
@@ -57,153 +58,9 @@ struct TileSmem {
 __device__ __forceinline__ int sidx(int r, int c) { return (c + 2) * kSR + (r + 2); }
 __device__ __forceinline__ int vidx(int r, int c) { return c * kVR + r; }
 
-// a * b + c: one fused multiply-add for plain doubles, the dual product and sum otherwise.
-template <class A, class B, class C>
-__device__ __forceinline__ promote_t<A, promote_t<B, C>> fmad(const A& a, const B& b,
-                                                             const C& c) {
-  if constexpr (std::is_same<A, double>::value && std::is_same<B, double>::value &&
-                std::is_same<C, double>::value)
-    return fma(a, b, c);
-  else
-    return a * b + c;
-}
-
-template <class T>
-struct St {  // a state with its derived quantities
-  T rho, j1, j2, e, p, ir, cs;
-};
-
-template <class T>
-__device__ __forceinline__ St<T> derive(const T& rho, const T& j1, const T& j2, const T& e) {
-  St<T> s;
-  s.rho = rho;
-  s.j1 = j1;
-  s.j2 = j2;
-  s.e = e;
-  s.ir = 1.0 / rho;
-  s.p = kGm1 * (e - (j1 * j1 + j2 * j2) * s.ir * 0.5);
-  s.cs = sqrt_(kGamma * s.p * s.ir);
-  return s;
-}
-
 template <class T>
 __device__ __forceinline__ St<T> staged(const TileSmem<T>& S, int i) {
   return St<T>{S.rho[i], S.j1[i], S.j2[i], S.e[i], S.p[i], S.ir[i], S.cs[i]};
-}
-
-template <class T>
-__device__ __forceinline__ T sensor(const T& pa, const T& pb, const T& pc) {
-  return abs_c(pa - 2.0 * pb + pc) / (pa + 2.0 * pb + pc);
-}
-
-// max_c(0, c) (f90:111-120 with x = 0): 0 only if 0 > Re c + 1e-8.
-template <class T>
-__device__ __forceinline__ T max_c0(const T& c) {
-  return (0.0 > value(c) + 1e-8) ? lift<T>(0.0) : c;
-}
-
-// Wall ghost (make_wall_ghost_state, f90:231-240) of state s for face normal n, grid velocity g.
-template <class T>
-__device__ __forceinline__ St<T> wall_ghost_st(const St<T>& s, const T& nx, const T& nz,
-                                               const T& gx, const T& gz) {
-  const T proj = nx * (s.j1 - gx * s.rho) + nz * (s.j2 - gz * s.rho);
-  const T nn = nx * nx + nz * nz;
-  return derive<T>(s.rho, s.j1 - 2.0 * nx * proj / nn, s.j2 - 2.0 * nz * proj / nn, s.e);
-}
-
-// Far-field ghost (make_farfield_ghost_state, f90:269-274): 2 U_inf - U.
-template <class T>
-__device__ __forceinline__ St<T> farfield_ghost_st(const St<T>& s, const T& mach,
-                                                   const Instance& in) {
-  const T speed = mach * sqrt_(kGamma);
-  const T f1 = speed * in.cos_aoa, f2 = speed * in.sin_aoa;
-  const T fe = 1.0 / kGm1 + speed * speed / 2.0;
-  return derive<T>(2.0 - s.rho, 2.0 * f1 - s.j1, 2.0 * f2 - s.j2, 2.0 * fe - s.e);
-}
-
-template <class T>
-struct Flux {
-  T f[4];
-};
-
-// Central part + ALE term of make_face_flux (f90:197, 219) for l, r through normal (nx, nz)
-// with grid-velocity flux vn = g.n.
-template <class T>
-__device__ __forceinline__ Flux<T> central(const St<T>& l, const St<T>& r, const T& nx,
-                                           const T& nz, const T& vn) {
-  const T vl = (nx * l.j1 + nz * l.j2) * l.ir;
-  const T vr = (nx * r.j1 + nz * r.j2) * r.ir;
-  Flux<T> F;
-  F.f[0] = (l.rho * vl + r.rho * vr) / 2.0 - (l.rho + r.rho) / 2.0 * vn;
-  F.f[1] = ((l.j1 * vl + nx * l.p) + (r.j1 * vr + nx * r.p)) / 2.0 - (l.j1 + r.j1) / 2.0 * vn;
-  F.f[2] = ((l.j2 * vl + nz * l.p) + (r.j2 * vr + nz * r.p)) / 2.0 - (l.j2 + r.j2) / 2.0 * vn;
-  F.f[3] = ((l.e + l.p) * vl + (r.e + r.p) * vr) / 2.0 - (l.e + r.e) / 2.0 * vn;
-  return F;
-}
-
-// make_face_flux with JST dissipation (f90:189-220); s1, s2 are the sensors centred on l and r.
-template <class T>
-__device__ __forceinline__ Flux<T> jst(const St<T>& ll, const St<T>& l, const St<T>& r,
-                                       const St<T>& rr, const T& nx, const T& nz, const T& len,
-                                       const T& vn, const T& s1, const T& s2,
-                                       const Instance& in) {
-  const T vl = (nx * l.j1 + nz * l.j2) * l.ir;
-  const T vr = (nx * r.j1 + nz * r.j2) * r.ir;
-  const T lam = max_c(abs_c(vl) + l.cs * len, abs_c(vr) + r.cs * len);
-  const T coef2 = in.k2 * max_c(s1, s2) * lam;
-  const T coef4 = max_c0(in.k4 * lam - in.c4 * coef2);
-  Flux<T> F;
-  const T lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
-  const T llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
-  const T fl[4] = {l.rho * vl, l.j1 * vl + nx * l.p, l.j2 * vl + nz * l.p, (l.e + l.p) * vl};
-  const T fr[4] = {r.rho * vr, r.j1 * vr + nx * r.p, r.j2 * vr + nz * r.p, (r.e + r.p) * vr};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    T c = (fl[k] + fr[k]) / 2.0;
-    c = c - (coef2 * (rv[k] - lv[k]) - coef4 * (rrv[k] - 3.0 * rv[k] + 3.0 * lv[k] - llv[k]));
-    F.f[k] = c - (lv[k] + rv[k]) / 2.0 * vn;
-  }
-  return F;
-}
-
-// Both orientations of one JST face: F = make_face_flux(ll, l, r, rr, n) for the cell l and
-// F' = make_face_flux(rr, r, l, ll, -n) for the cell r (f90:189-220). Mathematically F' shares
-// F's central and ALE parts and its first and third differences, all negated; the orientations
-// differ only in the asymmetric max_c decisions (spectral radius and sensor), which are taken per
-// orientation as the reference takes them. The shared parts are formed once: the central flux
-// minus the grid-velocity flux as (F(l) + F(r)) . n / 2 - (l + r) vn / 2 with the face-relative
-// normal velocities vl - vn and vr - vn, and the third difference in F's orientation.
-template <class T>
-__device__ __forceinline__ void jst_pair(const St<T>& ll, const St<T>& l, const St<T>& r,
-                                         const St<T>& rr, const T& nx, const T& nz,
-                                         const T& len, const T& vn, const T& sl, const T& sr,
-                                         const Instance& in, Flux<T>& F, Flux<T>& Fp) {
-  const T vl = (nx * l.j1 + nz * l.j2) * l.ir;
-  const T vr = (nx * r.j1 + nz * r.j2) * r.ir;
-  // F' sees the normal velocities -vr, -vl: abs_c takes its derivative's sign from the value
-  // with zeros as positive, so at a zero velocity the two orientations' derivatives differ
-  // (the values, and plain-double results, do not)
-  const T al = abs_c(vl) + l.cs * len, ar = abs_c(vr) + r.cs * len;
-  const T alp = abs_c(-vl) + l.cs * len, arp = abs_c(-vr) + r.cs * len;
-  const T lam = max_c(al, ar), lamp = max_c(arp, alp);
-  const T coef2 = in.k2 * max_c(sl, sr) * lam;
-  const T coef2p = in.k2 * max_c(sr, sl) * lamp;
-  const T coef4 = max_c0(in.k4 * lam - in.c4 * coef2);
-  const T coef4p = max_c0(in.k4 * lamp - in.c4 * coef2p);
-  const T wl = vl - vn, wr = vr - vn, ps = l.p + r.p;
-  const T ca[4] = {0.5 * fmad(l.rho, wl, r.rho * wr),
-                   0.5 * fmad(l.j1, wl, fmad(r.j1, wr, nx * ps)),
-                   0.5 * fmad(l.j2, wl, fmad(r.j2, wr, nz * ps)),
-                   0.5 * fmad(l.e, wl, fmad(r.e, wr, fmad(l.p, vl, r.p * vr)))};
-  const T lv[4] = {l.rho, l.j1, l.j2, l.e}, rv[4] = {r.rho, r.j1, r.j2, r.e};
-  const T llv[4] = {ll.rho, ll.j1, ll.j2, ll.e}, rrv[4] = {rr.rho, rr.j1, rr.j2, rr.e};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const T d1 = rv[k] - lv[k];
-    const T d3 = fmad(3.0, lv[k], fmad(-3.0, rv[k], rrv[k])) - llv[k];
-    F.f[k] = fmad(coef4, d3, fmad(-coef2, d1, ca[k]));
-    Fp.f[k] = fmad(-coef4p, d3, fmad(coef2p, d1, -ca[k]));
-  }
 }
 
 // Phases 2-4 of a tile whose states (with derived quantities) and vertices are staged in S:
