@@ -109,9 +109,15 @@ int eb_compute_forces(const eb_batch* b, const double* X, const double* U, doubl
 int eb_compute_odes_wrt_mach(const eb_batch* b, const double* X, const double* V,
                              const double* U, double* J, void* stream);
 /* compute_odes_wrt_states, f90:666-750. J: (4, 4, M, N, 9) per instance, 144*cell_offset.
- * Blocks the reference does not compute (slots reaching past the radial boundary) are 0. */
+ * Blocks the reference does not compute (slots reaching past the radial boundary) are 0.
+ * Tiled kernel: each face evaluated once for both cells, per seeded stencil state. */
 int eb_compute_odes_wrt_states(const eb_batch* b, const double* X, const double* V,
                                const double* U, double* J, void* stream);
+/* The same Jacobian by the plain one-thread-per-cell kernel (each slot's block from that cell's
+ * own face evaluations, as the reference's per-cell complex step); a baseline for the tiled
+ * kernel. */
+int eb_compute_odes_wrt_states_untiled(const eb_batch* b, const double* X, const double* V,
+                                       const double* U, double* J, void* stream);
 /* compute_odes_wrt_vertices, f90:933-993. J: (4, 2, M, N, 4) per instance, 32*cell_offset. */
 int eb_compute_odes_wrt_vertices(const eb_batch* b, const double* X, const double* V,
                                  const double* U, double* J, void* stream);

@@ -88,6 +88,7 @@ _SIGNATURES: dict[str, list] = {
     "eb_compute_forces": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_odes_wrt_mach": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_odes_wrt_states": ["b", "p", "p", "p", "p", "s"],
+    "eb_compute_odes_wrt_states_untiled": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_odes_wrt_vertices": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_odes_wrt_velocities": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_forces_wrt_states": ["b", "p", "p", "p", "s"],

@@ -30,7 +30,8 @@ NVCC_FLAGS = [
 # primitives (abs_c, max_c) are decided by exact ties and cancellations at degenerate states (an
 # exact free stream), and only uncontracted evaluation keeps equal inputs bitwise equal across
 # the differently inlined call sites. The residual itself is continuous there and keeps FMA.
-PER_FILE_FLAGS = {"jacobians.cu": ["-fmad=false"], "second_order.cu": ["-fmad=false"]}
+PER_FILE_FLAGS = {"jacobians.cu": ["-fmad=false"], "second_order.cu": ["-fmad=false"],
+                  "jac_tiled.cu": ["-fmad=false"]}
 # cuBLAS serves the dense super-block products (strided-batched GEMM / GEMV) of the ring-block LU.
 LINK_FLAGS = ["-L/usr/local/cuda/lib64", "-lcublas",
               "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]

@@ -103,6 +103,63 @@ def test_tangent_at_exact_free_stream(cuda, oracle, golden_grids, name):
     check_tangent(name + "_free_stream", Gpu(cuda, case), oracle_eval(oracle, case))
 
 
+@pytest.mark.parametrize("entry", ["eb_compute_odes_wrt_states",
+                                   "eb_compute_odes_wrt_states_untiled"])
+@pytest.mark.parametrize("name", ["naca0004_33_sym", "naca0012_33", "ref8x9"])
+def test_states_jacobian_at_exact_free_stream(cuda, oracle, golden_grids, name, entry):
+    """At an exact free stream sensor numerators cancel to exactly zero and abs_c takes its
+    derivative sign from a zero: every entry of d(odes)/d(states) matches the complex-step
+    Jacobian there (a branch taken differently changes an entry by O(1), not by rounding)."""
+    from pyeulerale_b200 import grid as G
+
+    case = make_case(name, golden_grids)
+    M, N = case["U"].shape[1], case["U"].shape[2]
+    case["U"] = G.perturbed_states(M, N, case["mach"], case["aoa"], 0.0,
+                                   np.random.default_rng(0))
+    gpu = Gpu(cuda, case)
+    J = gpu.empty(144 * M * N)
+    gpu.call(entry, gpu.X, gpu.V, gpu.U, J)
+    got = gpu.host(J, (4, 4, M, N, 9))
+    ref = oracle_eval(oracle, case)["J_u"]
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) <= TOL_J * scale, (name, entry)
+
+
+def test_states_jacobian_tiled_uneven_batch(cuda, oracle, golden_grids):
+    """The tiled states Jacobian over one launch of instances of uneven sizes (partial tiles in
+    both directions, grids down to M = 4, N = 5) and different flows, moving grids: each
+    instance's blocks match the oracle's complex-step Jacobian and the per-cell kernel's."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    rng = np.random.default_rng(19)
+    grids = [G.naca_ogrid(33, 41, 0.12, 1.0, 20.0, 0.01), G.naca_ogrid(20, 13, 0.06, 2.0, 30.0, 0.05),
+             G.naca_ogrid(5, 6, 0.12, 1.0, 10.0, 0.05), G.naca_ogrid(70, 37, 0.10, 1.0, 15.0, 0.02),
+             golden_grids["naca0004_129x129"]]
+    flows = [(0.5, 1.25), (0.3, -2.0), (0.45, 0.5), (0.6, 3.0), (0.5, 0.0)]
+    specs = [InstanceSpec(X, ma, a) for X, (ma, a) in zip(grids, flows)]
+    states = [G.perturbed_states(s.M, s.N, s.mach, s.aoa_deg, 0.01, rng) for s in specs]
+    vels = [G.smooth_velocities(X, rng) for X in grids]
+    inst = InstanceSet(specs)
+    dX = cuda.from_numpy(inst.pack_vertices()).cuda()
+    dV = cuda.from_numpy(inst.pack_vertices(vels)).cuda()
+    dU = cuda.from_numpy(inst.pack_cells(states)).cuda()
+    Jt = cuda.full((144 * inst.n_cells,), np.nan, dtype=cuda.float64, device="cuda")
+    Ju = cuda.zeros(144 * inst.n_cells, dtype=cuda.float64, device="cuda")
+    inst.call("eb_compute_odes_wrt_states", dX, dV, dU, Jt)
+    inst.call("eb_compute_odes_wrt_states_untiled", dX, dV, dU, Ju)
+    got = inst.unpack_cells(Jt.cpu().numpy(), per_cell=144)
+    plain = inst.unpack_cells(Ju.cpu().numpy(), per_cell=144)
+    for k, (s, X, V, U) in enumerate(zip(specs, grids, vels, states)):
+        shape = (4, 4, s.M, s.N, 9)
+        g = np.reshape(got[k].ravel(order="F"), shape, order="F")
+        u = np.reshape(plain[k].ravel(order="F"), shape, order="F")
+        assert np.all(np.isfinite(g)), k
+        ref = oracle_eval(oracle, dict(X=X, V=V, U=U, mach=s.mach, aoa=s.aoa_deg))["J_u"]
+        assert rel_err(g, ref) <= TOL_J, (k, rel_err(g, ref))
+        assert rel_err(g, u) <= 1e-12, (k, rel_err(g, u))
+
+
 def check_tangent(name, gpu, o):
     M, N = gpu.M, gpu.N
     rng = np.random.default_rng(5)
