@@ -619,6 +619,9 @@ def run_b200(args) -> None:
         J_u = torch.empty(144 * cells, **f64)
         t_jac = per_call(lambda: inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u,
                                            stream=sp), 5)
+        t_jac_plain = per_call(lambda: inst.call("eb_compute_odes_wrt_states_untiled", dX, dV,
+                                                 dU, J_u, stream=sp), 2)
+        inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u, stream=sp)
         gen = torch.Generator(device="cuda").manual_seed(77 + rank)
         tU = torch.randn(8 * cells, generator=gen, **f64)
         tX = torch.randn(4 * inst.n_verts, generator=gen, **f64)
@@ -694,7 +697,10 @@ def run_b200(args) -> None:
         linear = {
             "jacobian_states": {"value": world * cells / t_jac, "unit": "cells/s",
                                 "achieved_gbs": BYTES_PER_CELL_JAC_STATES * cells / t_jac / 1e9,
-                                "bytes_per_cell": BYTES_PER_CELL_JAC_STATES},
+                                "bytes_per_cell": BYTES_PER_CELL_JAC_STATES,
+                                "kernel": "k_jac_states_tiled",
+                                "untiled": {"value": world * cells / t_jac_plain,
+                                            "kernel": "k_jac_states (one thread per cell)"}},
             "tangent": {"value": world * cells / t_tan, "unit": "cells/s",
                         "achieved_gbs": BYTES_PER_CELL_TANGENT * cells / t_tan / 1e9,
                         "bytes_per_cell": BYTES_PER_CELL_TANGENT,

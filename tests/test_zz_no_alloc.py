@@ -58,7 +58,7 @@ def test_noalloc_two_instances_allocates_nothing(cuda, golden_grids):
     J = cuda.zeros(144 * inst.n_cells, dtype=cuda.float64, device="cuda")
     inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J)
     sys_inst = [1, 0, 1]
-    shifts = [0.4 + 0.3j, 1.5, 1.0j]
+    shifts = [2.0 + 1.0j, 1.5, 3.0j]
     sizes = [8 * specs[i].M * specs[i].N for i in sys_inst]
     rhs = cuda.from_numpy(rng.standard_normal(sum(sizes))).cuda()
     kw = dict(sys_inst=sys_inst, host_table=inst.host_table)
