@@ -43,6 +43,8 @@ METRIC = "cell-residual evals/s; VJP/s; batched resolvent solves/s vs plain at 1
 UNIT = "cell-residual evals/s"
 BYTES_PER_CELL_RESIDUAL = 96          # U 32 + X 16 + V 16 + R 32 (FP64)
 BYTES_PER_CELL_VJP = 1152 + 256 + 256 + 32 + 4 * 64 + 64 + 2 * 32 + 8
+# matrix-free VJP set: U, X, V and complex w in; complex d_states, d_vertices, d_velocities out
+BYTES_PER_CELL_ADJOINT = 32 + 16 + 16 + 64 + 64 + 32 + 32
 BYTES_PER_CELL_JAC_STATES = 32 + 16 + 16 + 1152   # U, X, V in; nine 4x4 blocks out
 # U, X, V, complex dU, dX, dV in; complex dR out
 BYTES_PER_CELL_TANGENT = 32 + 16 + 16 + 64 + 32 + 32 + 64
@@ -560,43 +562,69 @@ def run_b200(args) -> None:
     e2e_serial = world * cells * e2e_steps / t_serial
     dX, dV, dU = pipe.bufs[0]["X"], pipe.bufs[0]["V"], pipe.bufs[0]["U"]
 
-    # VJP set on stored Jacobians (d/dU, d/dX, d/dV, d/dMa) per instance
-    vjp_rate = vjp_gbs = None
+    # VJP set (d/dU, d/dX, d/dV, d/dMa of <w, R> per instance, complex w as the reference's
+    # reverse products take): the matrix-free adjoint kernel from (U, X, V, w), all work timed;
+    # beside it the reverse products with stored Jacobians, alone and with the Jacobian builds
+    vjp = None
     if "vjp" in parts:
-        J_u = torch.empty(144 * cells, **f64)
-        J_x = torch.empty(32 * cells, **f64)
-        J_v = torch.empty(32 * cells, **f64)
-        J_m = torch.empty(4 * cells, **f64)
-        inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u, stream=sp)
-        inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, J_x, stream=sp)
-        inst.call("eb_compute_odes_wrt_velocities", dX, dV, dU, J_v, stream=sp)
-        inst.call("eb_compute_odes_wrt_mach", dX, dV, dU, J_m, stream=sp)
         w = torch.randn(8 * cells, **f64)
         gU = torch.empty(8 * cells, **f64)
         gX = torch.empty(4 * inst.n_verts, **f64)
         gV = torch.empty(4 * inst.n_verts, **f64)
         gM = torch.empty(2 * B, **f64)
 
-        def vjp():
+        def timed(fn, n):
+            for _ in range(args.warmup):
+                fn()
+            barrier()
+            v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            v0.record(stream)
+            for _ in range(n):
+                fn()
+            v1.record(stream)
+            barrier()
+            return max_over_ranks(v0.elapsed_time(v1) / 1e3) / n
+
+        def adjoint():
+            inst.call("eb_apply_odes_adjoint", dX, dV, dU, w, 1, gU, gX, gV, gM, stream=sp)
+
+        t_adj = timed(adjoint, max(5, args.steps // 4))
+        J_u = torch.empty(144 * cells, **f64)
+        J_x = torch.empty(32 * cells, **f64)
+        J_v = torch.empty(32 * cells, **f64)
+        J_m = torch.empty(4 * cells, **f64)
+
+        def build():
+            inst.call("eb_compute_odes_wrt_states", dX, dV, dU, J_u, stream=sp)
+            inst.call("eb_compute_odes_wrt_vertices", dX, dV, dU, J_x, stream=sp)
+            inst.call("eb_compute_odes_wrt_velocities", dX, dV, dU, J_v, stream=sp)
+            inst.call("eb_compute_odes_wrt_mach", dX, dV, dU, J_m, stream=sp)
+
+        def products():
             inst.call("eb_apply_odes_wrt_states_rev", J_u, w, gU, stream=sp)
             inst.call("eb_apply_odes_wrt_vertices_rev", J_x, w, gX, stream=sp)
             inst.call("eb_apply_odes_wrt_vertices_rev", J_v, w, gV, stream=sp)
             inst.call("eb_apply_odes_wrt_mach_rev", J_m, w, gM, stream=sp)
 
-        for _ in range(args.warmup):
-            vjp()
-        barrier()
-        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        vsteps = max(5, args.steps // 2)
-        v0.record(stream)
-        for _ in range(vsteps):
-            vjp()
-        v1.record(stream)
-        barrier()
-        t_vjp = max_over_ranks(v0.elapsed_time(v1) / 1e3)
-        vjp_rate = world * B * vsteps / t_vjp
-        vjp_gbs = BYTES_PER_CELL_VJP * cells * vsteps / t_vjp / 1e9
-        del J_u, J_x, J_v, J_m
+        t_build = timed(build, 3)
+        t_prod = timed(products, max(5, args.steps // 2))
+        vjp = {"value": world * B / t_adj,
+               "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa of <w, R> per instance, from U, X, "
+                       "V and complex w, all work timed)",
+               "kernel": "k_residual_adjoint + k_mach_adjoint (eb_apply_odes_adjoint)",
+               "achieved_gbs": BYTES_PER_CELL_ADJOINT * cells / t_adj / 1e9,
+               "bytes_per_cell": BYTES_PER_CELL_ADJOINT,
+               "cells_per_s": world * cells / t_adj,
+               "stored_blocks": {
+                   "value": world * B / t_prod,
+                   "unit": "VJP/s, reverse products with the Jacobians already built",
+                   "achieved_gbs": BYTES_PER_CELL_VJP * cells / t_prod / 1e9,
+                   "launches_per_vjp_batch": 4},
+               "stored_blocks_with_build": {
+                   "value": world * B / (t_build + t_prod),
+                   "unit": "VJP/s, Jacobian builds (states, vertices, velocities, Mach) + "
+                           "reverse products"}}
+        del J_u, J_x, J_v, J_m, gU, gX, gV, gM, w
 
     # linearisation: the 4x4-block Jacobian d(odes)/d(states) of every instance, the
     # matrix-free forward tangent (complex dU, dX, dV, dMa in one stencil pass) of every
@@ -975,12 +1003,11 @@ def run_b200(args) -> None:
                            "path": "one stream: H2D of X, V, U, eb_compute_odes, D2H of R"}},
         "gpu_launches": args.steps,
         "clocks": clk,
-        "vjp": None if vjp_rate is None else {
-            "value": vjp_rate, "unit": "VJP/s (dR/dU, dR/dX, dR/dV, dR/dMa per instance)",
-            "achieved_gbs": vjp_gbs, "launches_per_vjp_batch": 4,
+        "vjp": None if vjp is None else {
+            **vjp, "roofline_frac": vjp["achieved_gbs"] / peak,
             "cpu_reference_method": None if cpu_lin is None else cpu_lin["vjp"],
             "vs_cpu_reference_method": None if cpu_lin is None
-            else vjp_rate / cpu_lin["vjp"]["value"]},
+            else vjp["value"] / cpu_lin["vjp"]["value"]},
         "linear": linear,
         "second_order": second,
         "resolvent": res,

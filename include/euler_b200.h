@@ -169,6 +169,18 @@ int eb_apply_odes_tangent(const eb_batch* b, const double* X, const double* V, c
                           const double* dU, const double* dX, const double* dV,
                           const double* dMa, double* dR, double* R, void* stream);
 
+/* Matrix-free reverse products for the cotangent w (4, M, N): d_states = (dR/dU)^T w
+ * (4, M, N), d_vertices = (dR/dX)^T w and d_velocities = (dR/dV)^T w (2, M+1, N+1), d_mach =
+ * (dR/dMa)^T w (one per instance): what apply_odes_wrt_states_rev, apply_odes_wrt_vertices_rev
+ * and apply_odes_wrt_mach_rev (f90:604-650, 875-918, 1044-1072) give with the stored Jacobians,
+ * in one reverse pass over the faces (no Jacobian built). is_complex = 1: w and the outputs are
+ * interleaved complex (the transposes are of the real Jacobians, no conjugation); 0: real.
+ * Outputs are overwritten; any of them may be NULL (not formed). Grids must be closed
+ * O-grids (vertex column N equal to column 0). */
+int eb_apply_odes_adjoint(const eb_batch* b, const double* X, const double* V, const double* U,
+                          const double* w, int is_complex, double* d_states, double* d_vertices,
+                          double* d_velocities, double* d_mach, void* stream);
+
 /* ---- BSR form of d(odes)/d(states) --------------------------------------------------- */
 
 /* convert_odes_wrt_states, f90:765-814, for a single instance: data (4, 4, nnzb), 1-based

@@ -104,6 +104,7 @@ _SIGNATURES: dict[str, list] = {
     "eb_apply_forces_wrt_vertices_fwd": ["b", "p", "p", "p", "s"],
     "eb_apply_forces_wrt_vertices_rev": ["b", "p", "p", "p", "s"],
     "eb_apply_odes_tangent": ["b", "p", "p", "p", "p", "p", "p", "p", "p", "p", "s"],
+    "eb_apply_odes_adjoint": ["b", "p", "p", "p", "p", "i", "p", "p", "p", "p", "s"],
     "eb_convert_odes_wrt_states": ["b", "p", "p", "p", "p", "s"],
     "eb_compute_pressure_coefficients": ["b", "p", "p", "s"],
     "eb_apply_pressure_coefficients_wrt_states_fwd": ["b", "p", "p", "p", "s"],

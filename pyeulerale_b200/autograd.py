@@ -2,15 +2,15 @@
 
 ``residual(U, X, V, mach, instances)`` and ``forces(U, X, instances)`` return R(Ma, U, X, V)
 (``eb_compute_odes``) and F(U, X) (``eb_compute_forces``) as differentiable float64 tensors in the
-packed layouts of ``InstanceSet`` (reference layouts per instance, back to back). Their
-backward passes are the hand-written reverse products of the C ABI, which gather the transpose
-stencil per output cell (no atomics): d/dU, d/dX, d/dV and d/dMa of R
-(``eb_apply_odes_wrt_*_rev``, core.py:375-510 and 294-346 of the reference), d/dU and d/dX of F
-(``eb_apply_forces_wrt_*_rev``, core.py:637-716). The Jacobian blocks a backward pass needs are
-rebuilt inside it from the saved inputs and released afterwards (nothing is stored between
-the forward and the backward pass but U, X and V), and only the blocks of the inputs that
-require gradients are built. ``mach`` is a CPU float64 tensor with one Mach number per
-instance; its gradient is the per-instance d<w, R>/dMa.
+packed layouts of ``InstanceSet`` (reference layouts per instance, back to back). The
+residual's backward pass is the matrix-free adjoint kernel (``eb_apply_odes_adjoint``): d/dU,
+d/dX, d/dV and d/dMa of <w, R> in one reverse pass over the faces that recomputes the face
+quantities from the saved U, X, V and gathers every output element without atomics (the
+reference's counterparts are the stored-Jacobian reverse products, core.py:375-510 and
+294-346). The forces' backward pass uses the wall-force Jacobians and their reverse products
+(``eb_apply_forces_wrt_*_rev``, core.py:637-716), rebuilt inside it from the saved inputs.
+Only the gradients of inputs that require them are formed. ``mach`` is a CPU float64 tensor
+with one Mach number per instance; its gradient is the per-instance d<w, R>/dMa.
 """
 
 from __future__ import annotations
@@ -51,29 +51,14 @@ class _Residual(torch.autograd.Function):
         U, X, V = ctx.saved_tensors
         inst: InstanceSet = ctx.inst
         dev, nc, nv, st = U.device, inst.n_cells, inst.n_verts, _stream()
-        w = _complex(gR.contiguous())
-        grads = [None, None, None, None, None]
-        if ctx.needs_input_grad[0]:
-            J = _empty(144 * nc, dev)
-            inst.call("eb_compute_odes_wrt_states", X, V, U, J, stream=st)
-            y = _empty(8 * nc, dev)
-            inst.call("eb_apply_odes_wrt_states_rev", J, w, y, stream=st)
-            grads[0] = y[0::2].contiguous()
-            del J
-        for k, builder in ((1, "eb_compute_odes_wrt_vertices"), (2, "eb_compute_odes_wrt_velocities")):
-            if ctx.needs_input_grad[k]:
-                J = _empty(32 * nc, dev)
-                inst.call(builder, X, V, U, J, stream=st)
-                y = _empty(4 * nv, dev)
-                inst.call("eb_apply_odes_wrt_vertices_rev", J, w, y, stream=st)
-                grads[k] = y[0::2].contiguous()
-                del J
-        if ctx.needs_input_grad[3]:
-            J = _empty(4 * nc, dev)
-            inst.call("eb_compute_odes_wrt_mach", X, V, U, J, stream=st)
-            y = _empty(2 * len(inst), dev)
-            inst.call("eb_apply_odes_wrt_mach_rev", J, w, y, stream=st)
-            grads[3] = y[0::2].to("cpu")
+        need = ctx.needs_input_grad
+        out = [_empty(n, dev) if need[k] else None
+               for k, n in enumerate((4 * nc, 2 * nv, 2 * nv, len(inst)))]
+        if any(o is not None for o in out):
+            inst.call("eb_apply_odes_adjoint", X, V, U, gR.contiguous(), 0, *out, stream=st)
+        grads = [*out, None]
+        if grads[3] is not None:
+            grads[3] = grads[3].to("cpu")
         return tuple(grads)
 
 

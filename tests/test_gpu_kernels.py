@@ -160,6 +160,106 @@ def test_states_jacobian_tiled_uneven_batch(cuda, oracle, golden_grids):
         assert rel_err(g, u) <= 1e-12, (k, rel_err(g, u))
 
 
+def run_adjoint(gpu, w, is_complex=True):
+    """d_states, d_vertices, d_velocities, d_mach of the matrix-free adjoint (host arrays)."""
+    M, N = gpu.M, gpu.N
+    f = 2 if is_complex else 1
+    gU, gX, gV, gM = (gpu.empty(f * n) for n in (4 * M * N, 2 * (M + 1) * (N + 1),
+                                                 2 * (M + 1) * (N + 1), 1))
+    gpu.call("eb_apply_odes_adjoint", gpu.X, gpu.V, gpu.U, gpu.dev(w), 1 if is_complex else 0,
+             gU, gX, gV, gM)
+    sv = (2, M + 1, N + 1)
+    return (gpu.host(gU, (4, M, N), is_complex), gpu.host(gX, sv, is_complex),
+            gpu.host(gV, sv, is_complex), gpu.host(gM, (1,), is_complex))
+
+
+def test_adjoint_kernel_matches_reverse_products(evaluated, oracle):
+    """The matrix-free adjoint equals the reverse products with the oracle's complex-step
+    Jacobians (apply_odes_wrt_states_rev, _vertices_rev with J_x and J_v, _mach_rev)."""
+    name, case, gpu, g, o = evaluated
+    M, N = gpu.M, gpu.N
+    w = crandn(np.random.default_rng(11), (4, M, N))
+    got = run_adjoint(gpu, w)
+    for (fn, key, shape), y in zip([("apply_odes_wrt_states_rev", "J_u", (4, M, N)),
+                                    ("apply_odes_wrt_vertices_rev", "J_x", (2, M + 1, N + 1)),
+                                    ("apply_odes_wrt_vertices_rev", "J_v", (2, M + 1, N + 1)),
+                                    ("apply_odes_wrt_mach_rev", "J_ma", (1,))], got):
+        ref = np.asfortranarray(np.zeros(shape, dtype=complex))
+        getattr(oracle, fn)(o[key], w, ref)
+        assert rel_err(y, ref) <= TOL_J, (name, key, rel_err(y, ref))
+
+
+def test_adjoint_kernel_dot_product_with_tangent(evaluated):
+    """<w, dR(d)> from the tiled tangent equals <dR^T w, d> from the adjoint, for complex w and
+    complex directions on U, X, V and Ma together (bilinear, no conjugation)."""
+    name, case, gpu, g, o = evaluated
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(13)
+    w = crandn(rng, (4, M, N))
+    d = [crandn(rng, (4, M, N)), crandn(rng, (2, M + 1, N + 1)), crandn(rng, (2, M + 1, N + 1)),
+         np.array([0.4 + 0.1j])]
+    dR = gpu.empty(8 * M * N)
+    gpu.call("eb_apply_odes_tangent", gpu.X, gpu.V, gpu.U, *[gpu.dev(a) for a in d], dR, None)
+    lhs = np.sum(w * gpu.host(dR, (4, M, N), complex_=True))
+    rhs = sum(np.sum(a * b) for a, b in zip(run_adjoint(gpu, w), d))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1.0), (name, lhs, rhs)
+
+
+def test_adjoint_kernel_real_cotangent(evaluated):
+    """A real cotangent (is_complex = 0) gives the real parts of the complex products."""
+    name, case, gpu, g, o = evaluated
+    M, N = gpu.M, gpu.N
+    w = crandn(np.random.default_rng(17), (4, M, N))
+    full = run_adjoint(gpu, w)
+    real = run_adjoint(gpu, np.asfortranarray(w.real), is_complex=False)
+    for a, b in zip(real, full):
+        np.testing.assert_array_equal(a, b.real)
+
+
+def test_adjoint_kernel_uneven_batch(cuda, oracle, golden_grids):
+    """One launch over uneven instances (partial tiles, M = 4 / N = 5, moving grids): each
+    instance's reverse products equal the oracle's with its complex-step Jacobians."""
+    from pyeulerale_b200 import grid as G
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    rng = np.random.default_rng(29)
+    grids = [G.naca_ogrid(33, 41, 0.12, 1.0, 20.0, 0.01), G.naca_ogrid(5, 6, 0.12, 1.0, 10.0, 0.05),
+             G.naca_ogrid(70, 37, 0.10, 1.0, 15.0, 0.02), G.naca_ogrid(20, 13, 0.06, 2.0, 30.0, 0.05)]
+    flows = [(0.5, 1.25), (0.45, 0.5), (0.6, 3.0), (0.3, -2.0)]
+    specs = [InstanceSpec(X, ma, a) for X, (ma, a) in zip(grids, flows)]
+    states = [G.perturbed_states(s.M, s.N, s.mach, s.aoa_deg, 0.01, rng) for s in specs]
+    vels = [G.smooth_velocities(X, rng) for X in grids]
+    ws = [crandn(rng, (4, s.M, s.N)) for s in specs]
+    inst = InstanceSet(specs)
+    dX = cuda.from_numpy(inst.pack_vertices()).cuda()
+    dV = cuda.from_numpy(inst.pack_vertices(vels)).cuda()
+    dU = cuda.from_numpy(inst.pack_cells(states)).cuda()
+    dw = cuda.from_numpy(inst.pack_cells(ws).view(np.float64)).cuda()
+    f64 = dict(dtype=cuda.float64, device="cuda")
+    gU = cuda.full((8 * inst.n_cells,), np.nan, **f64)
+    gX = cuda.full((4 * inst.n_verts,), np.nan, **f64)
+    gV = cuda.full((4 * inst.n_verts,), np.nan, **f64)
+    gM = cuda.full((2 * len(specs),), np.nan, **f64)
+    inst.call("eb_apply_odes_adjoint", dX, dV, dU, dw, 1, gU, gX, gV, gM)
+    hU, hX, hV, hM = (a.cpu().numpy().view(np.complex128) for a in (gU, gX, gV, gM))
+    for k, (s, X, V, U, w) in enumerate(zip(specs, grids, vels, states, ws)):
+        o = oracle_eval(oracle, dict(X=X, V=V, U=U, mach=s.mach, aoa=s.aoa_deg))
+        M, N = s.M, s.N
+        c0, v0 = inst.cell_offsets[k], inst.vert_offsets[k]
+        nv = (M + 1) * (N + 1)
+        got = [np.reshape(hU[4 * c0:4 * (c0 + M * N)], (4, M, N), order="F"),
+               np.reshape(hX[2 * v0:2 * (v0 + nv)], (2, M + 1, N + 1), order="F"),
+               np.reshape(hV[2 * v0:2 * (v0 + nv)], (2, M + 1, N + 1), order="F"),
+               hM[k:k + 1]]
+        for (fn, key, shape), y in zip([("apply_odes_wrt_states_rev", "J_u", (4, M, N)),
+                                        ("apply_odes_wrt_vertices_rev", "J_x", (2, M + 1, N + 1)),
+                                        ("apply_odes_wrt_vertices_rev", "J_v", (2, M + 1, N + 1)),
+                                        ("apply_odes_wrt_mach_rev", "J_ma", (1,))], got):
+            ref = np.asfortranarray(np.zeros(shape, dtype=complex))
+            getattr(oracle, fn)(o[key], np.asfortranarray(w), ref)
+            assert rel_err(y, ref) <= TOL_J, (k, key, rel_err(y, ref))
+
+
 def check_tangent(name, gpu, o):
     M, N = gpu.M, gpu.N
     rng = np.random.default_rng(5)
