@@ -516,6 +516,9 @@ def run_b200(args) -> None:
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
         if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
+    peak_source = ("MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else
+                   "no MEASURED_PEAKS.json on this machine: the pool's earlier measured copy "
+                   "bandwidth 6650 GB/s (of fallback)")
     traffic_cell = read_traffic()
 
     # end to end through the C ABI with host buffers: every step copies its inputs (X, V, U)
@@ -993,7 +996,7 @@ def run_b200(args) -> None:
                      "per cell of the same kernel, scaled to this launch's cells), not "
                      "measured in this run",
                      "algorithmic_bytes_per_launch": BYTES_PER_CELL_RESIDUAL * cells,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "peak_source": peak_source},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": e2e_steps,

@@ -297,6 +297,27 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
                          int64_t workspace_stride, const double* const* rhs, double* const* x,
                          double tol, int max_refine, double* rel_residuals, void* stream);
 
+/* ---- PTC/SER steady state ---------------------------------------------------------------- */
+
+/* Device workspace (bytes) of eb_ptc_run for an M x N instance and at most max_steps steps: the
+ * ring-LU factors of one shift, two complex vectors, the control block and the history. */
+int64_t eb_ptc_workspace_bytes(int M, int N, int max_steps);
+
+/* The pseudo-transient continuation with switched evolution relaxation of the reference's
+ * example driver (examples/response/run.py:84-123) for one instance, on the device: each step
+ * evaluates R(U) into R, rel = max|R| / max|R_0| (R_0: the residual of U on entry), records rel,
+ * stops if rel <= rtol or rel is not finite, else builds the states Jacobian into J and updates
+ * U += Re((J - shift I)^-1 (-R)) with shift = (ser / rel)^-1 (ring-block LU, one refinement
+ * step). At most max_steps steps. The first step runs eagerly, the others replay one captured
+ * CUDA graph; the control values stay on the device and the host reads one stop flag per step.
+ * On return U is the final state, R and J its residual and Jacobian (of the state before the
+ * last update when max_steps ends the loop), history (HOST, 2 max_steps) the pairs (max|R|,
+ * rel) of the steps and *n_steps their count. EB_ERR_NAN if rel became non-finite or a ring block was singular;
+ * reaching max_steps is not an error (as in the example driver). Synchronises `stream`. */
+int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, double* R,
+               double* J, double ser, double rtol, int max_steps, void* workspace,
+               int64_t workspace_bytes, double* history, int* n_steps, void* stream);
+
 /* ---- pressure coefficients --------------------------------------------------------------- */
 /* cp (real, one per cell, packed like the cells) of the states U: ((gamma-1)(E - |j|^2/2/rho) -
  * 1) / q with q = gamma Ma^2 / 2 per instance (compute_pressure_coefficients,

@@ -13,6 +13,11 @@
 // same face terms in the same order, -(((F_b + F_f) + F_i) + F_o) / area (f90:395-400). The
 // sensors (f90:208-211) are recomputed from the staged pressures with the seeded one dual.
 //
+// The seeded state's four conserved variables are differentiated kW at a time: with kW = 4 one
+// pass over the faces (255 registers, one CTA per SM), with kW = 2 two passes that repeat the
+// value arithmetic but hold half the derivative state (two CTAs per SM). Each derivative
+// component is formed by the same operations either way, so both give identical blocks.
+//
 // Layout of a CTA: a tile of kTM = 32 radial x kTN = 7 angular cells on 256 threads; thread
 // (r, c), c < 8, evaluates the angular face between cells (r, c - 1) and (r, c), so the tile's
 // 32 x 8 angular faces take one evaluation per thread, and thread (r, c < 7) the radial face
@@ -41,30 +46,33 @@ constexpr int kStaged = kSR * kSC;
 constexpr int kVR = kTM + 1, kVC = kTN + 1;
 constexpr int kVerts = kVR * kVC;
 
-using D4 = Dual<double, 4>;
+// The four conserved variables of the seeded state are differentiated kW at a time (kGroups
+// passes over the faces): two-component duals halve the live derivative state, which lets two
+// CTAs share an SM, for a second evaluation of the values.
+constexpr int kW = 2;
+constexpr int kGroups = 4 / kW;
+constexpr int kB = 4 * kW;  // the part of a 4 x 4 block one pass forms: columns G kW .. G kW + kW - 1
+using D4 = Dual<double, kW>;
 
 struct Smem {
   double rho[kStaged], j1[kStaged], j2[kStaged], e[kStaged];
   double p[kStaged], ir[kStaged], cs[kStaged];
   double x[kVerts], z[kVerts], vx[kVerts], vz[kVerts];
-  double nb[16][kTN][kTM];  // derivative block of the neighbour face's flux, per cell
+  double nb[kB][kTN][kTM];  // derivative (block part) of the neighbour face's flux, per cell
 };
 
 __device__ __forceinline__ int sidx(int r, int c) { return (c + 2) * kSR + (r + 2); }
 __device__ __forceinline__ int vidx(int r, int c) { return c * kVR + r; }
 
-// Staged state i, seeded (the four conserved variables as the dual components, derived
-// quantities in dual arithmetic) or plain.
-template <bool Seed>
+// Staged state i, seeded (conserved variables G kW .. G kW + kW - 1 as the dual components,
+// derived quantities in dual arithmetic) or plain.
+template <bool Seed, int G>
 __device__ __forceinline__ auto state(const Smem& S, int i) {
   if constexpr (Seed) {
-    D4 rho = lift<D4>(S.rho[i]), j1 = lift<D4>(S.j1[i]), j2 = lift<D4>(S.j2[i]),
-       e = lift<D4>(S.e[i]);
-    rho.d[0] = 1.0;
-    j1.d[1] = 1.0;
-    j2.d[2] = 1.0;
-    e.d[3] = 1.0;
-    return derive<D4>(rho, j1, j2, e);
+    D4 u[4] = {lift<D4>(S.rho[i]), lift<D4>(S.j1[i]), lift<D4>(S.j2[i]), lift<D4>(S.e[i])};
+#pragma unroll
+    for (int j = 0; j < kW; ++j) u[G * kW + j].d[j] = 1.0;
+    return derive<D4>(u[0], u[1], u[2], u[3]);
   } else {
     return St<double>{S.rho[i], S.j1[i], S.j2[i], S.e[i], S.p[i], S.ir[i], S.cs[i]};
   }
@@ -83,13 +91,13 @@ __device__ __forceinline__ Flux<D4> lift_flux(const Flux<T>& f) {
 // Angular face between cells (fr, fc) [l] and (fr, fc - 1) [r]: the stencil line is
 // (fr, fc + 1), (fr, fc), (fr, fc - 1), (fr, fc - 2); position K is seeded. F is the flux of
 // cell l through its face b, Fp that of cell r through its face f.
-template <int K>
+template <int K, int G>
 __device__ __forceinline__ void angular_pair(const Smem& S, const Instance& in, int fr, int fc,
                                              Flux<D4>& F, Flux<D4>& Fp) {
-  const auto ll = state<K == 0>(S, sidx(fr, fc + 1));
-  const auto l = state<K == 1>(S, sidx(fr, fc));
-  const auto r = state<K == 2>(S, sidx(fr, fc - 1));
-  const auto rr = state<K == 3>(S, sidx(fr, fc - 2));
+  const auto ll = state<K == 0, G>(S, sidx(fr, fc + 1));
+  const auto l = state<K == 1, G>(S, sidx(fr, fc));
+  const auto r = state<K == 2, G>(S, sidx(fr, fc - 1));
+  const auto rr = state<K == 3, G>(S, sidx(fr, fc - 2));
   const double nbx = S.z[vidx(fr, fc)] - S.z[vidx(fr + 1, fc)];
   const double nbz = S.x[vidx(fr + 1, fc)] - S.x[vidx(fr, fc)];
   const double vn = (S.vx[vidx(fr + 1, fc)] + S.vx[vidx(fr, fc)]) / 2.0 * nbx +
@@ -105,7 +113,7 @@ __device__ __forceinline__ void angular_pair(const Smem& S, const Instance& in, 
 // stencil line is (fr + 1), (fr), (fr - 1), (fr - 2) in column fc; position K is seeded. F is
 // the flux of cell l through its face i, Fp that of cell r through its face o; the boundary
 // rows follow make_ode's five cases (f90:401-436).
-template <int K>
+template <int K, int G>
 __device__ __forceinline__ void radial_pair(const Smem& S, const Instance& in, int fm, int fr,
                                             int fc, Flux<D4>& F, Flux<D4>& Fp) {
   const int M = in.M;
@@ -118,19 +126,19 @@ __device__ __forceinline__ void radial_pair(const Smem& S, const Instance& in, i
 #pragma unroll
   for (int k = 0; k < 4; ++k) F.f[k] = Fp.f[k] = lift<D4>(0.0);
   if (fm == 0) {  // wall face of cell 0 (flag 1): central flux with the wall ghost
-    const auto C = state<K == 1>(S, sidx(fr, fc));
+    const auto C = state<K == 1, G>(S, sidx(fr, fc));
     F = lift_flux(central(C, wall_ghost_st(C, nix, niz, gx, gz), nix, niz, vn));
     return;
   }
   if (fm == M) {  // far-field face of cell M-1 (flag 5): central flux with the ghost
-    const auto C = state<K == 2>(S, sidx(fr - 1, fc));
+    const auto C = state<K == 2, G>(S, sidx(fr - 1, fc));
     Fp = lift_flux(central(C, farfield_ghost_st(C, mach, in), -nix, -niz, -vn));
     return;
   }
   const double len = sqrt_(nix * nix + niz * niz);
-  const auto O = state<K == 0>(S, sidx(fr + 1, fc));
-  const auto L = state<K == 1>(S, sidx(fr, fc));
-  const auto Rs = state<K == 2>(S, sidx(fr - 1, fc));
+  const auto O = state<K == 0, G>(S, sidx(fr + 1, fc));
+  const auto L = state<K == 1, G>(S, sidx(fr, fc));
+  const auto Rs = state<K == 2, G>(S, sidx(fr - 1, fc));
   if (fm == 1) {
     // face i of cell 1 (flag 2): central; face o of cell 0 (flag 1): JST whose outer neighbour
     // is the wall ghost of cell 0. Sensors: at cell 0 from its wall ghost, at cell 1 interior.
@@ -145,7 +153,7 @@ __device__ __forceinline__ void radial_pair(const Smem& S, const Instance& in, i
     Fp = lift_flux(jst(gh, Rs, L, O, -nix, -niz, len, -vn, sr, sl, in));
     return;
   }
-  const auto II = state<K == 3>(S, sidx(fr - 2, fc));
+  const auto II = state<K == 3, G>(S, sidx(fr - 2, fc));
   if (fm == M - 1) {
     // face i of cell M-1 (flag 5): JST whose outer neighbour is the far-field ghost; face o of
     // cell M-2 (flag 4): central. Sensors: at cell M-1 from its ghost, at cell M-2 interior.
@@ -162,27 +170,27 @@ __device__ __forceinline__ void radial_pair(const Smem& S, const Instance& in, i
   jst_pair(O, L, Rs, II, nix, niz, len, vn, sl, sr, in, F, Fp);
 }
 
-// Finishes a block: J <- -acc / area for an active slot, 0 for a slot the reference does not
-// write (f90:727-746); 16 consecutive doubles (one cell's block of one slot).
-__device__ __forceinline__ void store_block(double* out, const double (&acc)[16], double area,
+// Finishes a block part: J <- -acc / area for an active slot, 0 for a slot the reference does
+// not write (f90:727-746); kB consecutive doubles of one cell's column-major block.
+__device__ __forceinline__ void store_block(double* out, const double (&acc)[kB], double area,
                                             bool active) {
   double2* o = reinterpret_cast<double2*>(out);
 #pragma unroll
-  for (int e = 0; e < 16; e += 2)
+  for (int e = 0; e < kB; e += 2)
     o[e / 2] = active ? make_double2(-acc[e] / area, -acc[e + 1] / area) : make_double2(0.0, 0.0);
 }
 
-__device__ __forceinline__ void add_to(double (&acc)[16], const double (&b)[16]) {
+__device__ __forceinline__ void add_to(double (&acc)[kB], const double (&b)[kB]) {
 #pragma unroll
-  for (int e = 0; e < 16; ++e) acc[e] = acc[e] + b[e];
+  for (int e = 0; e < kB; ++e) acc[e] = acc[e] + b[e];
 }
 
 // One seeded stencil position K of the angular faces (Radial = false) or the radial faces:
 // evaluate this thread's face, pass the neighbour's derivative block through shared memory, and
 // advance this cell's blocks.
-template <bool Radial, int K>
+template <bool Radial, int K, int G>
 __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, int n0,
-                                          double (&acc_c)[16], double (&acc_x)[16],
+                                          double (&acc_c)[kB], double (&acc_x)[kB],
                                           double area, double* Jc, int64_t slot_stride) {
   const int M = in.M, N = in.N;
   const int tid = threadIdx.x, r = tid % kTM, c = tid / kTM;
@@ -191,9 +199,9 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
     return rr >= 0 && cc >= 0 && rr < kTM && cc < kTN && m0 + rr < M && n0 + cc < N;
   };
   const bool own = exists(r, c);
-  double fo[16];  // this cell's own face, differentiated
+  double fo[kB];  // this cell's own face, differentiated
 #pragma unroll
-  for (int e = 0; e < 16; ++e) fo[e] = 0.0;
+  for (int e = 0; e < kB; ++e) fo[e] = 0.0;
   {
     int fr = r, fc = c;  // the face this thread evaluates
     int tr, tc;          // the cell that receives its neighbour flux
@@ -215,43 +223,43 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
     }
     if (eval) {
       Flux<D4> F, Fp;
-      if (!Radial) angular_pair<K>(S, in, fr, fc, F, Fp);
-      else radial_pair<K>(S, in, m0 + fr, fr, fc, F, Fp);
+      if (!Radial) angular_pair<K, G>(S, in, fr, fc, F, Fp);
+      else radial_pair<K, G>(S, in, m0 + fr, fr, fc, F, Fp);
       if (exists(tr, tc)) {
 #pragma unroll
         for (int r4 = 0; r4 < 4; ++r4)
 #pragma unroll
-          for (int i = 0; i < 4; ++i) S.nb[r4 + 4 * i][tc][tr] = Fp.f[r4].d[i];
+          for (int i = 0; i < kW; ++i) S.nb[r4 + 4 * i][tc][tr] = Fp.f[r4].d[i];
       }
       if (fr == r && fc == c && own) {
 #pragma unroll
         for (int r4 = 0; r4 < 4; ++r4)
 #pragma unroll
-          for (int i = 0; i < 4; ++i) fo[r4 + 4 * i] = F.f[r4].d[i];
+          for (int i = 0; i < kW; ++i) fo[r4 + 4 * i] = F.f[r4].d[i];
       }
     }
   }
   __syncthreads();
   if (own) {
-    double fn[16];  // the neighbour's face, differentiated
+    double fn[kB];  // the neighbour's face, differentiated
 #pragma unroll
-    for (int e = 0; e < 16; ++e) fn[e] = S.nb[e][c][r];
+    for (int e = 0; e < kB; ++e) fn[e] = S.nb[e][c][r];
     // angular: own face b seeded at (f, c, b, bb)[K], the f neighbour's at (ff, f, c, b)[K];
     // radial: own face i seeded at (o, c, i, ii)[K], the o neighbour's at (oo, o, c, i)[K]
     constexpr int s_own = Radial ? (K == 0 ? kO : K == 1 ? kC : K == 2 ? kI : kII)
                                  : (K == 0 ? kF : K == 1 ? kC : K == 2 ? kB : kBB);
     constexpr int s_nb = Radial ? (K == 0 ? kOO : K == 1 ? kO : K == 2 ? kC : kI)
                                 : (K == 0 ? kFF : K == 1 ? kF : K == 2 ? kC : kB);
-    double* out_own = Jc + slot_stride * s_own;
-    double* out_nb = Jc + slot_stride * s_nb;
+    double* out_own = Jc + slot_stride * s_own + kB * G;
+    double* out_nb = Jc + slot_stride * s_nb + kB * G;
     if constexpr (K == 0) {
       store_block(out_nb, fn, area, slot_active(s_nb, m, M));
 #pragma unroll
-      for (int e = 0; e < 16; ++e) acc_x[e] = fo[e];
+      for (int e = 0; e < kB; ++e) acc_x[e] = fo[e];
     } else if constexpr (K == 1) {
       if constexpr (!Radial) {
 #pragma unroll
-        for (int e = 0; e < 16; ++e) acc_c[e] = fo[e];
+        for (int e = 0; e < kB; ++e) acc_c[e] = fo[e];
       } else {
         add_to(acc_c, fo);
       }
@@ -259,7 +267,7 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
       store_block(out_nb, acc_x, area, slot_active(s_nb, m, M));
     } else if constexpr (K == 2) {
 #pragma unroll
-      for (int e = 0; e < 16; ++e) acc_x[e] = fo[e];
+      for (int e = 0; e < kB; ++e) acc_x[e] = fo[e];
       add_to(acc_c, fn);
       if constexpr (Radial) store_block(out_nb, acc_c, area, true);
     } else {
@@ -271,7 +279,22 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+// The eight seed steps of one pass (component group G of the seeded states).
+template <int G>
+__device__ __forceinline__ void all_steps(Smem& S, const Instance& in, int m0, int n0,
+                                          double (&acc_c)[kB], double (&acc_x)[kB], double area,
+                                          double* Jc, int64_t slot_stride) {
+  seed_step<false, 0, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 1, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 2, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 3, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 0, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 1, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 2, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 3, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+}
+
+__global__ void __launch_bounds__(kThreads, kW == 4 ? 1 : 2)
     k_jac_states_tiled(Table t, const double* X, const double* V, const double* U, double* J) {
   extern __shared__ __align__(16) unsigned char jt_smem[];
   Smem& S = *reinterpret_cast<Smem*>(jt_smem);
@@ -329,15 +352,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   const int64_t slot_stride = 16 * (int64_t)M * N;
   double* Jc = J + 144 * in.cell_offset + 16 * ((int64_t)(m0 + r) + (int64_t)M * (n0 + c));
-  double acc_c[16], acc_x[16];
-  seed_step<false, 0>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<false, 1>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<false, 2>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<false, 3>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 0>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 1>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 2>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 3>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  double acc_c[kB], acc_x[kB];
+  all_steps<0>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  if constexpr (kGroups > 1) all_steps<1>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
 }
 
 int tiles(int M, int N) { return ((M + kTM - 1) / kTM) * ((N + kTN - 1) / kTN); }

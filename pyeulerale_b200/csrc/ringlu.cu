@@ -1161,3 +1161,310 @@ int eb_ringlu_solve(const eb_batch* b, const double* J, double shift_re, double 
 }
 
 }  // extern "C"
+
+// ---- PTC/SER steady state on the device ------------------------------------------------------
+//
+// The pseudo-transient continuation with switched evolution relaxation of the reference's
+// example driver (examples/response/run.py:84-123): per step the residual R of the current state,
+// its infinity norm relative to the initial state's (rel), the shift rel / ser (the inverse of
+// the time step ser / rel), the states Jacobian, and the update U += Re((J - shift I)^-1 (-R));
+// the loop stops at rel <= rtol (or a non-finite rel) or after max_steps steps. Here a step is a
+// fixed launch sequence whose control values (norm, rel, shift, the stop flag) live in device
+// memory: the first step runs eagerly, the sequence is then captured once in a CUDA graph and
+// replayed, and the host reads only the stop flag of the previous step (so at most one replay
+// runs past the last step; its update and history entry are skipped on the device). The solve is
+// the ring-block LU with one refinement step against the device residual.
+
+namespace eb {
+namespace rl {
+
+struct PtcCtl {
+  unsigned long long norm_bits;  // max |R| of the step (bits of a non-negative double)
+  double norm0;                  // max |R| of the initial state
+  int run;                       // the loop had not stopped when this step began
+  int done;                      // stopped: rel <= rtol, rel not finite, or a singular block
+  int steps;                     // relative norms recorded
+  int status;                    // EB_OK or EB_ERR_NAN
+};
+
+struct PtcLayout {
+  Layout lu;
+  size_t off_lu, off_x, off_r, off_ctl, off_hist, total;
+};
+
+PtcLayout ptc_plan(int M, int N, int max_steps) {
+  PtcLayout P;
+  P.lu = plan(M, N);
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = align_up(o + bytes);
+    return at;
+  };
+  P.off_lu = take(P.lu.total);
+  P.off_x = take(sizeof(double) * 8 * (size_t)M * N);
+  P.off_r = take(sizeof(double) * 8 * (size_t)M * N);
+  P.off_ctl = take(sizeof(PtcCtl));
+  P.off_hist = take(sizeof(double) * 2 * (size_t)max_steps);
+  P.total = o;
+  return P;
+}
+
+__global__ void k_ptc_begin(PtcCtl* c) {
+  c->run = !c->done;
+  c->norm_bits = 0ull;
+}
+
+// max |v| over v, as the maximum of the bit patterns of |v| (ordered like the values for
+// non-negative doubles; a NaN compares above every finite value and infinity)
+__global__ void __launch_bounds__(256) k_ptc_absmax(int64_t n, const double* v, PtcCtl* c) {
+  unsigned long long m = 0ull;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, (unsigned long long)__double_as_longlong(fabs(v[i])));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(&c->norm_bits, m);
+}
+
+__global__ void k_ptc_init(PtcCtl* c) {
+  c->norm0 = __longlong_as_double((long long)c->norm_bits);
+  c->run = 1;
+  c->done = 0;
+  c->steps = 0;
+  c->status = EB_OK;
+}
+
+// rel = |R| / |R_0|, the history entry (|R|, rel), the stop test and the shift of the step
+// (time step ser * rel^-1, shift = time step^-1, the example driver's arithmetic).
+__global__ void k_ptc_control(PtcCtl* c, double ser, double rtol, double* hist, double* shift) {
+  if (!c->run) return;
+  const double norm = __longlong_as_double((long long)c->norm_bits);
+  const double rel = norm / c->norm0;
+  hist[2 * c->steps] = norm;
+  hist[2 * c->steps + 1] = rel;
+  c->steps += 1;
+  if (rel <= rtol || isnan(rel)) {
+    c->done = 1;
+    c->status = isnan(rel) ? EB_ERR_NAN : EB_OK;
+    return;
+  }
+  const double time_step = ser * (1.0 / rel);
+  shift[0] = 1.0 / time_step;
+  shift[1] = 0.0;
+}
+
+// y (ring layout, complex) = -R
+__global__ void k_ptc_rhs(int M, int N, const double* R, const PtcCtl* c, cuDoubleComplex* y) {
+  if (c->done) return;
+  const int64_t cells = (int64_t)M * N;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(g % M), n = (int)(g / M);
+    for (int v = 0; v < 4; ++v)
+      y[(int64_t)m * 4 * N + 4 * n + v] = make_cuDoubleComplex(-R[4 * g + v], 0.0);
+  }
+}
+
+// r = -R - (J - s I) x for the solution x of the first solve (x copied to the reference layout
+// into xs): the residual the refinement step solves for.
+__global__ void __launch_bounds__(128) k_ptc_refine_rhs(int M, int N, const double* J,
+                                                        const double* shift,
+                                                        const cuDoubleComplex* x_ring,
+                                                        const double* R, const PtcCtl* c,
+                                                        double* xs, double* r) {
+  if (c->done) return;
+  const int64_t cells = (int64_t)M * N, slot_stride = 16 * cells;
+  const double sr = shift[0], si = shift[1];
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(g % M), n = (int)(g / M);
+    double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+    for (int s = 0; s < 9; ++s) {
+      if (!slot_active(s, m, M)) continue;
+      const double* blk = J + slot_stride * s + 16 * g;
+      const int mm = m + slot_dm(s), nn = wrap(n + slot_dn(s), N);
+      const cuDoubleComplex* xj = x_ring + (int64_t)mm * 4 * N + 4 * nn;
+      for (int i = 0; i < 4; ++i)
+        for (int q = 0; q < 4; ++q) {
+          ar[q] += blk[q + 4 * i] * xj[i].x;
+          ai[q] += blk[q + 4 * i] * xj[i].y;
+        }
+    }
+    const cuDoubleComplex* xc = x_ring + (int64_t)m * 4 * N + 4 * n;
+    for (int q = 0; q < 4; ++q) {
+      const double xr = xc[q].x, xi = xc[q].y;
+      xs[8 * g + 2 * q] = xr;
+      xs[8 * g + 2 * q + 1] = xi;
+      r[8 * g + 2 * q] = -R[4 * g + q] - (ar[q] - (sr * xr - si * xi));
+      r[8 * g + 2 * q + 1] = -(ai[q] - (sr * xi + si * xr));
+    }
+  }
+}
+
+// U += Re(xs + correction); a singular ring block (LU info) stops the loop instead
+__global__ void k_ptc_update(int M, int N, const cuDoubleComplex* x_ring, const double* xs,
+                             const int* lu_info, PtcCtl* c, double* U) {
+  if (c->done) return;
+  if (*lu_info != 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      c->done = 1;
+      c->status = EB_ERR_NAN;
+    }
+    return;
+  }
+  const int64_t cells = (int64_t)M * N;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < cells;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(g % M), n = (int)(g / M);
+    for (int v = 0; v < 4; ++v)
+      U[4 * g + v] += xs[8 * g + 2 * v] + x_ring[(int64_t)m * 4 * N + 4 * n + v].x;
+  }
+}
+
+// One PTC step's launch sequence on st (all control values on the device).
+int issue_ptc_step(const eb_batch* b, const PtcLayout& P, char* ws, const double* X,
+                   const double* V, double* U, double* R, double* J, double ser, double rtol,
+                   cudaStream_t st) {
+  const int M = P.lu.M, N = P.lu.N;
+  const int64_t cells = (int64_t)M * N;
+  PtcCtl* ctl = reinterpret_cast<PtcCtl*>(ws + P.off_ctl);
+  char* lw = ws + P.off_lu;
+  const Group g{P.lu, lw, (int64_t)P.lu.total, 1};
+  double* shift = reinterpret_cast<double*>(lw + P.lu.off_shift);
+  cuDoubleComplex* y = reinterpret_cast<cuDoubleComplex*>(lw + P.lu.off_y);
+  cuDoubleComplex* x = reinterpret_cast<cuDoubleComplex*>(lw + P.lu.off_x);
+  double* xs = reinterpret_cast<double*>(ws + P.off_x);
+  double* r = reinterpret_cast<double*>(ws + P.off_r);
+  const int gc = grid_for(cells, 128);
+  int rc;
+  k_ptc_begin<<<1, 1, 0, st>>>(ctl);
+  if ((rc = eb_compute_odes(b, X, V, U, R, st)) != EB_OK) return rc;
+  k_ptc_absmax<<<grid_for(4 * cells, 256), 256, 0, st>>>(4 * cells, R, ctl);
+  k_ptc_control<<<1, 1, 0, st>>>(ctl, ser, rtol, reinterpret_cast<double*>(ws + P.off_hist),
+                                 shift);
+  if ((rc = eb_compute_odes_wrt_states(b, X, V, U, J, st)) != EB_OK) return rc;
+  const double* js[1] = {J};
+  if ((rc = issue_factor(g, js, st)) != EB_OK) return rc;
+  cublasHandle_t h = nullptr;
+  if ((rc = blas_handle(st, h)) != EB_OK) return rc;
+  k_ptc_rhs<<<gc, 128, 0, st>>>(M, N, R, ctl, y);
+  if ((rc = ring_solve(g, h, false, st)) != EB_OK) return rc;
+  k_ptc_refine_rhs<<<gc, 128, 0, st>>>(M, N, J, shift, x, R, ctl, xs, r);
+  k_to_rings<<<gc, 128, 0, st>>>(M, N, r, y);
+  if ((rc = ring_solve(g, h, false, st)) != EB_OK) return rc;
+  k_ptc_update<<<gc, 128, 0, st>>>(M, N, x, xs, reinterpret_cast<int*>(lw + P.lu.off_info), ctl,
+                                   U);
+  return check_launch("ptc step");
+}
+
+}  // namespace rl
+}  // namespace eb
+
+extern "C" {
+
+int64_t eb_ptc_workspace_bytes(int M, int N, int max_steps) {
+  if (M < 4 || N < 5 || panel_width(4 * N) == 0 || max_steps < 1) return -1;
+  return (int64_t)ptc_plan(M, N, max_steps).total;
+}
+
+int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, double* R,
+               double* J, double ser, double rtol, int max_steps, void* workspace,
+               int64_t workspace_bytes, double* history, int* n_steps, void* stream) {
+  int rc = validate(b);
+  if (rc != EB_OK) return rc;
+  if (b->n_inst != 1 || b->d_table) return fail(EB_ERR_ARG, "ptc: single instance only");
+  if (!X || !U || !R || !J || !workspace || !history || !n_steps)
+    return fail(EB_ERR_ARG, "ptc: null argument");
+  if ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(V) |
+       reinterpret_cast<uintptr_t>(U) | reinterpret_cast<uintptr_t>(R) |
+       reinterpret_cast<uintptr_t>(J)) & 15)
+    return fail(EB_ERR_ARG, "ptc: arrays must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail(EB_ERR_ARG, "ptc: workspace not 256-byte aligned");
+  if (max_steps < 1 || !(ser > 0) || !(rtol >= 0)) return fail(EB_ERR_ARG, "ptc: bad options");
+  const int M = b->single.M, N = b->single.N;
+  if (M < 4 || N < 5 || panel_width(4 * N) == 0) return fail(EB_ERR_ARG, "ptc: unsupported grid size");
+  const PtcLayout P = ptc_plan(M, N, max_steps);
+  if (workspace_bytes < (int64_t)P.total) return fail(EB_ERR_ARG, "ptc: workspace too small");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  PtcCtl* ctl = reinterpret_cast<PtcCtl*>(ws + P.off_ctl);
+  const int64_t cells = (int64_t)M * N;
+  *n_steps = 0;
+  // the initial state's residual norm
+  k_ptc_begin<<<1, 1, 0, st>>>(ctl);
+  if ((rc = eb_compute_odes(b, X, V, U, R, st)) != EB_OK) return rc;
+  k_ptc_absmax<<<grid_for(4 * cells, 256), 256, 0, st>>>(4 * cells, R, ctl);
+  k_ptc_init<<<1, 1, 0, st>>>(ctl);
+  if ((rc = check_launch("ptc init")) != EB_OK) return rc;
+  int done_h[2] = {0, 0};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec = nullptr;
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  };
+  for (auto& e : ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cleanup();
+      return check_launch("ptc events");
+    }
+  for (int k = 0; k < max_steps; ++k) {
+    if (k == 0) {  // eagerly (cuBLAS and the kernels initialise outside any capture)
+      rc = issue_ptc_step(b, P, ws, X, V, U, R, J, ser, rtol, st);
+    } else {
+      if (!exec) {
+        cudaGraph_t graph = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+        if (err == cudaSuccess) {
+          rc = issue_ptc_step(b, P, ws, X, V, U, R, J, ser, rtol, st);
+          err = cudaStreamEndCapture(st, &graph);
+        }
+        if (rc == EB_OK && err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != EB_OK || err != cudaSuccess) {
+          cleanup();
+          if (rc != EB_OK) return rc;
+          return fail(EB_ERR_CUDA, (std::string("ptc: graph capture failed: ") +
+                                    cudaGetErrorString(err)).c_str());
+        }
+      }
+      rc = cudaGraphLaunch(exec, st) == cudaSuccess ? EB_OK : check_launch("ptc graph launch");
+    }
+    if (rc != EB_OK) {
+      cleanup();
+      return rc;
+    }
+    // the stop flag of this step, read back once the next step is queued
+    if (cudaMemcpyAsync(&done_h[k & 1], &ctl->done, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaEventRecord(ev[k & 1], st) != cudaSuccess) {
+      cleanup();
+      return check_launch("ptc flag");
+    }
+    if (k >= 1) {
+      if (cudaEventSynchronize(ev[(k - 1) & 1]) != cudaSuccess) {
+        cleanup();
+        return check_launch("ptc flag");
+      }
+      if (done_h[(k - 1) & 1]) break;
+    }
+  }
+  PtcCtl hc;
+  const cudaError_t e1 = cudaMemcpyAsync(&hc, ctl, sizeof(PtcCtl), cudaMemcpyDeviceToHost, st);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  cleanup();
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return check_launch("ptc result");
+  const int n = std::min(hc.steps, max_steps);
+  if (n > 0 && cudaMemcpy(history, ws + P.off_hist, sizeof(double) * 2 * n,
+                          cudaMemcpyDeviceToHost) != cudaSuccess)
+    return check_launch("ptc history");
+  *n_steps = n;
+  if (hc.status != EB_OK)
+    return fail(hc.status, "ptc: non-finite residual or singular ring block");
+  return EB_OK;
+}
+
+}  // extern "C"

@@ -31,11 +31,17 @@ class PtcResult:
 
 
 def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None, ser: float = 0.1,
-        safeguard: bool = False, growth: float = 10.0, max_retries: int = 8) -> PtcResult:
+        safeguard: bool = False, growth: float = 10.0, max_retries: int = 8,
+        device: bool = True) -> PtcResult:
     """Pseudo-transient continuation with switched evolution relaxation
     (examples/response/run.py:84-123): the time step is ``ser`` / (relative infinity-norm of the
     residual), each step solves (dR/dU - dt^-1 I) dU = -R on the device, and the loop stops at
     rel <= rtol (or NaN), leaving the solver linearized at the final state.
+
+    With ``device`` (the default) the whole loop runs on the GPU (``eb_ptc_run``: residual,
+    infinity norm, shift, Jacobian, ring-block LU solve and update with their control values in
+    device memory, one CUDA graph replayed per step); the states, residual and history come back
+    once at the end. ``device=False`` runs the same loop step by step from the host.
 
     ``safeguard`` (off by default, which is the reference's loop) rejects a step whose residual
     is not finite or grows by more than ``growth``, and retries it with a ten times larger shift
@@ -43,6 +49,8 @@ def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None, ser: float = 
     half per accepted step. This keeps the iterates of cases whose undamped steps overshoot
     into negative densities finite; whether they then converge depends on the case."""
     res = PtcResult()
+    if device and not safeguard:
+        return _ptc_device(solver, rtol, max_iter, out, ser)
     solver.compute_odes()
     norm_free_stream = np.max(np.abs(solver.odes))
     if out is not None:
@@ -77,6 +85,28 @@ def ptc(solver, rtol: float = 1e-9, max_iter: int = 100, out=None, ser: float = 
                 break
             shift *= 10.0
         floor = shift / 2.0 if shift > rel / ser else floor / 2.0
+    return res
+
+
+def _ptc_device(solver, rtol: float, max_iter: int, out, ser: float) -> PtcResult:
+    """``ptc`` through the device loop of one instance (``solver.ptc_run``)."""
+    from . import solver as solver_mod
+
+    solver._upload()
+    norms, rels, _ = solver_mod.ptc_run(solver._batch(), solver._dX, solver._dV, solver._dU,
+                                        solver._dR, solver._dJ_u, ser=ser, rtol=rtol,
+                                        max_steps=max_iter)
+    solver._states[...] = np.reshape(solver._dU.cpu().numpy(), solver._states.shape, order="F")
+    res = PtcResult(norms=[float(v) for v in norms], rel_norms=[float(v) for v in rels])
+    if out is not None:
+        print(f"\nPseudo-transient continuation:\n{'it':>6} {'residual':>15} "
+              f"{'rel residual':>15}", file=out)
+        for it, (norm, rel) in enumerate(zip(res.norms, res.rel_norms)):
+            print(f"{it:>6} {norm:>15.1e} {rel:>15.1e}", file=out)
+    # the solver's host residual, Jacobians and forces at the final state
+    solver.compute_odes()
+    solver.linearize()
+    solver.compute_forces()
     return res
 
 

@@ -313,3 +313,48 @@ def solve_shifted_noalloc(batch: _lib.Batch, J, rhs, shifts, *, adjoint: bool = 
     return x, SolveInfo({"iterations": i.iterations, "cycles": i.cycles,
                          "converged": bool(i.converged), "rel_residual": i.rel_residual}
                         for i in infos)
+
+
+def _bind_ptc() -> ctypes.CDLL:
+    lib = _lib.load()
+    if not getattr(lib, "_ptc_bound", False):
+        P = ctypes.c_void_p
+        lib.eb_ptc_workspace_bytes.restype = ctypes.c_int64
+        lib.eb_ptc_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.eb_ptc_run.restype = ctypes.c_int
+        lib.eb_ptc_run.argtypes = [ctypes.POINTER(_lib.Batch), P, P, P, P, P, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int, P, ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                   P]
+        lib._ptc_bound = True
+    return lib
+
+
+def ptc_run(batch: _lib.Batch, X, V, U, R, J, ser: float = 0.1, rtol: float = 1e-9,
+            max_steps: int = 100, workspace=None):
+    """The PTC/SER steady-state loop of one instance on the device (``eb_ptc_run``).
+
+    ``X``, ``V``, ``U`` (updated in place), ``R`` and ``J`` (receiving the final residual and
+    states Jacobian) are device float64 tensors in the reference layouts. Returns
+    ``(norms, rel_norms, status)``: per step max|R| and max|R| / max|R_0|, and the C ABI status
+    (``EB_OK``, or ``EB_ERR_NAN`` when the residual became non-finite or a ring block singular).
+    """
+    import torch
+
+    lib = _bind_ptc()
+    need = lib.eb_ptc_workspace_bytes(batch.single.M, batch.single.N, int(max_steps))
+    if need < 0:
+        raise ValueError("PTC needs a single instance with M >= 4, N >= 5")
+    if workspace is None or workspace.numel() < need or workspace.data_ptr() % 256:
+        workspace = torch.empty(int(need), dtype=torch.uint8, device=U.device)
+    hist = (ctypes.c_double * (2 * int(max_steps)))()
+    n = ctypes.c_int(0)
+    V_ptr = None if V is None else V.data_ptr()
+    rc = lib.eb_ptc_run(ctypes.byref(batch), X.data_ptr(), V_ptr, U.data_ptr(), R.data_ptr(),
+                        J.data_ptr(), float(ser), float(rtol), int(max_steps),
+                        workspace.data_ptr(), int(workspace.numel()), hist, ctypes.byref(n),
+                        torch.cuda.current_stream().cuda_stream)
+    if rc not in (_lib.EB_OK, _lib.EB_ERR_NAN):
+        raise _lib.EulerB200Error("eb_ptc_run", rc, lib.eb_last_error().decode())
+    vals = list(hist)[:2 * n.value]
+    return vals[0::2], vals[1::2], rc

@@ -117,3 +117,45 @@ def test_ptc_batched_large_grids_match_single(cuda):
         assert rel_err(grads[k], ref) <= 1e-8, (k, rel_err(grads[k], ref))
         del s
         cuda.cuda.empty_cache()
+
+
+def test_ptc_device_loop_matches_host_loop(cuda):
+    """The device PTC loop (eb_ptc_run: one captured step replayed, control values on the
+    device) gives the host-driven loop's history, steady state and final residual."""
+    from pyeulerale_b200 import SpatialDiscretization, drivers
+    from pyeulerale_b200 import grid as G
+
+    X = G.naca_ogrid(33, 41, 0.10, 1.0, 20.0, 0.01)
+    a = SpatialDiscretization(X, mach_number=0.5, angle_of_attack=1.25)
+    b = SpatialDiscretization(X, mach_number=0.5, angle_of_attack=1.25)
+    ha = drivers.ptc(a, rtol=1e-10, max_iter=40, device=True)
+    hb = drivers.ptc(b, rtol=1e-10, max_iter=40, device=False)
+    assert ha.rel_norms[-1] <= 1e-10 and hb.rel_norms[-1] <= 1e-10
+    assert abs(ha.iterations - hb.iterations) <= 1, (ha.rel_norms, hb.rel_norms)
+    early = [i for i, r in enumerate(hb.rel_norms) if r > 1e-7 and i < ha.iterations]
+    assert np.allclose([ha.rel_norms[i] for i in early], [hb.rel_norms[i] for i in early],
+                       rtol=1e-6)
+    assert np.allclose(ha.norms[:len(early)], hb.norms[:len(early)], rtol=1e-6)
+    assert rel_err(a.states.real, b.states.real) <= 1e-9
+    assert np.max(np.abs(a.odes)) / np.max(np.abs(b.odes)) < 10.0  # both round-off level
+
+
+def test_ptc_device_loop_stops_on_nan_and_at_the_step_limit(cuda):
+    """A non-finite state ends the device loop with EB_ERR_NAN after recording a NaN norm; a
+    loop cut by max_steps returns EB_OK with max_steps entries (as the example driver)."""
+    from pyeulerale_b200 import _lib, grid as G, solver
+    from pyeulerale_b200.batch import InstanceSet, InstanceSpec
+
+    X = G.naca_ogrid(17, 21, 0.12, 1.0, 20.0, 0.01)
+    inst = InstanceSet([InstanceSpec(X, 0.5, 1.25)])
+    dX = cuda.from_numpy(inst.pack_vertices()).cuda()
+    dV = cuda.zeros_like(dX)
+    f64 = dict(dtype=cuda.float64, device="cuda")
+    U = cuda.empty(4 * inst.n_cells, **f64)
+    inst.call("eb_set_free_stream_state", U)
+    R, J = cuda.empty(4 * inst.n_cells, **f64), cuda.empty(144 * inst.n_cells, **f64)
+    norms, rels, rc = solver.ptc_run(inst.batch, dX, dV, U, R, J, rtol=1e-30, max_steps=3)
+    assert rc == _lib.EB_OK and len(rels) == 3 and rels[0] == 1.0
+    U[5] = float("nan")
+    norms, rels, rc = solver.ptc_run(inst.batch, dX, dV, U, R, J, rtol=1e-10, max_steps=5)
+    assert rc == _lib.EB_ERR_NAN and len(rels) == 1 and np.isnan(rels[0])

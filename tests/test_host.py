@@ -32,7 +32,8 @@ def test_library_exports_every_declared_symbol():
     bound = set(_lib.exported_symbols()) | {  # bound in pyeulerale_b200/solver.py
         "eb_gmres_solve", "eb_gmres_workspace_bytes", "eb_gmres_solve_noalloc",
         "eb_ringlu_factor", "eb_ringlu_solve", "eb_ringlu_workspace_bytes",
-        "eb_ringlu_factor_many", "eb_ringlu_solve_many"}
+        "eb_ringlu_factor_many", "eb_ringlu_solve_many", "eb_ptc_run",
+        "eb_ptc_workspace_bytes"}
     assert declared <= bound, declared - bound
 
 
