@@ -297,6 +297,15 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
                          int64_t workspace_stride, const double* const* rhs, double* const* x,
                          double tol, int max_refine, double* rel_residuals, void* stream);
 
+/* ---- launch-variant autotuner -------------------------------------------------------------- */
+
+/* Kernels with several launch variants of identical results (the states Jacobian: dual width 4
+ * at one CTA per SM or width 2 at two) time each variant on the first call for a problem size
+ * and keep the fastest (EB_AUTOTUNE=0, or a stream being captured: the default variant, untimed).
+ * Writes the choices and their times as text into buf (len bytes, NUL-terminated) and returns
+ * the report's full length. No counterpart in the reference (which has no GPU kernels). */
+int eb_autotune_report(char* buf, int len);
+
 /* ---- PTC/SER steady state ---------------------------------------------------------------- */
 
 /* Device workspace (bytes) of eb_ptc_run for an M x N instance and at most max_steps steps: the

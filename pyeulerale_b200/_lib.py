@@ -124,7 +124,7 @@ _CTYPE = {
 
 def exported_symbols() -> list[str]:
     """Entry points this binding expects the library to export (all of include/euler_b200.h)."""
-    return sorted([*_SIGNATURES, "eb_last_error", "eb_version"])
+    return sorted([*_SIGNATURES, "eb_last_error", "eb_version", "eb_autotune_report"])
 
 
 _lib = None
@@ -169,3 +169,15 @@ def as_f64_view(a: np.ndarray) -> np.ndarray:
     """Fortran-order complex/real array as a flat float64 view (copying if needed)."""
     flat = np.asarray(a).ravel(order="F")
     return flat.view(np.float64) if np.iscomplexobj(flat) else flat.astype(np.float64, copy=False)
+
+
+def autotune_report() -> str:
+    """The launch-variant autotuner's choices so far (``eb_autotune_report``)."""
+    lib = load()
+    fn = lib.eb_autotune_report
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    n = fn(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    fn(buf, n + 1)
+    return buf.value.decode()

@@ -396,3 +396,27 @@ def test_undersized_grids_are_rejected(cuda, M, N):
         _lib.call("eb_compute_odes", ctypes.byref(b), t.data_ptr(), t.data_ptr(), t.data_ptr(),
                   t.data_ptr(), None)
     assert err.value.code == _lib.EB_ERR_ARG
+
+
+def test_states_jacobian_variants_agree_and_autotune(cuda, golden_grids, monkeypatch):
+    """The two dual widths of the tiled states Jacobian give bit-identical blocks, and the
+    autotuner times both on the first call of a new size and reports its choice."""
+    from pyeulerale_b200 import _lib
+
+    case = make_case("naca0012_33", golden_grids, seed=2)
+    gpu = Gpu(cuda, case)
+    n = 144 * gpu.M * gpu.N
+    out = []
+    for v in ("v0", "v1"):
+        monkeypatch.setenv("EB_AUTOTUNE", v)
+        J = gpu.empty(n)
+        gpu.call("eb_compute_odes_wrt_states", gpu.X, gpu.V, gpu.U, J)
+        out.append(J.cpu().numpy())
+    np.testing.assert_array_equal(out[0], out[1])
+    monkeypatch.delenv("EB_AUTOTUNE")
+    J = gpu.empty(n)
+    gpu.call("eb_compute_odes_wrt_states", gpu.X, gpu.V, gpu.U, J)
+    np.testing.assert_array_equal(J.cpu().numpy(), out[0])
+    report = _lib.autotune_report()
+    line = [s for s in report.splitlines() if f"jac_states_tiled ({gpu.M * gpu.N}," in s]
+    assert line and "width 4" in line[0] and "width 2" in line[0] and "(kept)" in line[0]
