@@ -6,7 +6,8 @@
 // a warm-up and a run timed with CUDA events, and keeps the fastest; later calls launch the kept
 // variant directly. A call made while the stream is being captured into a CUDA graph, or with
 // the environment variable EB_AUTOTUNE=0, launches the default variant without timing (and
-// caches nothing). The choices and their times are listed by eb_autotune_report.
+// caches nothing); EB_AUTOTUNE=v<k> launches variant k. The choices and their times are listed
+// by eb_autotune_report.
 #pragma once
 
 #include <cuda_runtime.h>
