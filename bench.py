@@ -1012,6 +1012,7 @@ def run_b200(args) -> None:
             "vs_cpu_reference_method": None if cpu_lin is None
             else vjp["value"] / cpu_lin["vjp"]["value"]},
         "linear": linear,
+        "autotune": _lib.autotune_report().splitlines(),
         "second_order": second,
         "resolvent": res,
         "uneven": uneven,
