@@ -7,14 +7,15 @@
 // CTAs share an SM, for a second evaluation of the values.
 constexpr int kW = EB_JT_WIDTH;
 constexpr int kGroups = 4 / kW;
-constexpr int kB = 4 * kW;  // the part of a 4 x 4 block one pass forms: columns G kW .. G kW + kW - 1
+// the part of a 4 x 4 block one pass forms: its columns G kW .. G kW + kW - 1
+constexpr int kBlk = 4 * kW;
 using D4 = Dual<double, kW>;
 
 struct Smem {
   double rho[kStaged], j1[kStaged], j2[kStaged], e[kStaged];
   double p[kStaged], ir[kStaged], cs[kStaged];
   double x[kVerts], z[kVerts], vx[kVerts], vz[kVerts];
-  double nb[kB][kTN][kTM];  // derivative (block part) of the neighbour face's flux, per cell
+  double nb[kBlk][kTN][kTM];  // derivative (block part) of the neighbour face's flux, per cell
 };
 
 // Staged state i, seeded (conserved variables G kW .. G kW + kW - 1 as the dual components,
@@ -124,18 +125,18 @@ __device__ __forceinline__ void radial_pair(const Smem& S, const Instance& in, i
 }
 
 // Finishes a block part: J <- -acc / area for an active slot, 0 for a slot the reference does
-// not write (f90:727-746); kB consecutive doubles of one cell's column-major block.
-__device__ __forceinline__ void store_block(double* out, const double (&acc)[kB], double area,
+// not write (f90:727-746); kBlk consecutive doubles of one cell's column-major block.
+__device__ __forceinline__ void store_block(double* out, const double (&acc)[kBlk], double area,
                                             bool active) {
   double2* o = reinterpret_cast<double2*>(out);
 #pragma unroll
-  for (int e = 0; e < kB; e += 2)
+  for (int e = 0; e < kBlk; e += 2)
     o[e / 2] = active ? make_double2(-acc[e] / area, -acc[e + 1] / area) : make_double2(0.0, 0.0);
 }
 
-__device__ __forceinline__ void add_to(double (&acc)[kB], const double (&b)[kB]) {
+__device__ __forceinline__ void add_to(double (&acc)[kBlk], const double (&b)[kBlk]) {
 #pragma unroll
-  for (int e = 0; e < kB; ++e) acc[e] = acc[e] + b[e];
+  for (int e = 0; e < kBlk; ++e) acc[e] = acc[e] + b[e];
 }
 
 // One seeded stencil position K of the angular faces (Radial = false) or the radial faces:
@@ -143,7 +144,7 @@ __device__ __forceinline__ void add_to(double (&acc)[kB], const double (&b)[kB])
 // advance this cell's blocks.
 template <bool Radial, int K, int G>
 __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, int n0,
-                                          double (&acc_c)[kB], double (&acc_x)[kB],
+                                          double (&acc_c)[kBlk], double (&acc_x)[kBlk],
                                           double area, double* Jc, int64_t slot_stride) {
   const int M = in.M, N = in.N;
   const int tid = threadIdx.x, r = tid % kTM, c = tid / kTM;
@@ -152,9 +153,9 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
     return rr >= 0 && cc >= 0 && rr < kTM && cc < kTN && m0 + rr < M && n0 + cc < N;
   };
   const bool own = exists(r, c);
-  double fo[kB];  // this cell's own face, differentiated
+  double fo[kBlk];  // this cell's own face, differentiated
 #pragma unroll
-  for (int e = 0; e < kB; ++e) fo[e] = 0.0;
+  for (int e = 0; e < kBlk; ++e) fo[e] = 0.0;
   {
     int fr = r, fc = c;  // the face this thread evaluates
     int tr, tc;          // the cell that receives its neighbour flux
@@ -194,25 +195,26 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
   }
   __syncthreads();
   if (own) {
-    double fn[kB];  // the neighbour's face, differentiated
+    double fn[kBlk];  // the neighbour's face, differentiated
 #pragma unroll
-    for (int e = 0; e < kB; ++e) fn[e] = S.nb[e][c][r];
+    for (int e = 0; e < kBlk; ++e) fn[e] = S.nb[e][c][r];
     // angular: own face b seeded at (f, c, b, bb)[K], the f neighbour's at (ff, f, c, b)[K];
     // radial: own face i seeded at (o, c, i, ii)[K], the o neighbour's at (oo, o, c, i)[K]
     constexpr int s_own = Radial ? (K == 0 ? kO : K == 1 ? kC : K == 2 ? kI : kII)
                                  : (K == 0 ? kF : K == 1 ? kC : K == 2 ? kB : kBB);
     constexpr int s_nb = Radial ? (K == 0 ? kOO : K == 1 ? kO : K == 2 ? kC : kI)
                                 : (K == 0 ? kFF : K == 1 ? kF : K == 2 ? kC : kB);
-    double* out_own = Jc + slot_stride * s_own + kB * G;
-    double* out_nb = Jc + slot_stride * s_nb + kB * G;
+    static_assert(s_own >= 0 && s_own < 9 && s_nb >= 0 && s_nb < 9, "stencil slot out of range");
+    double* out_own = Jc + slot_stride * s_own + kBlk * G;
+    double* out_nb = Jc + slot_stride * s_nb + kBlk * G;
     if constexpr (K == 0) {
       store_block(out_nb, fn, area, slot_active(s_nb, m, M));
 #pragma unroll
-      for (int e = 0; e < kB; ++e) acc_x[e] = fo[e];
+      for (int e = 0; e < kBlk; ++e) acc_x[e] = fo[e];
     } else if constexpr (K == 1) {
       if constexpr (!Radial) {
 #pragma unroll
-        for (int e = 0; e < kB; ++e) acc_c[e] = fo[e];
+        for (int e = 0; e < kBlk; ++e) acc_c[e] = fo[e];
       } else {
         add_to(acc_c, fo);
       }
@@ -220,7 +222,7 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
       store_block(out_nb, acc_x, area, slot_active(s_nb, m, M));
     } else if constexpr (K == 2) {
 #pragma unroll
-      for (int e = 0; e < kB; ++e) acc_x[e] = fo[e];
+      for (int e = 0; e < kBlk; ++e) acc_x[e] = fo[e];
       add_to(acc_c, fn);
       if constexpr (Radial) store_block(out_nb, acc_c, area, true);
     } else {
@@ -235,7 +237,7 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, i
 // The eight seed steps of one pass (component group G of the seeded states).
 template <int G>
 __device__ __forceinline__ void all_steps(Smem& S, const Instance& in, int m0, int n0,
-                                          double (&acc_c)[kB], double (&acc_x)[kB], double area,
+                                          double (&acc_c)[kBlk], double (&acc_x)[kBlk], double area,
                                           double* Jc, int64_t slot_stride) {
   seed_step<false, 0, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
   seed_step<false, 1, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(kThreads, kW == 4 ? 1 : 2)
   }
   const int64_t slot_stride = 16 * (int64_t)M * N;
   double* Jc = J + 144 * in.cell_offset + 16 * ((int64_t)(m0 + r) + (int64_t)M * (n0 + c));
-  double acc_c[kB], acc_x[kB];
+  double acc_c[kBlk], acc_x[kBlk];
   all_steps<0>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
   if constexpr (kGroups > 1) all_steps<1>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
 }

@@ -1358,6 +1358,26 @@ int issue_ptc_step(const eb_batch* b, const PtcLayout& P, char* ws, const double
   return check_launch("ptc step");
 }
 
+// The stream the PTC loop runs on, one per thread and device: a CUDA graph cannot be captured
+// from the legacy default stream, which is what many callers pass.
+int ptc_stream(cudaStream_t& out) {
+  struct Own {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+  };
+  thread_local Own own;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("ptc device");
+  if (own.device != dev) {
+    own.stream = nullptr;  // a stream of another device is left to that device
+    if (cudaStreamCreateWithFlags(&own.stream, cudaStreamNonBlocking) != cudaSuccess)
+      return check_launch("ptc stream");
+    own.device = dev;
+  }
+  out = own.stream;
+  return EB_OK;
+}
+
 }  // namespace rl
 }  // namespace eb
 
@@ -1387,18 +1407,15 @@ int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, d
   if (M < 4 || N < 5 || panel_width(4 * N) == 0) return fail(EB_ERR_ARG, "ptc: unsupported grid size");
   const PtcLayout P = ptc_plan(M, N, max_steps);
   if (workspace_bytes < (int64_t)P.total) return fail(EB_ERR_ARG, "ptc: workspace too small");
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // the loop runs on a stream of its own, after the work queued on the caller's stream (and
+  // the caller's stream waits for the loop before anything queued on it later)
+  const cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
+  cudaStream_t st = nullptr;
+  if ((rc = ptc_stream(st)) != EB_OK) return rc;
   char* ws = static_cast<char*>(workspace);
   PtcCtl* ctl = reinterpret_cast<PtcCtl*>(ws + P.off_ctl);
   const int64_t cells = (int64_t)M * N;
   *n_steps = 0;
-  // the initial state's residual norm
-  k_ptc_begin<<<1, 1, 0, st>>>(ctl);
-  if ((rc = eb_compute_odes(b, X, V, U, R, st)) != EB_OK) return rc;
-  k_ptc_absmax<<<grid_for(4 * cells, 256), 256, 0, st>>>(4 * cells, R, ctl);
-  k_ptc_init<<<1, 1, 0, st>>>(ctl);
-  if ((rc = check_launch("ptc init")) != EB_OK) return rc;
-  int done_h[2] = {0, 0};
   cudaEvent_t ev[2] = {nullptr, nullptr};
   cudaGraphExec_t exec = nullptr;
   auto cleanup = [&]() {
@@ -1411,6 +1428,32 @@ int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, d
       cleanup();
       return check_launch("ptc events");
     }
+  if (cudaEventRecord(ev[0], caller) != cudaSuccess || cudaStreamWaitEvent(st, ev[0], 0) != cudaSuccess) {
+    cleanup();
+    return check_launch("ptc stream order");
+  }
+  // the initial state's residual norm
+  k_ptc_begin<<<1, 1, 0, st>>>(ctl);
+  if ((rc = eb_compute_odes(b, X, V, U, R, st)) == EB_OK) {
+    k_ptc_absmax<<<grid_for(4 * cells, 256), 256, 0, st>>>(4 * cells, R, ctl);
+    k_ptc_init<<<1, 1, 0, st>>>(ctl);
+    rc = check_launch("ptc init");
+  }
+  // two stop flags in pinned host memory (allocated once per thread), so that reading one back
+  // does not wait for the step queued after it
+  thread_local int* done_h = nullptr;
+  if (rc == EB_OK && !done_h &&
+      cudaHostAlloc(reinterpret_cast<void**>(&done_h), 2 * sizeof(int), cudaHostAllocDefault) !=
+          cudaSuccess) {
+    done_h = nullptr;
+    rc = check_launch("ptc flag buffer");
+  }
+  if (rc != EB_OK) {
+    cudaStreamSynchronize(st);
+    cleanup();
+    return rc;
+  }
+  done_h[0] = done_h[1] = 0;
   for (int k = 0; k < max_steps; ++k) {
     if (k == 0) {  // eagerly (cuBLAS and the kernels initialise outside any capture)
       rc = issue_ptc_step(b, P, ws, X, V, U, R, J, ser, rtol, st);
@@ -1425,6 +1468,8 @@ int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, d
         if (rc == EB_OK && err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
         if (rc != EB_OK || err != cudaSuccess) {
+          cudaGetLastError();  // a failed capture must not leave its error to later calls
+          cudaStreamSynchronize(st);
           cleanup();
           if (rc != EB_OK) return rc;
           return fail(EB_ERR_CUDA, (std::string("ptc: graph capture failed: ") +
@@ -1455,6 +1500,8 @@ int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, d
   PtcCtl hc;
   const cudaError_t e1 = cudaMemcpyAsync(&hc, ctl, sizeof(PtcCtl), cudaMemcpyDeviceToHost, st);
   const cudaError_t e2 = cudaStreamSynchronize(st);
+  cudaEventRecord(ev[0], st);
+  cudaStreamWaitEvent(caller, ev[0], 0);
   cleanup();
   if (e1 != cudaSuccess || e2 != cudaSuccess) return check_launch("ptc result");
   const int n = std::min(hc.steps, max_steps);
