@@ -521,6 +521,26 @@ def run_b200(args) -> None:
                    "bandwidth 6650 GB/s (of fallback)")
     traffic_cell = read_traffic()
 
+    # FP64 throughput (the FP64 roofline denominator): the library's DFMA probe on every SM
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    sink = torch.zeros(1, **f64)
+    fma_iters = 100_000
+
+    def fma_probe():
+        _lib.call("eb_fp64_fma_probe", fma_iters, sms, sink.data_ptr(), sp)
+
+    for _ in range(3):
+        fma_probe()
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(5):
+        fma_probe()
+    f1.record(stream)
+    barrier()
+    t_fma = f0.elapsed_time(f1) / 1e3 / 5
+    fp64_peak_tflops = 2.0 * 8 * sms * 256 * 8 * fma_iters / t_fma / 1e12
+
     # end to end through the C ABI with host buffers: every step copies its inputs (X, V, U)
     # from pinned host memory and its result R back. Serial: one stream, copies and launch in
     # sequence. Pipelined (the reported e2e): pyeulerale_b200.pipeline.ResidualPipeline, step
@@ -1013,6 +1033,9 @@ def run_b200(args) -> None:
             else vjp["value"] / cpu_lin["vjp"]["value"]},
         "linear": linear,
         "autotune": _lib.autotune_report().splitlines(),
+        "fp64_peak": {"tflops": fp64_peak_tflops, "sms": sms,
+                      "probe": "eb_fp64_fma_probe: 8 CTAs x 256 threads per SM, 8 independent "
+                               f"DFMA chains of {fma_iters} per thread, CUDA events"},
         "second_order": second,
         "resolvent": res,
         "uneven": uneven,

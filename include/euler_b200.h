@@ -297,6 +297,14 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
                          int64_t workspace_stride, const double* const* rhs, double* const* x,
                          double tol, int max_refine, double* rel_residuals, void* stream);
 
+/* ---- measurement ------------------------------------------------------------------------- */
+
+/* FP64 throughput probe (the FP64 roofline denominator of the stencil kernels): 8 * sms CTAs of
+ * 256 threads, each thread 8 independent chains of `iterations` fused multiply-adds (2 flops
+ * each); `sink` (one device double) is written only in a case that does not occur. No
+ * counterpart in the reference. */
+int eb_fp64_fma_probe(int64_t iterations, int sms, double* sink, void* stream);
+
 /* ---- launch-variant autotuner -------------------------------------------------------------- */
 
 /* Kernels with several launch variants of identical results (the states Jacobian: dual width 4

@@ -109,6 +109,7 @@ _SIGNATURES: dict[str, list] = {
     "eb_compute_pressure_coefficients": ["b", "p", "p", "s"],
     "eb_apply_pressure_coefficients_wrt_states_fwd": ["b", "p", "p", "p", "s"],
     "eb_bsr_shifted_spmv": ["i64", "p", "p", "p", "d", "d", "p", "p", "s"],
+    "eb_fp64_fma_probe": ["i64", "i", "p", "s"],
     "eb_odes_wrt_mach_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],
     "eb_odes_wrt_states_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],
     "eb_odes_wrt_vertices_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],
