@@ -32,9 +32,8 @@ NVCC_FLAGS = [
 # the differently inlined call sites. The residual itself is continuous there and keeps FMA.
 PER_FILE_FLAGS = {"jacobians.cu": ["-fmad=false"], "second_order.cu": ["-fmad=false"],
                   "jac_tiled.cu": ["-fmad=false"]}
-# cuBLAS serves the dense super-block products (strided-batched GEMM / GEMV) of the ring-block LU.
-LINK_FLAGS = ["-L/usr/local/cuda/lib64", "-lcublas",
-              "-Xlinker", "-rpath", "-Xlinker", "/usr/local/cuda/lib64"]
+# The library links only the CUDA runtime: its dense products are its own kernels (dense.cu).
+LINK_FLAGS = []
 
 
 def _nvcc() -> str:

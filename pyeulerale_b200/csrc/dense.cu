@@ -1,0 +1,276 @@
+// Dense complex double products of the ring-block LU (ringlu.cu): strided-batched
+// C = alpha A B + beta C (column-major, no transposes) on the FP64 tensor-core instruction
+// mma.sync.m8n8k4.f64, and strided-batched matrix-vector products y = alpha op(A) x + beta y with
+// op(A) = A or A^H. alpha and beta are real (the LU uses +-1 and 0 / 1).
+//
+// GEMM: a CTA computes a kBM x kBN tile of C for one batch entry with four warps, each a 32 x 32
+// sub-tile as 4 x 4 products of 8 x 8 (m8n8k4 fragments; real and imaginary parts in separate
+// accumulators: re += Ar Br - Ai Bi, im += Ar Bi + Ai Br, four real MMAs per complex product).
+// The kBK-deep slices of A and B go through shared memory as separate real / imaginary planes,
+// two slices in flight (the next slice's global loads are issued before the current slice's
+// MMAs). Edges (sizes not multiples of the tile) load zeros and store under bounds checks.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dense.cuh"
+
+namespace eb {
+
+int check_launch(const char* what);
+
+namespace dense {
+namespace {
+
+constexpr int kBM = 64, kBN = 64, kBK = 16;
+constexpr int kGemmThreads = 128;
+// Shared-memory pitches (doubles) of the A planes [k][m] and B planes [n][k], chosen so that a
+// warp's fragment loads (4 k x 8 m, and 8 n x 4 k) fall on distinct banks within each half.
+constexpr int kPadM = kBM + 8;
+constexpr int kPadK = kBK + 4;
+
+struct GemmSmem {
+  double ar[2][kBK][kPadM], ai[2][kBK][kPadM];
+  double br[2][kBN][kPadK], bi[2][kBN][kPadK];
+};
+
+// D = A B + C for one 8 x 8 x 4 FP64 tile (a: A[lane / 4][lane % 4], b: B[lane % 4][lane / 4],
+// c / d: C[lane / 4][2 (lane % 4) + {0, 1}]).
+__device__ __forceinline__ void mma884(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+// Global -> registers for one kBK slice: each thread holds kBM * kBK / kGemmThreads complex
+// elements of A and kBK * kBN / kGemmThreads of B (zero outside the matrices).
+constexpr int kAPer = kBM * kBK / kGemmThreads;  // 8
+constexpr int kBPer = kBK * kBN / kGemmThreads;  // 8
+
+__device__ __forceinline__ void load_slice(const double2* A, int lda, const double2* B, int ldb,
+                                           int M, int N, int K, int m0, int n0, int k0,
+                                           double2 (&ra)[kAPer], double2 (&rb)[kBPer]) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < kAPer; ++q) {  // A: consecutive threads along m (columns are contiguous)
+    const int e = tid + kGemmThreads * q, m = e % kBM, k = e / kBM;
+    const int gm = m0 + m, gk = k0 + k;
+    ra[q] = (gm < M && gk < K) ? A[gm + (int64_t)lda * gk] : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int q = 0; q < kBPer; ++q) {  // B: consecutive threads along k
+    const int e = tid + kGemmThreads * q, k = e % kBK, n = e / kBK;
+    const int gk = k0 + k, gn = n0 + n;
+    rb[q] = (gk < K && gn < N) ? B[gk + (int64_t)ldb * gn] : make_double2(0.0, 0.0);
+  }
+}
+
+__device__ __forceinline__ void store_slice(GemmSmem& S, int buf, const double2 (&ra)[kAPer],
+                                            const double2 (&rb)[kBPer]) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < kAPer; ++q) {
+    const int e = tid + kGemmThreads * q, m = e % kBM, k = e / kBM;
+    S.ar[buf][k][m] = ra[q].x;
+    S.ai[buf][k][m] = ra[q].y;
+  }
+#pragma unroll
+  for (int q = 0; q < kBPer; ++q) {
+    const int e = tid + kGemmThreads * q, k = e % kBK, n = e / kBK;
+    S.br[buf][n][k] = rb[q].x;
+    S.bi[buf][n][k] = rb[q].y;
+  }
+}
+
+__global__ void __launch_bounds__(kGemmThreads)
+    k_zgemm_nn(int M, int N, int K, double alpha, const double2* A, int lda, int64_t sa,
+               const double2* B, int ldb, int64_t sb, double beta, double2* C, int ldc,
+               int64_t sc) {
+  extern __shared__ __align__(16) unsigned char zg_smem[];
+  GemmSmem& S = *reinterpret_cast<GemmSmem*>(zg_smem);
+  const int64_t z = blockIdx.z;
+  A += sa * z;
+  B += sb * z;
+  C += sc * z;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;  // the warp's 32 x 32 sub-tile
+  const int fr = lane >> 2, fc = lane & 3;                 // fragment row / column indices
+  double re[4][4][2], im[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
+  double2 ra[kAPer], rb[kBPer];
+  load_slice(A, lda, B, ldb, M, N, K, m0, n0, 0, ra, rb);
+  store_slice(S, 0, ra, rb);
+  __syncthreads();
+  const int slices = (K + kBK - 1) / kBK;
+  for (int s = 0; s < slices; ++s) {
+    const int buf = s & 1;
+    if (s + 1 < slices) load_slice(A, lda, B, ldb, M, N, K, m0, n0, (s + 1) * kBK, ra, rb);
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 4) {
+      double a_r[4], a_i[4], a_n[4], b_r[4], b_i[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a_r[i] = S.ar[buf][kk + fc][wm + 8 * i + fr];
+        a_i[i] = S.ai[buf][kk + fc][wm + 8 * i + fr];
+        a_n[i] = -a_i[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        b_r[j] = S.br[buf][wn + 8 * j + fr][kk + fc];
+        b_i[j] = S.bi[buf][wn + 8 * j + fr][kk + fc];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          mma884(re[i][j], a_r[i], b_r[j]);
+          mma884(re[i][j], a_n[i], b_i[j]);
+          mma884(im[i][j], a_r[i], b_i[j]);
+          mma884(im[i][j], a_i[i], b_r[j]);
+        }
+    }
+    if (s + 1 < slices) {
+      store_slice(S, buf ^ 1, ra, rb);
+      __syncthreads();
+    }
+  }
+  // epilogue: C = alpha acc + beta C (beta == 0: C is not read)
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gm = m0 + wm + 8 * i + fr, gn = n0 + wn + 8 * j + 2 * fc + h;
+        if (gm < M && gn < N) {
+          double2* c = C + gm + (int64_t)ldc * gn;
+          double2 v = make_double2(alpha * re[i][j][h], alpha * im[i][j][h]);
+          if (beta != 0.0) {
+            const double2 o = *c;
+            v.x = fma(beta, o.x, v.x);
+            v.y = fma(beta, o.y, v.y);
+          }
+          *c = v;
+        }
+      }
+}
+
+}  // namespace
+
+int zgemm_nn_batched(int M, int N, int K, double alpha, const cuDoubleComplex* A, int lda,
+                     int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
+                     double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
+                     cudaStream_t st) {
+  if (M <= 0 || N <= 0 || batch <= 0) return 0;
+  if (cudaFuncSetAttribute(k_zgemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(GemmSmem)) != cudaSuccess)
+    return check_launch("zgemm attribute");
+  const dim3 grid((M + kBM - 1) / kBM, (N + kBN - 1) / kBN, batch);
+  k_zgemm_nn<<<grid, kGemmThreads, sizeof(GemmSmem), st>>>(
+      M, N, K, alpha, reinterpret_cast<const double2*>(A), lda, stride_a,
+      reinterpret_cast<const double2*>(B), ldb, stride_b, beta, reinterpret_cast<double2*>(C),
+      ldc, stride_c);
+  return check_launch("zgemm");
+}
+
+namespace {
+
+// y = alpha A x + beta y: a CTA of 256 threads takes 32 rows; thread (r, g) sums the columns
+// j = g (mod 8) of row r (a warp reads 32 consecutive rows of one column), the eight partial sums
+// of a row are added in a fixed order through shared memory.
+__global__ void __launch_bounds__(256) k_zgemv_n(int n, double alpha, const double2* A, int lda,
+                                                 int64_t sa, const double2* x, int64_t sx,
+                                                 double beta, double2* y, int64_t sy) {
+  __shared__ double2 part[8][32];
+  const int64_t z = blockIdx.y;
+  A += sa * z;
+  x += sx * z;
+  y += sy * z;
+  const int r = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + r;
+  double sr = 0.0, si = 0.0;
+  if (i < n) {
+    for (int j = g; j < n; j += 8) {
+      const double2 a = A[i + (int64_t)lda * j], v = x[j];
+      sr = fma(a.x, v.x, fma(-a.y, v.y, sr));
+      si = fma(a.x, v.y, fma(a.y, v.x, si));
+    }
+  }
+  part[g][r] = make_double2(sr, si);
+  __syncthreads();
+  if (g == 0 && i < n) {
+    double tr = 0.0, ti = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      tr += part[k][r].x;
+      ti += part[k][r].y;
+    }
+    double2 out = make_double2(alpha * tr, alpha * ti);
+    if (beta != 0.0) {
+      out.x = fma(beta, y[i].x, out.x);
+      out.y = fma(beta, y[i].y, out.y);
+    }
+    y[i] = out;
+  }
+}
+
+// y = alpha A^H x + beta y: one warp per output j (column j of A, read by the lanes in
+// consecutive rows), a fixed shuffle tree adds the lanes' partial sums.
+__global__ void __launch_bounds__(256) k_zgemv_c(int n, double alpha, const double2* A, int lda,
+                                                 int64_t sa, const double2* x, int64_t sx,
+                                                 double beta, double2* y, int64_t sy) {
+  const int64_t z = blockIdx.y;
+  A += sa * z;
+  x += sx * z;
+  y += sy * z;
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const double2* col = A + (int64_t)lda * j;
+  double sr = 0.0, si = 0.0;
+  for (int i = lane; i < n; i += 32) {  // conj(a) v
+    const double2 a = col[i], v = x[i];
+    sr = fma(a.x, v.x, fma(a.y, v.y, sr));
+    si = fma(a.x, v.y, fma(-a.y, v.x, si));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    si += __shfl_xor_sync(0xffffffffu, si, o);
+  }
+  if (lane == 0) {
+    double2 out = make_double2(alpha * sr, alpha * si);
+    if (beta != 0.0) {
+      out.x = fma(beta, y[j].x, out.x);
+      out.y = fma(beta, y[j].y, out.y);
+    }
+    y[j] = out;
+  }
+}
+
+}  // namespace
+
+int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A, int lda,
+                  int64_t stride_a, const cuDoubleComplex* x, int64_t stride_x, double beta,
+                  cuDoubleComplex* y, int64_t stride_y, int batch, cudaStream_t st) {
+  if (n <= 0 || batch <= 0) return 0;
+  const double2* a = reinterpret_cast<const double2*>(A);
+  const double2* v = reinterpret_cast<const double2*>(x);
+  double2* w = reinterpret_cast<double2*>(y);
+  if (conj_trans)
+    k_zgemv_c<<<dim3((n + 7) / 8, batch), 256, 0, st>>>(n, alpha, a, lda, stride_a, v, stride_x,
+                                                        beta, w, stride_y);
+  else
+    k_zgemv_n<<<dim3((n + 31) / 32, batch), 256, 0, st>>>(n, alpha, a, lda, stride_a, v,
+                                                          stride_x, beta, w, stride_y);
+  return check_launch("zgemv");
+}
+
+}  // namespace dense
+}  // namespace eb

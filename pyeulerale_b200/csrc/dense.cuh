@@ -1,0 +1,28 @@
+// Dense complex double products of the ring-block LU (dense.cu): the library's own strided-batched
+// GEMM on the FP64 tensor cores and matrix-vector products, in place of a BLAS library.
+#pragma once
+
+#include <cuComplex.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace eb {
+namespace dense {
+
+// C_z = alpha A_z B_z + beta C_z for z < batch, column-major, A_z = A + z stride_a (elements)
+// etc.; alpha, beta real; beta == 0 does not read C. Returns an EB_* status.
+int zgemm_nn_batched(int M, int N, int K, double alpha, const cuDoubleComplex* A, int lda,
+                     int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
+                     double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
+                     cudaStream_t st);
+
+// y_z = alpha op(A_z) x_z + beta y_z for z < batch, A_z square n x n column-major (lda),
+// op(A) = A (conj_trans = 0) or A^H (conj_trans = 1); alpha, beta real; beta == 0 does not
+// read y. x and y contiguous; strides in elements.
+int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A, int lda,
+                  int64_t stride_a, const cuDoubleComplex* x, int64_t stride_x, double beta,
+                  cuDoubleComplex* y, int64_t stride_y, int batch, cudaStream_t st);
+
+}  // namespace dense
+}  // namespace eb

@@ -26,7 +26,8 @@
 //
 // Batching: the shifts of one call share the instance and the Jacobian; shift s has its own
 // workspace at base + s * stride. Every step of the elimination is one launch for all shifts
-// (grid dimension = shift), the dense GEMMs and GEMVs are cuBLAS strided-batched calls, so the
+// (grid dimension = shift), the dense GEMMs and GEMVs are the library's own strided-batched
+// kernels (dense.cu: complex GEMM on the FP64 tensor cores, GEMV), so the
 // launch count per ring does not grow with the number of shifts. All device memory comes from
 // the caller's workspace.
 //
@@ -38,7 +39,6 @@
 // the pivot rows. After K steps the working array W holds T P (T = product of the elementary
 // transformations), and the inverse is Dinv[j, p_k] = W[p_j, k] (one permuting copy).
 
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,6 +49,7 @@
 #include <vector>
 
 #include "../../include/euler_b200.h"
+#include "dense.cuh"
 #include "physics.cuh"
 
 namespace eb {
@@ -59,11 +60,9 @@ int validate(const eb_batch* b);
 
 namespace rl {
 
-// A cuBLAS handle per concurrent lane (its workspace must not be shared by work that overlaps
-// on the device) and, for the lanes after the first, a stream of this library.
+// For the lanes after the first, a stream of this library and its fork / join events.
 struct Handle {
   int device = -1;
-  cublasHandle_t blas = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   cudaEvent_t start = nullptr;
@@ -74,25 +73,26 @@ struct Handle {
 constexpr int kLanes = 4;
 thread_local Handle g_handle[kLanes];
 
-int blas_handle(cudaStream_t st, cublasHandle_t& out, int lane = 0) {
+// The stream of a lane (lane 0: the caller's stream st), created on first use per device.
+int lane_stream(cudaStream_t st, cudaStream_t& out, int lane = 0) {
+  if (lane == 0) {
+    out = st;
+    return EB_OK;
+  }
   int dev = 0;
   cudaGetDevice(&dev);
   Handle& h = g_handle[lane];
   if (h.device != dev) {
-    if (h.blas) cublasDestroy(h.blas);
-    h.blas = nullptr;
     h.stream = nullptr;  // streams and events of another device are left to that device
     h.done = nullptr;
     h.start = nullptr;
-    if (cublasCreate(&h.blas) != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "cublasCreate failed");
-    if (lane > 0 && (cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking) != cudaSuccess ||
-                     cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) != cudaSuccess ||
-                     cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming) != cudaSuccess))
+    if (cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming) != cudaSuccess)
       return check_launch("ringlu lane stream");
     h.device = dev;
   }
-  cublasSetStream(h.blas, lane > 0 ? h.stream : st);
-  out = h.blas;
+  out = h.stream;
   return EB_OK;
 }
 
@@ -714,10 +714,6 @@ int check_group(const eb_batch* b, int n_shifts, const void* ws, int64_t stride,
   return EB_OK;
 }
 
-int blas_ok(cublasStatus_t st, const char* what) {
-  return st == CUBLAS_STATUS_SUCCESS ? EB_OK : fail(EB_ERR_CUDA, what);
-}
-
 // Panel steps j0 .. j0 + NB - 1 (in -> out) and their update of the columns [c_lo, c_hi).
 template <int NB, int ROWS>
 void gj_pass(const Group& g, int j0, int c_lo, int c_hi, size_t off_in, size_t off_out,
@@ -747,7 +743,7 @@ void gj_pass_any(const Group& g, int nb, int rows, int j0, int c_lo, int c_hi, s
 // the panels of a block update only the block's columns (an even number of passes, so the
 // block ends in D_m), and the rest of D_m takes the block's combined rank-kGjBlock update as
 // strided-batched ZGEMMs (tensor-core DMMA) instead of kGjBlock / nb streaming passes.
-int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int side_lane) {
+int invert_ring(const Group& g, int m, cudaStream_t st, int side_lane) {
   const Layout& L = g.L;
   const int K = L.K, nb = panel_width(K), rows = (K + kPanelThreads - 1) / kPanelThreads;
   const size_t buf[2] = {g.boff(L.off_D, m), L.off_T};
@@ -761,21 +757,18 @@ int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int si
     // next block's panels; its update of every other column runs on the side stream, under
     // those panels. st waits for the side stream before it moves the next pivot rows (which
     // reads and zeroes rows of those columns and overwrites R) and at the end.
-    cublasHandle_t hs = nullptr;
-    int rc = blas_handle(st, hs, side_lane);
+    cudaStream_t hs = nullptr;
+    int rc = lane_stream(st, hs, side_lane);
     if (rc != EB_OK) return rc;
     Handle& side = g_handle[side_lane];
-    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
     const int64_t es = g.es();
     cuDoubleComplex* W = g.blk(L.off_D, m);
     cuDoubleComplex* Rp = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_Rp);
-    auto update = [&](cublasHandle_t hh, int c_lo, int c_hi, int b0) {
+    auto update = [&](cudaStream_t hh, int c_lo, int c_hi, int b0) {
       if (c_hi <= c_lo) return EB_OK;
-      return blas_ok(cublasZgemmStridedBatched(hh, CUBLAS_OP_N, CUBLAS_OP_N, K, c_hi - c_lo,
-                                               kGjBlock, &one, W + (size_t)K * b0, K, es,
-                                               Rp + (size_t)kGjBlock * c_lo, kGjBlock, es, &one,
-                                               W + (size_t)K * c_lo, K, es, g.S),
-                     "ringlu: gemm Gauss-Jordan block update");
+      return dense::zgemm_nn_batched(K, c_hi - c_lo, kGjBlock, 1.0, W + (size_t)K * b0, K, es,
+                                     Rp + (size_t)kGjBlock * c_lo, kGjBlock, es, 1.0,
+                                     W + (size_t)K * c_lo, K, es, g.S, hh);
     };
     bool side_busy = false;
     for (int b0 = 0; b0 < K; b0 += kGjBlock) {
@@ -787,7 +780,7 @@ int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int si
       k_gj_take_pivot_rows<<<dim3(K, g.S), 64, 0, st>>>(K, b0, kGjBlock, g.base, g.stride, buf[0],
                                                         L.off_Rp, L.off_perm, L.off_info);
       const int n0 = b0 + kGjBlock, n1 = std::min(K, b0 + 2 * kGjBlock);  // the next block
-      if ((rc = update(h, n0, n1, b0)) != EB_OK) return rc;
+      if ((rc = update(st, n0, n1, b0)) != EB_OK) return rc;
       if (cudaEventRecord(side.start, st) != cudaSuccess ||
           cudaStreamWaitEvent(side.stream, side.start, 0) != cudaSuccess)
         return check_launch("ringlu side fork");
@@ -811,36 +804,30 @@ int invert_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int si
 }
 
 // One ring of the block elimination for every shift of the group.
-int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int side_lane) {
+int factor_ring(const Group& g, int m, cudaStream_t st, int side_lane) {
   const Layout& L = g.L;
   const int M = L.M, K = L.K, N = L.N;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
-  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
   const int64_t es = g.es();
-  int rc = invert_ring(g, h, m, st, side_lane);
+  int rc = invert_ring(g, m, st, side_lane);
   if (rc != EB_OK) return rc;
   if (m + 1 < M) {
     // T = L1[m+1] = B1'[m+1] Dinv_m;  D[m+1] -= T C1'[m]
-    if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &one,
-                                                g.blk(L.off_L1, m + 1), K, es, g.blk(L.off_D, m), K, es,
-                                                &zero, g.blk(L.off_T, 0), K, es, g.S),
-                      "ringlu: gemm L1")) != EB_OK)
+    if ((rc = dense::zgemm_nn_batched(K, K, K, 1.0, g.blk(L.off_L1, m + 1), K, es,
+                                      g.blk(L.off_D, m), K, es, 0.0, g.blk(L.off_T, 0), K, es,
+                                      g.S, st)) != EB_OK)
       return rc;
-    if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone,
-                                                g.blk(L.off_T, 0), K, es, g.blk(L.off_C1, m), K, es,
-                                                &one, g.blk(L.off_D, m + 1), K, es, g.S),
-                      "ringlu: gemm D1")) != EB_OK)
+    if ((rc = dense::zgemm_nn_batched(K, K, K, -1.0, g.blk(L.off_T, 0), K, es,
+                                      g.blk(L.off_C1, m), K, es, 1.0, g.blk(L.off_D, m + 1), K,
+                                      es, g.S, st)) != EB_OK)
       return rc;
   }
   if (m + 2 < M) {
     // L2[m+2] = B2[m+2] Dinv_m (scratch);  B1'[m+2] -= L2[m+2] C1'[m]
     k_bd_left<<<dim3(N, g.S), 256, 0, st>>>(K, g.base, g.stride, L.off_B2 + L.bdr * (m + 2),
                                             g.boff(L.off_D, m), L.off_L2);
-    if ((rc = blas_ok(cublasZgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, K, K, K, &mone,
-                                                g.blk(L.off_L2, 0), K, es, g.blk(L.off_C1, m), K, es,
-                                                &one, g.blk(L.off_L1, m + 2), K, es, g.S),
-                      "ringlu: gemm L1 update")) != EB_OK)
+    if ((rc = dense::zgemm_nn_batched(K, K, K, -1.0, g.blk(L.off_L2, 0), K, es,
+                                      g.blk(L.off_C1, m), K, es, 1.0, g.blk(L.off_L1, m + 2), K,
+                                      es, g.S, st)) != EB_OK)
       return rc;
     // D[m+2] -= L2[m+2] C2[m];  C1'[m+1] -= L1[m+1] C2[m]
     k_bd_right<<<dim3(N, g.S, 2), 256, 0, st>>>(K, g.base, g.stride, L.off_C2 + L.bdr * m,
@@ -859,12 +846,9 @@ int factor_ring(const Group& g, cublasHandle_t h, int m, cudaStream_t st, int si
 // A = Lt Ut with L2[m] = B2[m] Dinv_{m-2}, so the forward sweep keeps w[m] = Dinv_m y[m] of the
 // finished rings and subtracts B2[m] w[m-2]; the adjoint sweep applies L2[m+2]^H as
 // Dinv_m^H (B2[m+2]^T x[m+2]).
-int ring_solve(const Group& g, cublasHandle_t h, bool adjoint, cudaStream_t stream) {
+int ring_solve(const Group& g, bool adjoint, cudaStream_t stream) {
   const Layout& L = g.L;
   const int M = L.M, K = L.K, N = L.N;
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  const cuDoubleComplex zero = make_cuDoubleComplex(0.0, 0.0);
-  const cuDoubleComplex mone = make_cuDoubleComplex(-1.0, 0.0);
   const int64_t es = g.es();
   cuDoubleComplex* y = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_y);
   cuDoubleComplex* x = reinterpret_cast<cuDoubleComplex*>(g.base + L.off_x);
@@ -873,45 +857,46 @@ int ring_solve(const Group& g, cublasHandle_t h, bool adjoint, cudaStream_t stre
   auto xv = [&](int m) { return x + (size_t)K * m; };
   auto wv = [&](int m) { return w + (size_t)K * m; };
   const size_t vb = sizeof(cuDoubleComplex) * (size_t)K;  // bytes of one ring vector
-  auto gemv = [&](cublasOperation_t op, const cuDoubleComplex* alpha, const cuDoubleComplex* A,
-                  const cuDoubleComplex* v, const cuDoubleComplex* beta, cuDoubleComplex* out) {
-    return cublasZgemvStridedBatched(h, op, K, K, alpha, A, K, es, v, 1, es, beta, out, 1, es, g.S);
+  const int kN = 0, kH = 1;  // op(A) = A, A^H
+  auto gemv = [&](int op, double alpha, const cuDoubleComplex* A, const cuDoubleComplex* v,
+                  double beta, cuDoubleComplex* out) {
+    return dense::zgemv_batched(op, K, alpha, A, K, es, v, es, beta, out, es, g.S, stream);
   };
   const dim3 bdg((4 * N + 127) / 128, g.S);
   // out -= Bd v (trans: Bd^T v), ring vectors given by workspace offsets; assign: out = -Bd v
   auto bdvec = [&](size_t off_bd, size_t off_v, size_t off_out, int trans, int assign) {
     k_bd_vec<<<bdg, 128, 0, stream>>>(N, g.base, g.stride, off_bd, off_v, off_out, trans, assign);
   };
-  cublasStatus_t st = CUBLAS_STATUS_SUCCESS;
-  auto run = [&](cublasStatus_t s) {
-    if (s != CUBLAS_STATUS_SUCCESS) st = s;
+  int st = EB_OK;
+  auto run = [&](int s) {
+    if (s != EB_OK) st = s;
   };
   if (!adjoint) {
     for (int m = 0; m < M; ++m) {  // Lt z = b (z in y), w[m] = Dinv_m z[m]
-      if (m >= 1) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_L1, m), yv(m - 1), &one, yv(m)));
+      if (m >= 1) run(gemv(kN, -1.0, g.blk(L.off_L1, m), yv(m - 1), 1.0, yv(m)));
       if (m >= 2) bdvec(L.off_B2 + L.bdr * m, L.off_w + vb * (m - 2), L.off_y + vb * m, 0, 0);
-      if (m + 2 < M) run(gemv(CUBLAS_OP_N, &one, g.blk(L.off_D, m), yv(m), &zero, wv(m)));
+      if (m + 2 < M) run(gemv(kN, 1.0, g.blk(L.off_D, m), yv(m), 0.0, wv(m)));
     }
     for (int m = M - 1; m >= 0; --m) {  // Ut x = z
-      if (m + 1 < M) run(gemv(CUBLAS_OP_N, &mone, g.blk(L.off_C1, m), xv(m + 1), &one, yv(m)));
+      if (m + 1 < M) run(gemv(kN, -1.0, g.blk(L.off_C1, m), xv(m + 1), 1.0, yv(m)));
       if (m + 2 < M) bdvec(L.off_C2 + L.bdr * m, L.off_x + vb * (m + 2), L.off_y + vb * m, 0, 0);
-      run(gemv(CUBLAS_OP_N, &one, g.blk(L.off_D, m), yv(m), &zero, xv(m)));
+      run(gemv(kN, 1.0, g.blk(L.off_D, m), yv(m), 0.0, xv(m)));
     }
   } else {
     for (int m = 0; m < M; ++m) {  // Ut^H z = b (z in x)
-      if (m >= 1) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_C1, m - 1), xv(m - 1), &one, yv(m)));
+      if (m >= 1) run(gemv(kH, -1.0, g.blk(L.off_C1, m - 1), xv(m - 1), 1.0, yv(m)));
       if (m >= 2) bdvec(L.off_C2 + L.bdr * (m - 2), L.off_x + vb * (m - 2), L.off_y + vb * m, 1, 0);
-      run(gemv(CUBLAS_OP_C, &one, g.blk(L.off_D, m), yv(m), &zero, xv(m)));
+      run(gemv(kH, 1.0, g.blk(L.off_D, m), yv(m), 0.0, xv(m)));
     }
     for (int m = M - 1; m >= 0; --m) {  // Lt^H x = z
-      if (m + 1 < M) run(gemv(CUBLAS_OP_C, &mone, g.blk(L.off_L1, m + 1), xv(m + 1), &one, xv(m)));
+      if (m + 1 < M) run(gemv(kH, -1.0, g.blk(L.off_L1, m + 1), xv(m + 1), 1.0, xv(m)));
       if (m + 2 < M) {  // x[m] -= Dinv_m^H (B2[m+2]^T x[m+2]), with w[m] = -B2[m+2]^T x[m+2]
         bdvec(L.off_B2 + L.bdr * (m + 2), L.off_x + vb * (m + 2), L.off_w + vb * m, 1, 1);
-        run(gemv(CUBLAS_OP_C, &one, g.blk(L.off_D, m), wv(m), &one, xv(m)));
+        run(gemv(kH, 1.0, g.blk(L.off_D, m), wv(m), 1.0, xv(m)));
       }
     }
   }
-  if (st != CUBLAS_STATUS_SUCCESS) return fail(EB_ERR_CUDA, "ringlu: gemv failed");
+  if (st != EB_OK) return st;
   return check_launch("ring solve");
 }
 
@@ -940,9 +925,7 @@ namespace rl {
 int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
   const Layout& L = g.L;
   const int M = L.M, N = L.N, n_shifts = g.S;
-  cublasHandle_t h = nullptr;
-  int rc = blas_handle(st, h);
-  if (rc != EB_OK) return rc;
+  int rc = EB_OK;
   for (int s = 0; s < n_shifts; ++s) {
     char* w = g.base + (int64_t)s * g.stride;
     cudaMemsetAsync(w, 0, L.off_T, st);  // the stored super-blocks and block diagonals
@@ -956,13 +939,13 @@ int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
   if ((rc = check_launch("ringlu assemble")) != EB_OK) return rc;
   if (n_shifts == 1) {
     for (int m = 0; m < M; ++m)
-      if ((rc = factor_ring(g, h, m, st, 2)) != EB_OK) return rc;
+      if ((rc = factor_ring(g, m, st, 2)) != EB_OK) return rc;
     return EB_OK;
   }
   // Two halves of the shifts on two streams, ring by ring: one half's latency-bound
   // Gauss-Jordan panels overlap the other half's GEMMs on the rest of the GPU.
-  cublasHandle_t h2 = nullptr;
-  if ((rc = blas_handle(st, h2, 1)) != EB_OK) return rc;
+  cudaStream_t s2 = nullptr;
+  if ((rc = lane_stream(st, s2, 1)) != EB_OK) return rc;
   const Handle& lane = g_handle[1];
   const int s1 = (n_shifts + 1) / 2;
   const Group g1{L, g.base, g.stride, s1};
@@ -970,8 +953,8 @@ int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
   cudaEventRecord(lane.start, st);
   cudaStreamWaitEvent(lane.stream, lane.start, 0);
   for (int m = 0; m < M; ++m) {
-    if ((rc = factor_ring(g1, h, m, st, 2)) != EB_OK) return rc;
-    if ((rc = factor_ring(g2, h2, m, lane.stream, 3)) != EB_OK) return rc;
+    if ((rc = factor_ring(g1, m, st, 2)) != EB_OK) return rc;
+    if ((rc = factor_ring(g2, m, s2, 3)) != EB_OK) return rc;
   }
   cudaEventRecord(lane.done, lane.stream);
   cudaStreamWaitEvent(st, lane.done, 0);
@@ -979,7 +962,7 @@ int issue_factor(const Group& g, const double* const* J, cudaStream_t st) {
 }
 
 // Captured factorisations: the first call with a given (device, workspace, stride, sizes,
-// Jacobian pointers) runs eagerly (cuBLAS initialises outside any capture), the second
+// Jacobian pointers) runs eagerly (kernel attributes are set outside any capture), the second
 // captures the launch sequence into a CUDA graph, later ones replay it. A few graphs are kept
 // per thread (least recently used first out). EB_RINGLU_GRAPHS=0 turns capture off.
 struct GraphKey {
@@ -1103,8 +1086,6 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
       return fail(EB_ERR_ARG, "ringlu: rhs and x must be 16-byte aligned");
   }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  cublasHandle_t h = nullptr;
-  if ((rc = blas_handle(st, h)) != EB_OK) return rc;
   const Group g{L, static_cast<char*>(const_cast<void*>(workspace)), workspace_stride, n_shifts};
   const int M = L.M, N = L.N;
   const int gc = grid_for((int64_t)M * N, 128);
@@ -1116,7 +1097,7 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
     for (int s = 0; s < n_shifts; ++s)
       k_to_rings<<<gc, 128, 0, st>>>(M, N, it == 0 ? rhs[s] : reinterpret_cast<double*>(ws(s) + L.off_r),
                                      reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_y));
-    if ((rc = ring_solve(g, h, adjoint != 0, st)) != EB_OK) return rc;
+    if ((rc = ring_solve(g, adjoint != 0, st)) != EB_OK) return rc;
     for (int s = 0; s < n_shifts; ++s) {
       double* a = reinterpret_cast<double*>(ws(s) + L.off_acc);
       k_from_rings<<<gc, 128, 0, st>>>(M, N, reinterpret_cast<cuDoubleComplex*>(ws(s) + L.off_x), x[s],
@@ -1346,13 +1327,11 @@ int issue_ptc_step(const eb_batch* b, const PtcLayout& P, char* ws, const double
   if ((rc = eb_compute_odes_wrt_states(b, X, V, U, J, st)) != EB_OK) return rc;
   const double* js[1] = {J};
   if ((rc = issue_factor(g, js, st)) != EB_OK) return rc;
-  cublasHandle_t h = nullptr;
-  if ((rc = blas_handle(st, h)) != EB_OK) return rc;
   k_ptc_rhs<<<gc, 128, 0, st>>>(M, N, R, ctl, y);
-  if ((rc = ring_solve(g, h, false, st)) != EB_OK) return rc;
+  if ((rc = ring_solve(g, false, st)) != EB_OK) return rc;
   k_ptc_refine_rhs<<<gc, 128, 0, st>>>(M, N, J, shift, x, R, ctl, xs, r);
   k_to_rings<<<gc, 128, 0, st>>>(M, N, r, y);
-  if ((rc = ring_solve(g, h, false, st)) != EB_OK) return rc;
+  if ((rc = ring_solve(g, false, st)) != EB_OK) return rc;
   k_ptc_update<<<gc, 128, 0, st>>>(M, N, x, xs, reinterpret_cast<int*>(lw + P.lu.off_info), ctl,
                                    U);
   return check_launch("ptc step");
@@ -1455,7 +1434,7 @@ int eb_ptc_run(const eb_batch* b, const double* X, const double* V, double* U, d
   }
   done_h[0] = done_h[1] = 0;
   for (int k = 0; k < max_steps; ++k) {
-    if (k == 0) {  // eagerly (cuBLAS and the kernels initialise outside any capture)
+    if (k == 0) {  // eagerly (the autotuner times its variants outside any capture)
       rc = issue_ptc_step(b, P, ws, X, V, U, R, J, ser, rtol, st);
     } else {
       if (!exec) {
