@@ -28,6 +28,7 @@
 // A complex cotangent (the reference's complex vectors) is two real products: the CTA pair
 // 2 t + h of tile t carries part h.
 
+#include "autotune.cuh"
 #include "common.cuh"
 #include "tile_faces_rev.cuh"
 
@@ -284,7 +285,10 @@ __device__ __forceinline__ void clear(FaceAdj& A) {
   A.wl = A.wr = 0.0;
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+// MinBlocks = 2: capped at 128 registers (with spills) so that two CTAs share an SM;
+// MinBlocks = 1: no cap, one CTA per SM. The same code, so the two give identical results.
+template <int MinBlocks>
+__global__ void __launch_bounds__(kThreads, MinBlocks)
     k_residual_adjoint(Table t, const double* X, const double* V, const double* U,
                        const double* W, int cstride, double* gU, double* gX, double* gV) {
   extern __shared__ __align__(16) unsigned char adj_smem[];
@@ -674,14 +678,20 @@ extern "C" int eb_apply_odes_adjoint(const eb_batch* b, const double* X, const d
   const Table t = make_table(b);
   const int cs = is_complex ? 2 : 1;
   cudaStream_t st = EB_STREAM(stream);
-  if (cudaFuncSetAttribute(adj::k_residual_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(adj::Smem)) != cudaSuccess)
-    return check_launch("apply_odes_adjoint attribute");
   if (d_states || d_vertices || d_velocities) {
-    adj::k_residual_adjoint<<<dim3(cs * adj::tiles(dim, dim), b->n_inst), adj::kThreads,
-                              sizeof(adj::Smem), st>>>(t, X, V, U, w, cs, d_states, d_vertices,
-                                                       d_velocities);
-    if (int rc = check_launch("apply_odes_adjoint")) return rc;
+    auto launch = [&](int v) {
+      auto kernel = v == 0 ? adj::k_residual_adjoint<2> : adj::k_residual_adjoint<1>;
+      if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(adj::Smem)) != cudaSuccess)
+        return check_launch("apply_odes_adjoint attribute");
+      kernel<<<dim3(cs * adj::tiles(dim, dim), b->n_inst), adj::kThreads, sizeof(adj::Smem),
+               st>>>(t, X, V, U, w, cs, d_states, d_vertices, d_velocities);
+      return check_launch("apply_odes_adjoint");
+    };
+    static const char* const kNames[2] = {"2 CTAs/SM (128 registers)", "1 CTA/SM"};
+    if (int rc = tune::launch_tuned(is_complex ? "residual_adjoint complex" : "residual_adjoint",
+                                    b->n_cells, dim, 2, 0, kNames, st, launch))
+      return rc;
   }
   if (d_mach) {
     adj::k_mach_adjoint<<<b->n_inst, 256, 0, st>>>(t, X, V, U, w, cs, d_mach);

@@ -420,3 +420,26 @@ def test_states_jacobian_variants_agree_and_autotune(cuda, golden_grids, monkeyp
     report = _lib.autotune_report()
     line = [s for s in report.splitlines() if f"jac_states_tiled ({gpu.M * gpu.N}," in s]
     assert line and "width 4" in line[0] and "width 2" in line[0] and "(kept)" in line[0]
+
+
+def test_adjoint_variants_agree(cuda, golden_grids, monkeypatch):
+    """The two occupancy variants of the matrix-free adjoint (two CTAs per SM at 128 registers,
+    one CTA per SM uncapped) give bit-identical products, and the autotuner lists its choice."""
+    from pyeulerale_b200 import _lib
+
+    case = make_case("naca0012_33", golden_grids, seed=3)
+    gpu = Gpu(cuda, case)
+    w = crandn(np.random.default_rng(31), (4, gpu.M, gpu.N))
+    out = []
+    for v in ("v0", "v1"):
+        monkeypatch.setenv("EB_AUTOTUNE", v)
+        out.append(run_adjoint(gpu, w))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+    monkeypatch.delenv("EB_AUTOTUNE")
+    for a, b in zip(run_adjoint(gpu, w), out[0]):
+        np.testing.assert_array_equal(a, b)
+    report = _lib.autotune_report()
+    line = [s for s in report.splitlines()
+            if f"residual_adjoint complex ({gpu.M * gpu.N}," in s]
+    assert line and "1 CTA/SM" in line[0] and "(kept)" in line[0]
