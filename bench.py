@@ -442,6 +442,43 @@ def cpu_second_order_rate(X, V, U, mach: float) -> dict:
 
 # ---- B200 arm -------------------------------------------------------------------------------
 
+def time_zgemm(K: int, batch: int, stream, sp, reps: int = 10) -> dict:
+    """The ring LU's dense product at its factorisation shape (K x K x K complex, batch shifts):
+    the library's two GEMM variants (eb_zgemm_strided_batched) and, for comparison only, the
+    BLAS product torch.matmul issues on the same shape."""
+    import torch
+    from pyeulerale_b200 import _lib
+
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A, B, C = (torch.randn(batch, K, K, dtype=torch.complex128, device="cuda", generator=g)
+               for _ in range(3))
+    flops = 8.0 * K ** 3 * batch
+    out = {"shape": f"{K}x{K}x{K} complex, batch {batch}", "flops_per_call": flops}
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    for v, name in ((0, "register_staged"), (1, "cp_async")):
+        def call(v=v):
+            _lib.call("eb_zgemm_strided_batched", K, K, K, -1.0, A.data_ptr(), K, K * K,
+                      B.data_ptr(), K, K * K, 1.0, C.data_ptr(), K, K * K, batch, v, sp)
+        t = timed(call)
+        out[name] = {"ms": t * 1e3, "tflops": flops / t / 1e12}
+    with torch.cuda.stream(stream):
+        t = timed(lambda: torch.matmul(A, B, out=C))
+    out["blas_torch_matmul"] = {"ms": t * 1e3, "tflops": flops / t / 1e12,
+                                "note": "library comparison only; not on the product path"}
+    return out
+
+
 def read_traffic() -> float | None:
     """DRAM bytes per residual launch from the committed ncu summary, scaled per cell."""
     if not PROFILE_SUMMARY.exists():
@@ -540,6 +577,17 @@ def run_b200(args) -> None:
     barrier()
     t_fma = f0.elapsed_time(f1) / 1e3 / 5
     fp64_peak_tflops = 2.0 * 8 * sms * 256 * 8 * fma_iters / t_fma / 1e12
+    # FP64 tensor-core throughput (the dense products' denominator): the library's DMMA probe
+    mma_iters = 20_000
+    for _ in range(3):
+        _lib.call("eb_fp64_mma_probe", mma_iters, sms, sink.data_ptr(), sp)
+    f0.record(stream)
+    for _ in range(5):
+        _lib.call("eb_fp64_mma_probe", mma_iters, sms, sink.data_ptr(), sp)
+    f1.record(stream)
+    barrier()
+    t_mma = f0.elapsed_time(f1) / 1e3 / 5
+    fp64_mma_tflops = 512.0 * 8 * (4 * sms * 256 // 32) * mma_iters / t_mma / 1e12
 
     # end to end through the C ABI with host buffers: every step copies its inputs (X, V, U)
     # from pinned host memory and its result R back. Serial: one stream, copies and launch in
@@ -897,6 +945,7 @@ def run_b200(args) -> None:
                        "seconds": t_ptc},
                "method": "ring-block LU (batched Gauss-Jordan ring inversions + strided-batched "
                          "ZGEMM), refined to 1e-10 relative residual"}
+        res["dense_products"] = time_zgemm(4 * sd_cols, min(group, 16), stream, sp)
         if rank == 0 and not args.no_cpu_baseline:
             res["cpu_reference_method"] = cpu_resolvent_rate(
                 sd.vertices, sd.velocities, sd.states, FLOW["mach"],
@@ -1035,7 +1084,10 @@ def run_b200(args) -> None:
         "autotune": _lib.autotune_report().splitlines(),
         "fp64_peak": {"tflops": fp64_peak_tflops, "sms": sms,
                       "probe": "eb_fp64_fma_probe: 8 CTAs x 256 threads per SM, 8 independent "
-                               f"DFMA chains of {fma_iters} per thread, CUDA events"},
+                               f"DFMA chains of {fma_iters} per thread, CUDA events",
+                      "mma_tflops": fp64_mma_tflops,
+                      "mma_probe": "eb_fp64_mma_probe: 4 CTAs x 8 warps per SM, 8 independent "
+                                   f"m8n8k4 FP64 accumulators of {mma_iters} MMAs per warp"},
         "second_order": second,
         "resolvent": res,
         "uneven": uneven,

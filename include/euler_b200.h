@@ -305,6 +305,22 @@ int eb_ringlu_solve_many(const eb_batch* b, const double* const* J, int n_shifts
  * counterpart in the reference. */
 int eb_fp64_fma_probe(int64_t iterations, int sms, double* sink, void* stream);
 
+/* FP64 tensor-core throughput probe (the denominator of the dense ring-LU products): 4 * sms
+ * CTAs of 256 threads, each warp 8 independent accumulators updated `iterations` times by
+ * mma.sync.m8n8k4.f64 (512 flops each). No counterpart in the reference. */
+int eb_fp64_mma_probe(int64_t iterations, int sms, double* sink, void* stream);
+
+/* The ring LU's dense product as a library call: C_z = alpha A_z B_z + beta C_z for z < batch,
+ * complex double (interleaved), column-major, no transposes, A_z = A + z stride_a complex
+ * elements (likewise B, C); alpha and beta real, beta == 0 does not read C. variant: -1 the
+ * default, 0 the register-staged double buffer, 1 the cp.async three-stage ring (identical
+ * results). In the reference the dense products of its solves are SuperLU's and BLAS's
+ * (core.py:533-599). */
+int eb_zgemm_strided_batched(int M, int N, int K, double alpha, const double* A, int lda,
+                             int64_t stride_a, const double* B, int ldb, int64_t stride_b,
+                             double beta, double* C, int ldc, int64_t stride_c, int batch,
+                             int variant, void* stream);
+
 /* ---- launch-variant autotuner -------------------------------------------------------------- */
 
 /* Kernels with several launch variants of identical results (the states Jacobian: dual width 4

@@ -110,6 +110,9 @@ _SIGNATURES: dict[str, list] = {
     "eb_apply_pressure_coefficients_wrt_states_fwd": ["b", "p", "p", "p", "s"],
     "eb_bsr_shifted_spmv": ["i64", "p", "p", "p", "d", "d", "p", "p", "s"],
     "eb_fp64_fma_probe": ["i64", "i", "p", "s"],
+    "eb_fp64_mma_probe": ["i64", "i", "p", "s"],
+    "eb_zgemm_strided_batched": ["i", "i", "i", "d", "p", "i", "i64", "p", "i", "i64", "d", "p",
+                                 "i", "i64", "i", "i", "s"],
     "eb_odes_wrt_mach_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],
     "eb_odes_wrt_states_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],
     "eb_odes_wrt_vertices_dir": ["b", "p", "p", "p", "i", "p", "p", "p", "s"],

@@ -45,7 +45,6 @@ constexpr int kQCells = kQR * kQC;
 constexpr int kAR = kTM + 1, kAC = kTN + 3;        // angular faces: rows [-1, kTM), cols [-1, kTN+2)
 constexpr int kRR = kTM + 3, kRC = kTN + 2;        // radial faces: rows [-1, kTM+2), cols [-1, kTN]
 constexpr int kNA = kAR * kAC, kNR = kRR * kRC;
-constexpr int kRounds = (kNA + kNR + kThreads - 1) / kThreads;
 constexpr int kER = kTM + 1, kEC = kTN + 1;        // cells whose area adjoint is formed: [-1, k)
 constexpr int kECells = kER * kEC;
 
@@ -370,18 +369,26 @@ __global__ void __launch_bounds__(kThreads, MinBlocks)
   }
   __syncthreads();
 
-  // 3. faces in reverse, kRounds rounds of one face per thread
-  for (int round = 0; round < kRounds; ++round) {
+  // 3. faces in reverse, one face per thread and round. The face lists span the tile's part
+  // inside the grid (tm x tn cells): angular faces of rows [-1, tm) x columns [-1, tn + 2),
+  // radial faces of rows [-1, tm + 2) x columns [-1, tn], the full lists (kNA + kNR faces, three
+  // rounds) for a full tile. The faces a partial tile leaves out reach no owned state, vertex or
+  // cell; their slots keep the zeros of phase 1.
+  const int tm = min(kTM, M - m0), tn = min(kTN, N - n0);
+  const int a_rows = tm + 1, r_rows = tm + 3;
+  const int na = a_rows * (tn + 3), nr = r_rows * (tn + 2);
+  const int rounds = (na + nr + kThreads - 1) / kThreads;
+  for (int round = 0; round < rounds; ++round) {
     const int f = tid + kThreads * round;
-    const bool angular = f < kNA;
-    const bool radial = !angular && f < kNA + kNR;
+    const bool angular = f < na;
+    const bool radial = !angular && f < na + nr;
     int fr = 0, fc = 0;
     if (angular) {
-      fr = f % kAR - 1;
-      fc = f / kAR - 1;
+      fr = f % a_rows - 1;
+      fc = f / a_rows - 1;
     } else if (radial) {
-      fr = (f - kNA) % kRR - 1;
-      fc = (f - kNA) / kRR - 1;
+      fr = (f - na) % r_rows - 1;
+      fc = (f - na) / r_rows - 1;
     }
     const int fm = m0 + fr;
     FaceAdj A;

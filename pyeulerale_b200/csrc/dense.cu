@@ -9,25 +9,32 @@
 // The kBK-deep slices of A and B go through shared memory as separate real / imaginary planes,
 // two slices in flight (the next slice's global loads are issued before the current slice's
 // MMAs). Edges (sizes not multiples of the tile) load zeros and store under bounds checks.
+// A second variant (kAsync) moves the slices with cp.async into a three-stage ring of shared
+// buffers that keep each complex element's two parts together (one 16-byte fragment load gives
+// both), with no register staging; it issues the same MMAs in the same order, so the two
+// variants give identical results.
 
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "../../include/euler_b200.h"
 #include "dense.cuh"
 
 namespace eb {
 
 int check_launch(const char* what);
+int fail(int code, const char* msg);
 
 namespace dense {
 namespace {
 
 constexpr int kBM = 64, kBN = 64, kBK = 16;
 constexpr int kGemmThreads = 128;
-// Shared-memory pitches (doubles) of the A planes [k][m] and B planes [n][k], chosen so that a
-// warp's fragment loads (4 k x 8 m, and 8 n x 4 k) fall on distinct banks within each half.
-constexpr int kPadM = kBM + 8;
+// Shared-memory pitches (doubles) of the A planes [k][m] and B planes [n][k], 4 modulo 16, so
+// that a warp's fragment loads (4 k x 8 m, and 8 n x 4 k) fall on distinct banks within each
+// half-warp.
+constexpr int kPadM = kBM + 4;
 constexpr int kPadK = kBK + 4;
 
 struct GemmSmem {
@@ -161,18 +168,140 @@ __global__ void __launch_bounds__(kGemmThreads)
       }
 }
 
+// ---- cp.async variant -------------------------------------------------------------------
+constexpr int kStages = 3;
+// pitches in complex elements: A rows [k][m] 2 modulo 8, B rows [n][k] 4 modulo 8, so that the
+// 16-byte fragment loads of each quarter-warp fall on distinct banks
+constexpr int kPitchA = kBM + 2;
+constexpr int kPitchB = kBK + 4;
+
+struct AsyncSmem {
+  double2 a[kStages][kBK][kPitchA];
+  double2 b[kStages][kBN][kPitchB];
+};
+
+// 16-byte global -> shared copy; valid == false fills zeros (src is then not read).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int Pending>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(Pending) : "memory");
+}
+
+__global__ void __launch_bounds__(kGemmThreads)
+    k_zgemm_nn_async(int M, int N, int K, double alpha, const double2* A, int lda, int64_t sa,
+                     const double2* B, int ldb, int64_t sb, double beta, double2* C, int ldc,
+                     int64_t sc) {
+  extern __shared__ __align__(16) unsigned char zg_smem[];
+  AsyncSmem& S = *reinterpret_cast<AsyncSmem*>(zg_smem);
+  const int64_t z = blockIdx.z;
+  A += sa * z;
+  B += sb * z;
+  C += sc * z;
+  const int tid = threadIdx.x;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  const int fr = lane >> 2, fc = lane & 3;
+  double re[4][4][2], im[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
+  const int slices = (K + kBK - 1) / kBK;
+  // slice s into buffer s % kStages (one commit group per call, empty past the last slice)
+  auto issue = [&](int s) {
+    if (s < slices) {
+      const int buf = s % kStages, k0 = s * kBK;
+#pragma unroll
+      for (int q = 0; q < kAPer; ++q) {  // A: consecutive threads along m
+        const int e = tid + kGemmThreads * q, m = e % kBM, k = e / kBM;
+        const int gm = m0 + m, gk = k0 + k;
+        const bool ok = gm < M && gk < K;
+        cp_async16(&S.a[buf][k][m], ok ? A + gm + (int64_t)lda * gk : A, ok);
+      }
+#pragma unroll
+      for (int q = 0; q < kBPer; ++q) {  // B: consecutive threads along k
+        const int e = tid + kGemmThreads * q, k = e % kBK, n = e / kBK;
+        const int gk = k0 + k, gn = n0 + n;
+        const bool ok = gk < K && gn < N;
+        cp_async16(&S.b[buf][n][k], ok ? B + gk + (int64_t)ldb * gn : B, ok);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) issue(s);
+  for (int s = 0; s < slices; ++s) {
+    cp_async_wait<kStages - 2>();  // slice s has landed (this thread's copies)
+    __syncthreads();               // ... everyone's; and slice s - 1's buffer is free
+    issue(s + kStages - 1);
+    const int buf = s % kStages;
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 4) {
+      double2 a[4], b[4];
+      double a_n[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a[i] = S.a[buf][kk + fc][wm + 8 * i + fr];
+        a_n[i] = -a[i].y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = S.b[buf][wn + 8 * j + fr][kk + fc];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          mma884(re[i][j], a[i].x, b[j].x);
+          mma884(re[i][j], a_n[i], b[j].y);
+          mma884(im[i][j], a[i].x, b[j].y);
+          mma884(im[i][j], a[i].y, b[j].x);
+        }
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gm = m0 + wm + 8 * i + fr, gn = n0 + wn + 8 * j + 2 * fc + h;
+        if (gm < M && gn < N) {
+          double2* c = C + gm + (int64_t)ldc * gn;
+          double2 v = make_double2(alpha * re[i][j][h], alpha * im[i][j][h]);
+          if (beta != 0.0) {
+            const double2 o = *c;
+            v.x = fma(beta, o.x, v.x);
+            v.y = fma(beta, o.y, v.y);
+          }
+          *c = v;
+        }
+      }
+}
+
 }  // namespace
 
 int zgemm_nn_batched(int M, int N, int K, double alpha, const cuDoubleComplex* A, int lda,
                      int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
                      double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
-                     cudaStream_t st) {
+                     cudaStream_t st, int variant) {
   if (M <= 0 || N <= 0 || batch <= 0) return 0;
-  if (cudaFuncSetAttribute(k_zgemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(GemmSmem)) != cudaSuccess)
+  if (variant < 0) variant = kDefaultVariant;
+  auto kernel = variant == kAsync ? k_zgemm_nn_async : k_zgemm_nn;
+  const int smem = variant == kAsync ? (int)sizeof(AsyncSmem) : (int)sizeof(GemmSmem);
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+      cudaSuccess)
     return check_launch("zgemm attribute");
   const dim3 grid((M + kBM - 1) / kBM, (N + kBN - 1) / kBN, batch);
-  k_zgemm_nn<<<grid, kGemmThreads, sizeof(GemmSmem), st>>>(
+  kernel<<<grid, kGemmThreads, smem, st>>>(
       M, N, K, alpha, reinterpret_cast<const double2*>(A), lda, stride_a,
       reinterpret_cast<const double2*>(B), ldb, stride_b, beta, reinterpret_cast<double2*>(C),
       ldc, stride_c);
@@ -274,3 +403,18 @@ int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A,
 
 }  // namespace dense
 }  // namespace eb
+
+extern "C" int eb_zgemm_strided_batched(int M, int N, int K, double alpha, const double* A,
+                                        int lda, int64_t stride_a, const double* B, int ldb,
+                                        int64_t stride_b, double beta, double* C, int ldc,
+                                        int64_t stride_c, int batch, int variant, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || batch < 0 || lda < (M > 1 ? M : 1) ||
+      ldb < (K > 1 ? K : 1) || ldc < (M > 1 ? M : 1) || variant < -1 || variant > 1 ||
+      (M > 0 && N > 0 && batch > 0 && (!A || !B || !C)))
+    return eb::fail(EB_ERR_ARG, "zgemm: bad sizes, leading dimensions, variant or pointers");
+  return eb::dense::zgemm_nn_batched(
+      M, N, K, alpha, reinterpret_cast<const cuDoubleComplex*>(A), lda, stride_a,
+      reinterpret_cast<const cuDoubleComplex*>(B), ldb, stride_b, beta,
+      reinterpret_cast<cuDoubleComplex*>(C), ldc, stride_c, batch,
+      reinterpret_cast<cudaStream_t>(stream), variant);
+}

@@ -10,12 +10,17 @@
 namespace eb {
 namespace dense {
 
+// GEMM kernel variants (identical results): register-staged double buffer, cp.async ring.
+constexpr int kStaged = 0, kAsync = 1;
+constexpr int kDefaultVariant = kAsync;
+
 // C_z = alpha A_z B_z + beta C_z for z < batch, column-major, A_z = A + z stride_a (elements)
-// etc.; alpha, beta real; beta == 0 does not read C. Returns an EB_* status.
+// etc.; alpha, beta real; beta == 0 does not read C. variant < 0 takes the default. Returns an
+// EB_* status.
 int zgemm_nn_batched(int M, int N, int K, double alpha, const cuDoubleComplex* A, int lda,
                      int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
                      double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
-                     cudaStream_t st);
+                     cudaStream_t st, int variant = -1);
 
 // y_z = alpha op(A_z) x_z + beta y_z for z < batch, A_z square n x n column-major (lda),
 // op(A) = A (conj_trans = 0) or A^H (conj_trans = 1); alpha, beta real; beta == 0 does not

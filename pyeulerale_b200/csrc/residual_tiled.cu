@@ -19,6 +19,10 @@
 //     (f90:111-120) are taken per orientation. Faces whose two evaluations use different
 //     stencils (next to the wall and the far field, f90:401-436) are evaluated per cell. Each
 //     cell then writes -(F_b + F_f + F_i + F_o) / area (f90:370-436).
+// Threads map to the cells of the tile's part inside the grid (tm x tn cells, tm = min(kTM, M -
+// m0), tn = min(kTN, N - n0)), so that a tile at the grid's outer rows or last columns (129 = 4 x
+// 32 + 1 rows leaves a one-row tile) occupies as many warps as it has cells instead of running
+// every warp for one valid lane; the full tiles take a path with the extents as constants.
 // Results agree with the reference to the rounding of the reordered arithmetic (<= 1e-12
 // relative); every branch (boundary cases, max_c tolerance) follows the reference.
 //
@@ -66,23 +70,30 @@ __device__ __forceinline__ St<T> staged(const TileSmem<T>& S, int i) {
 // Phases 2-4 of a tile whose states (with derived quantities) and vertices are staged in S:
 // sensors, faces, and the residual (or its tangent part) of the tile's cells. Every thread of
 // the CTA calls it.
-template <class T>
+// Full: the tile lies inside the grid (tm = kTM, tn = kTN as constants).
+template <class T, bool Full>
 __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in, const T& mach,
-                                             int m0, int n0, double* R, double* dR, int h) {
-  const int M = in.M, N = in.N;
+                                             int m0, int n0, int tm_in, int tn_in, double* R,
+                                             double* dR, int h) {
+  const int M = in.M;
+  const int tm = Full ? kTM : tm_in, tn = Full ? kTN : tn_in;
   const int tid = threadIdx.x;
   // 2. sensors centred on each needed state: every thread evaluates one angular and one radial
-  // sensor, and the kAngX + kRadX left over go to warps 2-4, so that no warp evaluates more
-  // than three (the phase ends at a barrier: its slowest warp sets its time)
-  constexpr int kAng = kTM * (kTN + 2), kRad = (kTM + 2) * kTN;
-  constexpr int kAngX = kAng - kThreads, kRadX = kRad - kThreads, kX0 = 64;
-  static_assert(kAngX >= 0 && kRadX >= 0 && kX0 + kAngX + kRadX <= kThreads, "sensor split");
+  // sensor, and the ones left over (na + nr - 2 kThreads in a full tile) go to warps 2-4, so
+  // that no warp evaluates more than three (the phase ends at a barrier: its slowest warp sets
+  // its time)
+  const int na = tm * (tn + 2), nr = (tm + 2) * tn;
+  const int ax = max(na - kThreads, 0), rx = max(nr - kThreads, 0);
+  constexpr int kX0 = 64;
+  static_assert(kX0 + (kTM * (kTN + 2) - kThreads) + ((kTM + 2) * kTN - kThreads) <= kThreads,
+                "sensor split");
   auto angular_sensor = [&](int e) {
-    const int r = e % kTM, c = e / kTM - 1;
-    S.s_ang[e] = sensor(S.p[sidx(r, c - 1)], S.p[sidx(r, c)], S.p[sidx(r, c + 1)]);
+    const int r = e % tm, c = e / tm - 1;
+    S.s_ang[(c + 1) * kTM + r] =
+        sensor(S.p[sidx(r, c - 1)], S.p[sidx(r, c)], S.p[sidx(r, c + 1)]);
   };
   auto radial_sensor = [&](int e) {
-    const int r = e % (kTM + 2) - 1, c = e / (kTM + 2);
+    const int r = e % (tm + 2) - 1, c = e / (tm + 2);
     const int m = m0 + r;
     T s = lift<T>(0.0);
     if (m == 0) {  // inner neighbour: the wall ghost of this wall cell (face o, flag 1)
@@ -98,27 +109,27 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
     } else if (m > 0 && m < M - 1) {
       s = sensor(S.p[sidx(r - 1, c)], S.p[sidx(r, c)], S.p[sidx(r + 1, c)]);
     }
-    S.s_rad[e] = s;
+    S.s_rad[c * (kTM + 2) + r + 1] = s;
   };
-  angular_sensor(tid);
-  radial_sensor(tid);
-  if (tid >= kX0 && tid < kX0 + kAngX) angular_sensor(kThreads + tid - kX0);
-  else if (tid >= kX0 + kAngX && tid < kX0 + kAngX + kRadX)
-    radial_sensor(kThreads + tid - kX0 - kAngX);
+  if (tid < na) angular_sensor(tid);
+  if (tid < nr) radial_sensor(tid);
+  if (tid >= kX0 && tid < kX0 + ax) angular_sensor(kThreads + tid - kX0);
+  else if (tid >= kX0 + ax && tid < kX0 + ax + rx) radial_sensor(kThreads + tid - kX0 - ax);
   __syncthreads();
 
   // 3. faces. Thread (r, c) evaluates the angular face between cells (r, c-1) and (r, c) and the
   // radial face between cells (r-1, c) and (r, c), each once for both adjacent cells where the
   // reference's two evaluations have the same stencil; its own cell's fluxes (faces b and i)
-  // stay in registers, the neighbours' (faces f and o) go to shared memory. The tile's last
-  // face column / row is evaluated by threads 0..31 / 32..39 in addition.
-  const int r = tid % kTM, c = tid / kTM;
-  const int m = m0 + r, n = n0 + c;
-  const bool own = m < M && n < N;
+  // stay in registers, the neighbours' (faces f and o) go to shared memory. The faces past the
+  // tile's last column / row (face f of column tn - 1, face o of row tm - 1: interior faces, or
+  // the far-field faces of a tile that ends at the grid's outer row) are evaluated by threads
+  // 0 .. tm - 1 / tm .. tm + tn - 1 in addition.
+  const int r = tid % tm, c = tid / tm;
+  const int m = m0 + r;
+  const bool own = tid < tm * tn;
   Flux<T> Fb, Fi;
 #pragma unroll
   for (int k = 0; k < 4; ++k) Fb.f[k] = Fi.f[k] = lift<T>(0.0);
-  auto exists = [&](int rr, int cc) { return rr >= 0 && cc >= 0 && m0 + rr < M && n0 + cc < N; };
   auto angular_face = [&](int fr, int fc, bool want_b, bool want_f, Flux<T>& Fb_out) {
     // l = (fr, fc), r = (fr, fc - 1): face b of (fr, fc) and face f of (fr, fc - 1)
     const T nbx = S.z[vidx(fr, fc)] - S.z[vidx(fr + 1, fc)];
@@ -143,62 +154,58 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
     const T gx = (S.vx[vidx(fr, fc)] + S.vx[vidx(fr, fc + 1)]) / 2.0;
     const T gz = (S.vz[vidx(fr, fc)] + S.vz[vidx(fr, fc + 1)]) / 2.0;
     const T vn = gx * nix + gz * niz;
-    Flux<T> F, Fp;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) F.f[k] = Fp.f[k] = lift<T>(0.0);
-    if (fm == 0) {  // wall face of cell 0 (flag 1): central flux with the wall ghost
-      const St<T> C = staged(S, sidx(fr, fc));
-      F = central(C, wall_ghost_st(C, nix, niz, gx, gz), nix, niz, vn);
-    } else if (fm == M) {  // far-field face of cell M-1 (flag 5): central flux with the ghost
-      const St<T> C = staged(S, sidx(fr - 1, fc));
-      Fp = central(C, farfield_ghost_st(C, mach, in), -nix, -niz, -vn);
-    } else {
-      const T len = sqrt_(nix * nix + niz * niz);
-      const St<T> L = staged(S, sidx(fr, fc)), Rs = staged(S, sidx(fr - 1, fc));
-      const T sl = S.s_rad[fc * (kTM + 2) + fr + 1], sr = S.s_rad[fc * (kTM + 2) + fr];
-      if (fm == 1) {
-        // face i of cell 1 (flag 2): central; face o of cell 0 (flag 1): JST whose outer
-        // neighbour is the wall ghost of cell 0
-        F = central(L, Rs, nix, niz, vn);
-        if (want_o) {
-          const T wx = S.z[vidx(fr - 1, fc + 1)] - S.z[vidx(fr - 1, fc)];
-          const T wz = S.x[vidx(fr - 1, fc)] - S.x[vidx(fr - 1, fc + 1)];
-          const T wgx = (S.vx[vidx(fr - 1, fc)] + S.vx[vidx(fr - 1, fc + 1)]) / 2.0;
-          const T wgz = (S.vz[vidx(fr - 1, fc)] + S.vz[vidx(fr - 1, fc + 1)]) / 2.0;
-          Fp = jst(wall_ghost_st(Rs, wx, wz, wgx, wgz), Rs, L, staged(S, sidx(fr + 1, fc)), -nix,
-                   -niz, len, -vn, sr, sl, in);
-        }
-      } else if (fm == M - 1) {
-        // face i of cell M-1 (flag 5): JST whose outer neighbour is the far-field ghost;
-        // face o of cell M-2 (flag 4): central
-        F = jst(farfield_ghost_st(L, mach, in), L, Rs, staged(S, sidx(fr - 2, fc)), nix, niz,
-                len, vn, sl, sr, in);
-        Fp = central(Rs, L, -nix, -niz, -vn);
-      } else {
-        jst_pair(staged(S, sidx(fr + 1, fc)), L, Rs, staged(S, sidx(fr - 2, fc)), nix, niz, len,
-                 vn, sl, sr, in, F, Fp);
-      }
+    // The stencil line (o, c, i, ii) = rows fr + 1, fr, fr - 1, fr - 2, with a ghost state in
+    // place of the missing neighbour at the wall and far-field rows (make_ode's five cases,
+    // f90:401-436), so that every case is one jst_pair and a warp spanning the boundary rows
+    // diverges only in forming its ghost:
+    //  fm = 0:     F (face i of cell 0, flag 1) = central(cell 0, its wall ghost)
+    //  fm = 1:     F (face i of cell 1, flag 2) = central; F' (face o of cell 0, flag 1) = JST
+    //              whose outer neighbour (ii) is the wall ghost of cell 0
+    //  fm = M - 1: F (face i of cell M-1, flag 5) = JST whose outer neighbour (o) is the
+    //              far-field ghost; F' (face o of cell M-2, flag 4) = central
+    //  fm = M:     F' (face o of cell M-1, flag 5) = central(cell M-1, its far-field ghost)
+    // A central flux is the pair's shared central/ALE part, its dissipation switched off. Rows
+    // outside the grid hold finite placeholders, which the switched-off terms multiply by zero.
+    const T len = sqrt_(nix * nix + niz * niz);
+    St<T> O = staged(S, sidx(fr + 1, fc)), L = staged(S, sidx(fr, fc));
+    St<T> Rs = staged(S, sidx(fr - 1, fc)), II = staged(S, sidx(fr - 2, fc));
+    if (fm == 0) {
+      Rs = wall_ghost_st(L, nix, niz, gx, gz);
+    } else if (fm == 1) {
+      const T wx = S.z[vidx(fr - 1, fc + 1)] - S.z[vidx(fr - 1, fc)];
+      const T wz = S.x[vidx(fr - 1, fc)] - S.x[vidx(fr - 1, fc + 1)];
+      const T wgx = (S.vx[vidx(fr - 1, fc)] + S.vx[vidx(fr - 1, fc + 1)]) / 2.0;
+      const T wgz = (S.vz[vidx(fr - 1, fc)] + S.vz[vidx(fr - 1, fc + 1)]) / 2.0;
+      II = wall_ghost_st(Rs, wx, wz, wgx, wgz);
+    } else if (fm == M - 1) {
+      O = farfield_ghost_st(L, mach, in);
+    } else if (fm == M) {
+      L = farfield_ghost_st(Rs, mach, in);
     }
+    const T sl = S.s_rad[fc * (kTM + 2) + fr + 1], sr = S.s_rad[fc * (kTM + 2) + fr];
+    const bool edge = fm == 0 || fm == M;
+    Flux<T> F, Fp;
+    jst_pair(O, L, Rs, II, nix, niz, len, vn, sl, sr, in, F, Fp, !edge && fm != 1,
+             !edge && fm != M - 1);
     if (want_i) Fi_out = F;
     if (want_o)
 #pragma unroll
       for (int k = 0; k < 4; ++k) S.fo[k][fc][fr - 1] = Fp.f[k];
   };
-  if (m < M && (own || exists(r, c - 1))) angular_face(r, c, own, exists(r, c - 1), Fb);
-  if (m <= M && n < N) radial_face(r, c, own, exists(r - 1, c), Fi);
-  if (tid < kTM) {
-    if (exists(tid, kTN - 1)) {
-      Flux<T> unused;
-      angular_face(tid, kTN, false, true, unused);
-    }
-  } else if (tid < kTM + kTN) {
-    if (exists(kTM - 1, tid - kTM)) {
-      Flux<T> unused;
-      radial_face(kTM, tid - kTM, false, true, unused);
-    }
+  if (own) {
+    angular_face(r, c, true, c > 0, Fb);
+    radial_face(r, c, true, r > 0, Fi);
+  }
+  if (tid < tm) {
+    Flux<T> unused;
+    angular_face(tid, tn, false, true, unused);
+  } else if (tid < tm + tn) {
+    Flux<T> unused;
+    radial_face(tm, tid - tm, false, true, unused);
   }
   __syncthreads();
   if (!own) return;
+  const int n = n0 + c;
   const T bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
   const T fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
   const T fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
@@ -237,6 +244,93 @@ __device__ __forceinline__ T with_part(double v, const double* d, int64_t at, in
   }
 }
 
+// One tile: staging (phase 1), then phases 2-4.
+template <class T, bool Full>
+__device__ __forceinline__ void tile_run(TileSmem<T>& S, const Instance& in, const T& mach,
+                                         int m0, int n0, int tm_in, int tn_in, const double* Ui,
+                                         const double* Xi, const double* Vi, const double* dUi,
+                                         const double* dXi, const double* dVi, double* R,
+                                         double* dR, int h) {
+  const int M = in.M, N = in.N;
+  const int tid = threadIdx.x;
+
+  // 1. stage states (cross-shaped halo) and derived quantities, vertices and grid velocities.
+  // A thread first issues all of its global loads (at most two staged states and two vertex
+  // pairs: kStaged = 432 and kVerts = 297 are below 2 * kThreads), then derives and stores, so
+  // its loads are in flight together instead of one round after another. The second-round
+  // states go to the highest threads and the second-round vertices to the lowest, so that no
+  // warp derives a second state and also stages a second vertex. A partial tile stages its
+  // (tm + 4) x (tn + 4) states and (tm + 1) x (tn + 1) vertices at their places in the full
+  // tile's layout; the places it leaves unwritten are read by none of its faces.
+  static_assert(kStaged <= 2 * kThreads && kVerts <= 2 * kThreads, "two staging rounds");
+  const int tm = Full ? kTM : tm_in, tn = Full ? kTN : tn_in;
+  const int sr = tm + 4, ns = sr * (tn + 4), vr = tm + 1, nv = vr * (tn + 1);
+  auto state_item = [&](int k) { return k == 0 ? tid : tid + ns - kThreads; };
+  auto state_valid = [&](int k, int e) { return (k == 0 || e >= kThreads) && e < ns; };
+  double2 sa[2], sb[2], xv[2], vv[2];
+  int64_t sj[2], vj[2];
+  bool sval[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int e = state_item(k);
+    const int r = e % sr - 2, c = e / sr - 2;
+    const bool corner = (r < 0 || r >= tm) && (c < 0 || c >= tn);
+    const int m = m0 + r;
+    sval[k] = state_valid(k, e) && !corner && m >= 0 && m < M;
+    sa[k] = make_double2(1.0, 0.0);
+    sb[k] = make_double2(0.0, 1.0);
+    sj[k] = 0;
+    if (sval[k]) {
+      int n = n0 + c;  // periodic in the angular index: n0 + c lies in [-2, N + kTN + 1]
+      while (n < 0) n += N;
+      while (n >= N) n -= N;
+      sj[k] = m + (int64_t)M * n;
+      const double* q = Ui + 4 * sj[k];
+      sa[k] = __ldg(reinterpret_cast<const double2*>(q));
+      sb[k] = __ldg(reinterpret_cast<const double2*>(q + 2));
+    }
+    const int ev = tid + k * kThreads;
+    xv[k] = make_double2(0.0, 0.0);
+    vv[k] = make_double2(0.0, 0.0);
+    vj[k] = 0;
+    if (ev < nv) {  // vm <= M, vn <= N
+      const int vm = m0 + ev % vr, vn = n0 + ev / vr;
+      vj[k] = vm + (int64_t)(M + 1) * vn;
+      xv[k] = __ldg(reinterpret_cast<const double2*>(Xi + 2 * vj[k]));
+      if (Vi) vv[k] = __ldg(reinterpret_cast<const double2*>(Vi + 2 * vj[k]));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int e = state_item(k);
+    if (state_valid(k, e)) {
+      const int i = sidx(e % sr - 2, e / sr - 2);
+      if (sval[k]) {
+        const double* dq = dUi ? dUi + 8 * sj[k] : nullptr;
+        const St<T> st = derive<T>(with_part<T>(sa[k].x, dq, 0, h), with_part<T>(sa[k].y, dq, 2, h),
+                                   with_part<T>(sb[k].x, dq, 4, h), with_part<T>(sb[k].y, dq, 6, h));
+        S.rho[i] = st.rho; S.j1[i] = st.j1; S.j2[i] = st.j2; S.e[i] = st.e;
+        S.p[i] = st.p; S.ir[i] = st.ir; S.cs[i] = st.cs;
+      } else {  // outside the grid or an unused corner: finite placeholders
+        S.rho[i] = lift<T>(1.0); S.j1[i] = lift<T>(0.0); S.j2[i] = lift<T>(0.0);
+        S.e[i] = lift<T>(1.0); S.p[i] = lift<T>(1.0); S.ir[i] = lift<T>(1.0);
+        S.cs[i] = lift<T>(1.0);
+      }
+    }
+    const int ev = tid + k * kThreads;
+    if (ev < nv) {
+      const int i = vidx(ev % vr, ev / vr);
+      S.x[i] = with_part<T>(xv[k].x, dXi, 4 * vj[k], h);
+      S.z[i] = with_part<T>(xv[k].y, dXi, 4 * vj[k] + 2, h);
+      S.vx[i] = with_part<T>(vv[k].x, dVi, 4 * vj[k], h);
+      S.vz[i] = with_part<T>(vv[k].y, dVi, 4 * vj[k] + 2, h);
+    }
+  }
+  __syncthreads();
+
+  tile_compute<T, Full>(S, in, mach, m0, n0, tm_in, tn_in, R, dR, h);
+}
+
 // Residual: three CTAs per SM (80 registers, with a few spills); on the 256-instance 129x129
 // batch this runs 11 % faster than two CTAs at 120 registers and 4 % faster than four at 64.
 // Tangent (twice the shared memory): two CTAs per SM.
@@ -267,77 +361,11 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, con
   const double* dXi = dX ? dX + 4 * in.vert_offset : nullptr;
   const double* dVi = dV ? dV + 4 * in.vert_offset : nullptr;
   const T mach = with_part<T>(in.mach, dMa, 2 * (int64_t)blockIdx.y, h);
-  const int tid = threadIdx.x;
-
-  // 1. stage states (cross-shaped halo) and derived quantities, vertices and grid velocities.
-  // A thread first issues all of its global loads (at most two staged states and two vertex
-  // pairs: kStaged = 432 and kVerts = 297 are below 2 * kThreads), then derives and stores, so
-  // its loads are in flight together instead of one round after another. The second-round
-  // states go to the highest threads and the second-round vertices to the lowest, so that no
-  // warp derives a second state and also stages a second vertex.
-  static_assert(kStaged <= 2 * kThreads && kVerts <= 2 * kThreads, "two staging rounds");
-  auto state_item = [&](int k) { return k == 0 ? tid : tid + kStaged - kThreads; };
-  auto state_valid = [&](int k, int e) { return (k == 0 || e >= kThreads) && e < kStaged; };
-  double2 sa[2], sb[2], xv[2], vv[2];
-  int64_t sj[2], vj[2];
-  bool sval[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int e = state_item(k);
-    const int r = e % kSR - 2, c = e / kSR - 2;
-    const bool corner = (r < 0 || r >= kTM) && (c < 0 || c >= kTN);
-    const int m = m0 + r;
-    sval[k] = state_valid(k, e) && !corner && m >= 0 && m < M;
-    sa[k] = make_double2(1.0, 0.0);
-    sb[k] = make_double2(0.0, 1.0);
-    sj[k] = 0;
-    if (sval[k]) {
-      int n = n0 + c;  // periodic in the angular index: n0 + c lies in [-2, N + kTN + 1]
-      while (n < 0) n += N;
-      while (n >= N) n -= N;
-      sj[k] = m + (int64_t)M * n;
-      const double* q = Ui + 4 * sj[k];
-      sa[k] = __ldg(reinterpret_cast<const double2*>(q));
-      sb[k] = __ldg(reinterpret_cast<const double2*>(q + 2));
-    }
-    const int ev = tid + k * kThreads;
-    xv[k] = make_double2(0.0, 0.0);
-    vv[k] = make_double2(0.0, 0.0);
-    vj[k] = 0;
-    if (ev < kVerts) {
-      const int vm = min(m0 + ev % kVR, M), vn = min(n0 + ev / kVR, N);
-      vj[k] = vm + (int64_t)(M + 1) * vn;
-      xv[k] = __ldg(reinterpret_cast<const double2*>(Xi + 2 * vj[k]));
-      if (Vi) vv[k] = __ldg(reinterpret_cast<const double2*>(Vi + 2 * vj[k]));
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int e = state_item(k);
-    if (state_valid(k, e)) {
-      if (sval[k]) {
-        const double* dq = dUi ? dUi + 8 * sj[k] : nullptr;
-        const St<T> st = derive<T>(with_part<T>(sa[k].x, dq, 0, h), with_part<T>(sa[k].y, dq, 2, h),
-                                   with_part<T>(sb[k].x, dq, 4, h), with_part<T>(sb[k].y, dq, 6, h));
-        S.rho[e] = st.rho; S.j1[e] = st.j1; S.j2[e] = st.j2; S.e[e] = st.e;
-        S.p[e] = st.p; S.ir[e] = st.ir; S.cs[e] = st.cs;
-      } else {  // outside the grid or an unused corner: finite placeholders
-        S.rho[e] = lift<T>(1.0); S.j1[e] = lift<T>(0.0); S.j2[e] = lift<T>(0.0);
-        S.e[e] = lift<T>(1.0); S.p[e] = lift<T>(1.0); S.ir[e] = lift<T>(1.0);
-        S.cs[e] = lift<T>(1.0);
-      }
-    }
-    const int ev = tid + k * kThreads;
-    if (ev < kVerts) {
-      S.x[ev] = with_part<T>(xv[k].x, dXi, 4 * vj[k], h);
-      S.z[ev] = with_part<T>(xv[k].y, dXi, 4 * vj[k] + 2, h);
-      S.vx[ev] = with_part<T>(vv[k].x, dVi, 4 * vj[k], h);
-      S.vz[ev] = with_part<T>(vv[k].y, dVi, 4 * vj[k] + 2, h);
-    }
-  }
-  __syncthreads();
-
-  tile_compute<T>(S, in, mach, m0, n0, R, dR, h);
+  const int tm = min(kTM, M - m0), tn = min(kTN, N - n0);
+  if (tm == kTM && tn == kTN)
+    tile_run<T, true>(S, in, mach, m0, n0, tm, tn, Ui, Xi, Vi, dUi, dXi, dVi, R, dR, h);
+  else
+    tile_run<T, false>(S, in, mach, m0, n0, tm, tn, Ui, Xi, Vi, dUi, dXi, dVi, R, dR, h);
 }
 
 int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,

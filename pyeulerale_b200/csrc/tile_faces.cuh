@@ -156,12 +156,16 @@ __device__ __forceinline__ Flux<promote_all_t<TLL, TL, TR, TRR, TG, TS1, TS2>> j
 // orientation as the reference takes them. The shared parts are formed once: the central flux
 // minus the grid-velocity flux as (F(l) + F(r)) . n / 2 - (l + r) vn / 2 with the face-relative
 // normal velocities vl - vn and vr - vn, and the third difference in F's orientation.
+// diss / diss_p = false switch an orientation's dissipation off (its coefficients are zero), which
+// leaves the central flux with the grid-velocity term (f90:197, 219) of the boundary-adjacent faces;
+// the states then need only be finite.
 template <class TLL, class TL, class TR, class TRR, class TG, class TSL, class TSR>
 __device__ __forceinline__ void jst_pair(
     const St<TLL>& ll, const St<TL>& l, const St<TR>& r, const St<TRR>& rr, const TG& nx,
     const TG& nz, const TG& len, const TG& vn, const TSL& sl, const TSR& sr, const Instance& in,
     Flux<promote_all_t<TLL, TL, TR, TRR, TG, TSL, TSR>>& F,
-    Flux<promote_all_t<TLL, TL, TR, TRR, TG, TSL, TSR>>& Fp) {
+    Flux<promote_all_t<TLL, TL, TR, TRR, TG, TSL, TSR>>& Fp, bool diss = true,
+    bool diss_p = true) {
   using R = promote_all_t<TLL, TL, TR, TRR, TG, TSL, TSR>;
   const auto vl = (nx * l.j1 + nz * l.j2) * l.ir;
   const auto vr = (nx * r.j1 + nz * r.j2) * r.ir;
@@ -189,7 +193,9 @@ __device__ __forceinline__ void jst_pair(
   const R rv[4] = {lift<R>(r.rho), lift<R>(r.j1), lift<R>(r.j2), lift<R>(r.e)};
   const R llv[4] = {lift<R>(ll.rho), lift<R>(ll.j1), lift<R>(ll.j2), lift<R>(ll.e)};
   const R rrv[4] = {lift<R>(rr.rho), lift<R>(rr.j1), lift<R>(rr.j2), lift<R>(rr.e)};
-  const R c2 = lift<R>(coef2), c2p = lift<R>(coef2p), c4 = lift<R>(coef4), c4p = lift<R>(coef4p);
+  const R zero = lift<R>(0.0);
+  const R c2 = diss ? lift<R>(coef2) : zero, c4 = diss ? lift<R>(coef4) : zero;
+  const R c2p = diss_p ? lift<R>(coef2p) : zero, c4p = diss_p ? lift<R>(coef4p) : zero;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const R d1 = rv[k] - lv[k];
