@@ -44,9 +44,10 @@ struct GemmSmem {
 
 // D = A B + C for one 8 x 8 x 4 FP64 tile (a: A[lane / 4][lane % 4], b: B[lane % 4][lane / 4],
 // c / d: C[lane / 4][2 (lane % 4) + {0, 1}]).
+// (Not volatile: the instruction has no effect beyond its outputs, so the compiler may
+// interleave independent MMAs to cover their latency.)
 __device__ __forceinline__ void mma884(double (&d)[2], double a, double b) {
-  asm volatile(
-      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
       : "+d"(d[0]), "+d"(d[1])
       : "d"(a), "d"(b));
 }
@@ -132,13 +133,20 @@ __global__ void __launch_bounds__(kGemmThreads)
         b_r[j] = S.br[buf][wn + 8 * j + fr][kk + fc];
         b_i[j] = S.bi[buf][wn + 8 * j + fr][kk + fc];
       }
+      // two rounds over the 4 x 4 tiles, so that an accumulator's two MMAs of a k-step are
+      // 32 independent MMAs apart (same order of the terms per accumulator)
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           mma884(re[i][j], a_r[i], b_r[j]);
-          mma884(re[i][j], a_n[i], b_i[j]);
           mma884(im[i][j], a_r[i], b_i[j]);
+        }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          mma884(re[i][j], a_n[i], b_i[j]);
           mma884(im[i][j], a_i[i], b_r[j]);
         }
     }
@@ -260,8 +268,13 @@ __global__ void __launch_bounds__(kGemmThreads)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           mma884(re[i][j], a[i].x, b[j].x);
-          mma884(re[i][j], a_n[i], b[j].y);
           mma884(im[i][j], a[i].x, b[j].y);
+        }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          mma884(re[i][j], a_n[i], b[j].y);
           mma884(im[i][j], a[i].y, b[j].x);
         }
     }

@@ -139,64 +139,53 @@ __device__ __forceinline__ void add_to(double (&acc)[kBlk], const double (&b)[kB
   for (int e = 0; e < kBlk; ++e) acc[e] = acc[e] + b[e];
 }
 
-// The cells of a tile inside the grid (tm x tn, tm = min(kTM, M - m0), tn = min(kTN, N - n0))
-// and the role of this thread: threads 0 .. tm tn - 1 own cell (r, c) = (tid % tm, tid / tm)
-// and evaluate its faces b and i; thread tm tn + x evaluates the angular face past the tile's
-// last column in row x < tm, and the radial face past its last row (an interior face, or the
-// far-field face of a tile that ends at the grid's outer row) in column x < tn. A full tile maps
-// as 32 x 7 cells on warps 0-6 and the extra faces on warp 7; a partial one (129 = 4 x 32 + 1
-// rows leaves a one-row tile) occupies as many warps as it has cells.
-struct TileMap {
-  int tm, tn, r, c, x;
-  bool own;
-};
-
 // One seeded stencil position K of the angular faces (Radial = false) or the radial faces:
 // evaluate this thread's face, pass the neighbour's derivative block through shared memory, and
 // advance this cell's blocks.
 template <bool Radial, int K, int G>
-__device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0,
-                                          const TileMap& tmap, double (&acc_c)[kBlk],
-                                          double (&acc_x)[kBlk], double area, double* Jc,
-                                          int64_t slot_stride) {
-  const int M = in.M;
-  const int r = tmap.r, c = tmap.c;
+__device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0, int n0,
+                                          double (&acc_c)[kBlk], double (&acc_x)[kBlk],
+                                          double area, double* Jc, int64_t slot_stride) {
+  const int M = in.M, N = in.N;
+  const int tid = threadIdx.x, r = tid % kTM, c = tid / kTM;
   const int m = m0 + r;
-  const bool own = tmap.own;
+  auto exists = [&](int rr, int cc) {
+    return rr >= 0 && cc >= 0 && rr < kTM && cc < kTN && m0 + rr < M && n0 + cc < N;
+  };
+  const bool own = exists(r, c);
   double fo[kBlk];  // this cell's own face, differentiated
 #pragma unroll
   for (int e = 0; e < kBlk; ++e) fo[e] = 0.0;
   {
-    int fr, fc;  // the face this thread evaluates
-    int tr, tc;  // the cell that receives its neighbour flux
-    bool eval = true;
-    if (own) {
-      fr = r;
-      fc = c;
-      tr = Radial ? r - 1 : r;
-      tc = Radial ? c : c - 1;
-    } else if (!Radial) {
-      eval = tmap.x < tmap.tm;
-      fr = tr = tmap.x;
-      fc = tmap.tn;
-      tc = tmap.tn - 1;
-    } else {
-      eval = tmap.x < tmap.tn;
-      fr = tmap.tm;
-      tr = tmap.tm - 1;
-      fc = tc = tmap.x;
+    int fr = r, fc = c;  // the face this thread evaluates
+    int tr, tc;          // the cell that receives its neighbour flux
+    bool eval;
+    if (!Radial) {
+      eval = m < M && (own || exists(r, c - 1));
+      tr = r;
+      tc = c - 1;
+    } else if (c < kTN) {
+      eval = m <= M && n0 + c < N;
+      tr = r - 1;
+      tc = c;
+    } else {  // threads (r < kTN, kTN): the radial faces past the tile's outer row
+      fr = kTM;
+      fc = r;
+      eval = r < kTN && exists(kTM - 1, r);
+      tr = kTM - 1;
+      tc = r;
     }
     if (eval) {
       Flux<D4> F, Fp;
       if (!Radial) angular_pair<K, G>(S, in, fr, fc, F, Fp);
       else radial_pair<K, G>(S, in, m0 + fr, fr, fc, F, Fp);
-      if (tr >= 0 && tc >= 0) {
+      if (exists(tr, tc)) {
 #pragma unroll
         for (int r4 = 0; r4 < 4; ++r4)
 #pragma unroll
           for (int i = 0; i < kW; ++i) S.nb[r4 + 4 * i][tc][tr] = Fp.f[r4].d[i];
       }
-      if (own) {
+      if (fr == r && fc == c && own) {
 #pragma unroll
         for (int r4 = 0; r4 < 4; ++r4)
 #pragma unroll
@@ -247,17 +236,17 @@ __device__ __forceinline__ void seed_step(Smem& S, const Instance& in, int m0,
 
 // The eight seed steps of one pass (component group G of the seeded states).
 template <int G>
-__device__ __forceinline__ void all_steps(Smem& S, const Instance& in, int m0, const TileMap& tm,
+__device__ __forceinline__ void all_steps(Smem& S, const Instance& in, int m0, int n0,
                                           double (&acc_c)[kBlk], double (&acc_x)[kBlk], double area,
                                           double* Jc, int64_t slot_stride) {
-  seed_step<false, 0, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<false, 1, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<false, 2, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<false, 3, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 0, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 1, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 2, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
-  seed_step<true, 3, G>(S, in, m0, tm, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 0, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 1, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 2, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<false, 3, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 0, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 1, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 2, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  seed_step<true, 3, G>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
 }
 
 __global__ void __launch_bounds__(kThreads, kW == 4 ? 1 : 2)
@@ -307,16 +296,9 @@ __global__ void __launch_bounds__(kThreads, kW == 4 ? 1 : 2)
   }
   __syncthreads();
 
-  TileMap tmap;
-  tmap.tm = min(kTM, M - m0);
-  tmap.tn = min(kTN, N - n0);
-  tmap.own = tid < tmap.tm * tmap.tn;
-  tmap.r = tmap.own ? tid % tmap.tm : 0;
-  tmap.c = tmap.own ? tid / tmap.tm : 0;
-  tmap.x = tid - tmap.tm * tmap.tn;
-  const int r = tmap.r, c = tmap.c;
+  const int r = tid % kTM, c = tid / kTM;
   double area = 1.0;
-  if (tmap.own) {  // make_area (f90:287-293), as the residual kernel forms it
+  if (c < kTN) {  // make_area (f90:287-293), as the residual kernel forms it
     const double bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
     const double fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
     const double fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
@@ -326,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, kW == 4 ? 1 : 2)
   const int64_t slot_stride = 16 * (int64_t)M * N;
   double* Jc = J + 144 * in.cell_offset + 16 * ((int64_t)(m0 + r) + (int64_t)M * (n0 + c));
   double acc_c[kBlk], acc_x[kBlk];
-  all_steps<0>(S, in, m0, tmap, acc_c, acc_x, area, Jc, slot_stride);
-  if constexpr (kGroups > 1) all_steps<1>(S, in, m0, tmap, acc_c, acc_x, area, Jc, slot_stride);
+  all_steps<0>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
+  if constexpr (kGroups > 1) all_steps<1>(S, in, m0, n0, acc_c, acc_x, area, Jc, slot_stride);
 }
 

@@ -32,6 +32,7 @@
 // max_c (f90:97-120) taking their branches from the values as the reference's complex step
 // does.
 
+#include "autotune.cuh"
 #include "common.cuh"
 #include "tile_faces.cuh"
 
@@ -70,8 +71,10 @@ __device__ __forceinline__ St<T> staged(const TileSmem<T>& S, int i) {
 // Phases 2-4 of a tile whose states (with derived quantities) and vertices are staged in S:
 // sensors, faces, and the residual (or its tangent part) of the tile's cells. Every thread of
 // the CTA calls it.
-// Full: the tile lies inside the grid (tm = kTM, tn = kTN as constants).
-template <class T, bool Full>
+// Full: the tile lies inside the grid (tm = kTM, tn = kTN as constants). Pre: a thread loads its
+// own cell's state and corners once for both of its faces and its area (more registers live
+// across the faces) instead of per use; the same arithmetic either way.
+template <class T, bool Full, bool Pre>
 __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in, const T& mach,
                                              int m0, int n0, int tm_in, int tn_in, double* R,
                                              double* dR, int h) {
@@ -130,15 +133,26 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
   Flux<T> Fb, Fi;
 #pragma unroll
   for (int k = 0; k < 4; ++k) Fb.f[k] = Fi.f[k] = lift<T>(0.0);
-  auto angular_face = [&](int fr, int fc, bool want_b, bool want_f, Flux<T>& Fb_out) {
-    // l = (fr, fc), r = (fr, fc - 1): face b of (fr, fc) and face f of (fr, fc - 1)
-    const T nbx = S.z[vidx(fr, fc)] - S.z[vidx(fr + 1, fc)];
-    const T nbz = S.x[vidx(fr + 1, fc)] - S.x[vidx(fr, fc)];
-    const T vn = (S.vx[vidx(fr + 1, fc)] + S.vx[vidx(fr, fc)]) / 2.0 * nbx +
-                 (S.vz[vidx(fr + 1, fc)] + S.vz[vidx(fr, fc)]) / 2.0 * nbz;
+  // The state of cell (fr, fc) and the vertices (fr, fc), (fr + 1, fc) [angular] or
+  // (fr, fc + 1) [radial] come as arguments: a thread loads its own cell's state and corners
+  // once for both of its faces and its area.
+  struct Vtx {
+    T x, z, vx, vz;
+  };
+  auto vtx = [&](int vr, int vc) {
+    const int i = vidx(vr, vc);
+    return Vtx{S.x[i], S.z[i], S.vx[i], S.vz[i]};
+  };
+  auto angular_face = [&](int fr, int fc, bool want_b, bool want_f, Flux<T>& Fb_out,
+                          const St<T>& L, const Vtx& v0, const Vtx& v1) {
+    // l = (fr, fc), r = (fr, fc - 1): face b of (fr, fc) and face f of (fr, fc - 1);
+    // v0 = vertex (fr, fc), v1 = vertex (fr + 1, fc)
+    const T nbx = v0.z - v1.z;
+    const T nbz = v1.x - v0.x;
+    const T vn = (v1.vx + v0.vx) / 2.0 * nbx + (v1.vz + v0.vz) / 2.0 * nbz;
     const T len = sqrt_(nbx * nbx + nbz * nbz);
     Flux<T> F, Fp;
-    jst_pair(staged(S, sidx(fr, fc + 1)), staged(S, sidx(fr, fc)), staged(S, sidx(fr, fc - 1)),
+    jst_pair(staged(S, sidx(fr, fc + 1)), L, staged(S, sidx(fr, fc - 1)),
              staged(S, sidx(fr, fc - 2)), nbx, nbz, len, vn, S.s_ang[fc * kTM + fr + kTM],
              S.s_ang[(fc - 1) * kTM + fr + kTM], in, F, Fp);
     if (want_b) Fb_out = F;
@@ -146,13 +160,15 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
 #pragma unroll
       for (int k = 0; k < 4; ++k) S.ff[k][fc - 1][fr] = Fp.f[k];
   };
-  auto radial_face = [&](int fr, int fc, bool want_i, bool want_o, Flux<T>& Fi_out) {
-    // l = (fr, fc), r = (fr - 1, fc): face i of (fr, fc) and face o of (fr - 1, fc)
+  auto radial_face = [&](int fr, int fc, bool want_i, bool want_o, Flux<T>& Fi_out,
+                         const St<T>& Lin, const Vtx& v0, const Vtx& v2) {
+    // l = (fr, fc), r = (fr - 1, fc): face i of (fr, fc) and face o of (fr - 1, fc);
+    // v0 = vertex (fr, fc), v2 = vertex (fr, fc + 1)
     const int fm = m0 + fr;
-    const T nix = S.z[vidx(fr, fc + 1)] - S.z[vidx(fr, fc)];
-    const T niz = S.x[vidx(fr, fc)] - S.x[vidx(fr, fc + 1)];
-    const T gx = (S.vx[vidx(fr, fc)] + S.vx[vidx(fr, fc + 1)]) / 2.0;
-    const T gz = (S.vz[vidx(fr, fc)] + S.vz[vidx(fr, fc + 1)]) / 2.0;
+    const T nix = v2.z - v0.z;
+    const T niz = v0.x - v2.x;
+    const T gx = (v0.vx + v2.vx) / 2.0;
+    const T gz = (v0.vz + v2.vz) / 2.0;
     const T vn = gx * nix + gz * niz;
     // The stencil line (o, c, i, ii) = rows fr + 1, fr, fr - 1, fr - 2, with a ghost state in
     // place of the missing neighbour at the wall and far-field rows (make_ode's five cases,
@@ -167,7 +183,7 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
     // A central flux is the pair's shared central/ALE part, its dissipation switched off. Rows
     // outside the grid hold finite placeholders, which the switched-off terms multiply by zero.
     const T len = sqrt_(nix * nix + niz * niz);
-    St<T> O = staged(S, sidx(fr + 1, fc)), L = staged(S, sidx(fr, fc));
+    St<T> O = staged(S, sidx(fr + 1, fc)), L = Lin;
     St<T> Rs = staged(S, sidx(fr - 1, fc)), II = staged(S, sidx(fr - 2, fc));
     if (fm == 0) {
       Rs = wall_ghost_st(L, nix, niz, gx, gz);
@@ -192,26 +208,41 @@ __device__ __forceinline__ void tile_compute(TileSmem<T>& S, const Instance& in,
 #pragma unroll
       for (int k = 0; k < 4; ++k) S.fo[k][fc][fr - 1] = Fp.f[k];
   };
+  T ia = lift<T>(1.0);
+  // make_area (f90:287-293) from the corners bi, fi, fo, bo
+  auto inv_area = [&](const T& bix, const T& biz, const T& fix, const T& fiz, const T& box,
+                      const T& boz) {
+    const T fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
+    const T area = abs_c((fox - bix) * (boz - fiz) - (foz - biz) * (box - fix)) / 2.0;
+    return T(1.0 / area);
+  };
   if (own) {
-    angular_face(r, c, true, c > 0, Fb);
-    radial_face(r, c, true, r > 0, Fi);
+    if constexpr (Pre) {
+      const St<T> L = staged(S, sidx(r, c));
+      const Vtx bi = vtx(r, c), bo = vtx(r + 1, c), fi = vtx(r, c + 1);
+      angular_face(r, c, true, c > 0, Fb, L, bi, bo);
+      radial_face(r, c, true, r > 0, Fi, L, bi, fi);
+      ia = inv_area(bi.x, bi.z, fi.x, fi.z, bo.x, bo.z);
+    } else {
+      angular_face(r, c, true, c > 0, Fb, staged(S, sidx(r, c)), vtx(r, c), vtx(r + 1, c));
+      radial_face(r, c, true, r > 0, Fi, staged(S, sidx(r, c)), vtx(r, c), vtx(r, c + 1));
+    }
   }
   if (tid < tm) {
     Flux<T> unused;
-    angular_face(tid, tn, false, true, unused);
+    angular_face(tid, tn, false, true, unused, staged(S, sidx(tid, tn)), vtx(tid, tn),
+                 vtx(tid + 1, tn));
   } else if (tid < tm + tn) {
     Flux<T> unused;
-    radial_face(tm, tid - tm, false, true, unused);
+    radial_face(tm, tid - tm, false, true, unused, staged(S, sidx(tm, tid - tm)),
+                vtx(tm, tid - tm), vtx(tm, tid - tm + 1));
   }
   __syncthreads();
   if (!own) return;
+  if constexpr (!Pre)
+    ia = inv_area(S.x[vidx(r, c)], S.z[vidx(r, c)], S.x[vidx(r, c + 1)], S.z[vidx(r, c + 1)],
+                  S.x[vidx(r + 1, c)], S.z[vidx(r + 1, c)]);
   const int n = n0 + c;
-  const T bix = S.x[vidx(r, c)], biz = S.z[vidx(r, c)];
-  const T fix = S.x[vidx(r, c + 1)], fiz = S.z[vidx(r, c + 1)];
-  const T fox = S.x[vidx(r + 1, c + 1)], foz = S.z[vidx(r + 1, c + 1)];
-  const T box = S.x[vidx(r + 1, c)], boz = S.z[vidx(r + 1, c)];
-  const T area = abs_c((fox - bix) * (boz - fiz) - (foz - biz) * (box - fix)) / 2.0;
-  const T ia = 1.0 / area;
   T res[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) res[k] = -(((Fb.f[k] + S.ff[k][c][r]) + Fi.f[k]) + S.fo[k][c][r]) * ia;
@@ -245,7 +276,7 @@ __device__ __forceinline__ T with_part(double v, const double* d, int64_t at, in
 }
 
 // One tile: staging (phase 1), then phases 2-4.
-template <class T, bool Full>
+template <class T, bool Full, bool Pre>
 __device__ __forceinline__ void tile_run(TileSmem<T>& S, const Instance& in, const T& mach,
                                          int m0, int n0, int tm_in, int tn_in, const double* Ui,
                                          const double* Xi, const double* Vi, const double* dUi,
@@ -328,7 +359,7 @@ __device__ __forceinline__ void tile_run(TileSmem<T>& S, const Instance& in, con
   }
   __syncthreads();
 
-  tile_compute<T, Full>(S, in, mach, m0, n0, tm_in, tn_in, R, dR, h);
+  tile_compute<T, Full, Pre>(S, in, mach, m0, n0, tm_in, tn_in, R, dR, h);
 }
 
 // Residual: three CTAs per SM (80 registers, with a few spills); on the 256-instance 129x129
@@ -337,7 +368,8 @@ __device__ __forceinline__ void tile_run(TileSmem<T>& S, const Instance& in, con
 template <class T>
 constexpr int kMinBlocks = std::is_same<T, double>::value ? 3 : 2;
 
-template <class T>
+// Pre: see tile_compute (two launch variants of identical results, chosen by the autotuner).
+template <class T, bool Pre>
 __global__ void __launch_bounds__(kThreads, kMinBlocks<T>)
 k_residual_tiled(Table t, const double* X, const double* V, const double* U, const double* dX,
                  const double* dV, const double* dU, const double* dMa, double* R, double* dR) {
@@ -363,34 +395,44 @@ k_residual_tiled(Table t, const double* X, const double* V, const double* U, con
   const T mach = with_part<T>(in.mach, dMa, 2 * (int64_t)blockIdx.y, h);
   const int tm = min(kTM, M - m0), tn = min(kTN, N - n0);
   if (tm == kTM && tn == kTN)
-    tile_run<T, true>(S, in, mach, m0, n0, tm, tn, Ui, Xi, Vi, dUi, dXi, dVi, R, dR, h);
+    tile_run<T, true, Pre>(S, in, mach, m0, n0, tm, tn, Ui, Xi, Vi, dUi, dXi, dVi, R, dR, h);
   else
-    tile_run<T, false>(S, in, mach, m0, n0, tm, tn, Ui, Xi, Vi, dUi, dXi, dVi, R, dR, h);
+    tile_run<T, false, false>(S, in, mach, m0, n0, tm, tn, Ui, Xi, Vi, dUi, dXi, dVi, R, dR, h);
 }
+
+static const char* const kVariantNames[2] = {"loads per use", "own cell preloaded"};
 
 int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
                           double* R, cudaStream_t stream, int max_tiles) {
   const Table t = make_table(b);
-  dim3 grid(max_tiles, b->n_inst);
-  if (cudaFuncSetAttribute(k_residual_tiled<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(TileSmem<double>)) != cudaSuccess)
-    return check_launch("compute_odes attribute");
-  k_residual_tiled<double><<<grid, kThreads, sizeof(TileSmem<double>), stream>>>(
-      t, X, V, U, nullptr, nullptr, nullptr, nullptr, R, nullptr);
-  return check_launch("compute_odes");
+  const dim3 grid(max_tiles, b->n_inst);
+  return tune::launch_tuned(
+      "residual_tiled", b->n_cells, max_tiles, 2, 0, kVariantNames, stream, [&](int v) {
+        auto kernel = v == 0 ? k_residual_tiled<double, false> : k_residual_tiled<double, true>;
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(TileSmem<double>)) != cudaSuccess)
+          return check_launch("compute_odes attribute");
+        kernel<<<grid, kThreads, sizeof(TileSmem<double>), stream>>>(
+            t, X, V, U, nullptr, nullptr, nullptr, nullptr, R, nullptr);
+        return check_launch("compute_odes");
+      });
 }
 
 int launch_tangent_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
                          const double* dU, const double* dX, const double* dV, const double* dMa,
                          double* dR, double* R, cudaStream_t stream, int max_tiles) {
   const Table t = make_table(b);
-  dim3 grid(2 * max_tiles, b->n_inst);
-  if (cudaFuncSetAttribute(k_residual_tiled<D1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(TileSmem<D1>)) != cudaSuccess)
-    return check_launch("apply_odes_tangent attribute");
-  k_residual_tiled<D1><<<grid, kThreads, sizeof(TileSmem<D1>), stream>>>(t, X, V, U, dX, dV, dU,
-                                                                         dMa, R, dR);
-  return check_launch("apply_odes_tangent");
+  const dim3 grid(2 * max_tiles, b->n_inst);
+  return tune::launch_tuned(
+      "tangent_tiled", b->n_cells, max_tiles, 2, 0, kVariantNames, stream, [&](int v) {
+        auto kernel = v == 0 ? k_residual_tiled<D1, false> : k_residual_tiled<D1, true>;
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(TileSmem<D1>)) != cudaSuccess)
+          return check_launch("apply_odes_tangent attribute");
+        kernel<<<grid, kThreads, sizeof(TileSmem<D1>), stream>>>(t, X, V, U, dX, dV, dU, dMa,
+                                                                 R, dR);
+        return check_launch("apply_odes_tangent");
+      });
 }
 
 int residual_tiles(int M, int N) { return ((M + kTM - 1) / kTM) * ((N + kTN - 1) / kTN); }

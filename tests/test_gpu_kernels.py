@@ -443,3 +443,26 @@ def test_adjoint_variants_agree(cuda, golden_grids, monkeypatch):
     line = [s for s in report.splitlines()
             if f"residual_adjoint complex ({gpu.M * gpu.N}," in s]
     assert line and "1 CTA/SM" in line[0] and "(kept)" in line[0]
+
+
+@pytest.mark.parametrize("case_name", ["naca0012_33_moving", "min4x5"])
+def test_residual_and_tangent_variants_agree(cuda, golden_grids, monkeypatch, case_name):
+    """The residual kernel's two launch variants (loads per use, own cell preloaded) give
+    bit-identical residuals and tangents, full and partial tiles alike."""
+    case = make_case(case_name, golden_grids, seed=4)
+    gpu = Gpu(cuda, case)
+    M, N = gpu.M, gpu.N
+    rng = np.random.default_rng(41)
+    d = [crandn(rng, (4, M, N)), crandn(rng, (2, M + 1, N + 1)), crandn(rng, (2, M + 1, N + 1)),
+         np.array([0.3 - 0.2j])]
+    dd = [gpu.dev(a) for a in d]
+    out = []
+    for v in ("v0", "v1"):
+        monkeypatch.setenv("EB_AUTOTUNE", v)
+        R = gpu.empty(4 * M * N)
+        gpu.call("eb_compute_odes", gpu.X, gpu.V, gpu.U, R)
+        dR, R2 = gpu.empty(8 * M * N), gpu.empty(4 * M * N)
+        gpu.call("eb_apply_odes_tangent", gpu.X, gpu.V, gpu.U, *dd, dR, R2)
+        out.append([R.cpu().numpy(), dR.cpu().numpy(), R2.cpu().numpy()])
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
