@@ -368,7 +368,8 @@ __device__ __forceinline__ void tile_run(TileSmem<T>& S, const Instance& in, con
 template <class T>
 constexpr int kMinBlocks = std::is_same<T, double>::value ? 3 : 2;
 
-// Pre: see tile_compute (two launch variants of identical results, chosen by the autotuner).
+// Pre: see tile_compute (for the residual two launch variants of identical results, chosen by
+// the autotuner; the tangent uses Pre = false).
 template <class T, bool Pre>
 __global__ void __launch_bounds__(kThreads, kMinBlocks<T>)
 k_residual_tiled(Table t, const double* X, const double* V, const double* U, const double* dX,
@@ -421,18 +422,17 @@ int launch_residual_tiled(const eb_batch* b, const double* X, const double* V, c
 int launch_tangent_tiled(const eb_batch* b, const double* X, const double* V, const double* U,
                          const double* dU, const double* dX, const double* dV, const double* dMa,
                          double* dR, double* R, cudaStream_t stream, int max_tiles) {
+  // One variant only: in dual arithmetic the compiler's multiply-add contraction follows the
+  // code layout, so the preloading variant's tangent differs in the last bits; a fixed variant
+  // keeps the tangent deterministic.
   const Table t = make_table(b);
   const dim3 grid(2 * max_tiles, b->n_inst);
-  return tune::launch_tuned(
-      "tangent_tiled", b->n_cells, max_tiles, 2, 0, kVariantNames, stream, [&](int v) {
-        auto kernel = v == 0 ? k_residual_tiled<D1, false> : k_residual_tiled<D1, true>;
-        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(TileSmem<D1>)) != cudaSuccess)
-          return check_launch("apply_odes_tangent attribute");
-        kernel<<<grid, kThreads, sizeof(TileSmem<D1>), stream>>>(t, X, V, U, dX, dV, dU, dMa,
-                                                                 R, dR);
-        return check_launch("apply_odes_tangent");
-      });
+  auto kernel = k_residual_tiled<D1, false>;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(TileSmem<D1>)) != cudaSuccess)
+    return check_launch("apply_odes_tangent attribute");
+  kernel<<<grid, kThreads, sizeof(TileSmem<D1>), stream>>>(t, X, V, U, dX, dV, dU, dMa, R, dR);
+  return check_launch("apply_odes_tangent");
 }
 
 int residual_tiles(int M, int N) { return ((M + kTM - 1) / kTM) * ((N + kTN - 1) / kTN); }
