@@ -247,6 +247,25 @@ int eb_gmres_solve_noalloc(const eb_batch* b, const eb_instance* host_table, con
                            int adjoint, const double* rhs, double* x,
                            const eb_gmres_options* opt, eb_gmres_info* info, void* stream);
 
+/* Many shifts of one instance by GMRES preconditioned with the ring-LU factors of a few nearby
+ * "anchor" shifts: system s (shift s, right-hand side s) is right-preconditioned by
+ * (J - a_k I)^-1 with k = sys_anchor[s], the anchors' factors being those eb_ringlu_factor_many
+ * left in ringlu_workspace (anchor k at ringlu_workspace + k * ringlu_stride). Each Arnoldi step
+ * applies every anchor's factors once to all of its systems (at most 8 per anchor) as a forward
+ * ring sweep over several right-hand sides; anchors whose systems have all converged drop out.
+ * Forward solves only (the frequency response's (dR/dU - s I) dU = rhs, core.py:533-565 per
+ * shift in the reference); single instance. workspace: eb_gmres_workspace_bytes(b, NULL, n_sys,
+ * NULL, restart) bytes; aux: eb_gmres_anchored_aux_bytes bytes, 256-byte aligned. Other
+ * arguments, statuses and info as eb_gmres_solve (EB_ERR_NOCONV leaves the unconverged systems'
+ * last iterates in x; a caller solves those directly). Synchronises `stream`. */
+int64_t eb_gmres_anchored_aux_bytes(int M, int N, int n_sys, int n_anchors,
+                                    const int32_t* sys_anchor);
+int eb_gmres_solve_anchored(const eb_batch* b, const double* J, int n_sys, const double* shifts,
+                            const double* rhs, double* x, const eb_gmres_options* opt,
+                            int n_anchors, const int32_t* sys_anchor, const void* ringlu_workspace,
+                            int64_t ringlu_stride, void* workspace, int64_t workspace_bytes,
+                            void* aux, int64_t aux_bytes, eb_gmres_info* info, void* stream);
+
 /* ---- resolvent: direct ring-block LU ----------------------------------------------------- */
 
 /* Device workspace (bytes) holding the block-LU factors of one M x N instance: 3 M dense

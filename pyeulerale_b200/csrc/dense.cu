@@ -396,6 +396,73 @@ __global__ void __launch_bounds__(256) k_zgemv_c(int n, double alpha, const doub
   }
 }
 
+// C = alpha A B + beta C with A n x n and B, C n x nr (nr <= kMaxRhs right-hand sides): the
+// multi-right-hand-side form of k_zgemv_n (one read of A serves all nr columns). B is staged in
+// shared memory; thread (r, g) of a 256-thread CTA sums the columns j = g (mod 8) of row r for
+// every right-hand side, and the eight partial sums of a row are added in a fixed order. Batch
+// entry z uses A + zmap[z] sa etc. (zmap == nullptr: z itself); entries z >= *n_batch exit.
+constexpr int kMaxRhs = 8;
+
+__global__ void __launch_bounds__(256) k_zgemm_skinny(int n, int nr, double alpha,
+                                                      const double2* A, int lda, int64_t sa,
+                                                      const double2* B, int ldb, int64_t sb,
+                                                      double beta, double2* C, int ldc,
+                                                      int64_t sc, const int* zmap,
+                                                      const int* n_batch) {
+  extern __shared__ __align__(16) unsigned char sk_smem[];
+  double2* Bs = reinterpret_cast<double2*>(sk_smem);               // n x nr
+  double2* part = Bs + (size_t)n * nr;                              // 8 x 32 x nr
+  if (n_batch && (int)blockIdx.y >= *n_batch) return;
+  const int64_t z = zmap ? zmap[blockIdx.y] : blockIdx.y;
+  A += sa * z;
+  B += sb * z;
+  C += sc * z;
+  for (int e = threadIdx.x; e < n * nr; e += blockDim.x) {
+    const int q = e / n, j = e - q * n;
+    Bs[e] = B[j + (int64_t)ldb * q];
+  }
+  __syncthreads();
+  const int r = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + r;
+  double sr[kMaxRhs], si[kMaxRhs];
+#pragma unroll
+  for (int q = 0; q < kMaxRhs; ++q) sr[q] = si[q] = 0.0;
+  if (i < n) {
+    for (int j = g; j < n; j += 8) {
+      const double2 a = A[i + (int64_t)lda * j];
+#pragma unroll
+      for (int q = 0; q < kMaxRhs; ++q) {
+        if (q < nr) {
+          const double2 v = Bs[j + n * q];
+          sr[q] = fma(a.x, v.x, fma(-a.y, v.y, sr[q]));
+          si[q] = fma(a.x, v.y, fma(a.y, v.x, si[q]));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kMaxRhs; ++q)
+    if (q < nr) part[(q * 8 + g) * 32 + r] = make_double2(sr[q], si[q]);
+  __syncthreads();
+  if (i < n) {
+    for (int q = g; q < nr; q += 8) {
+      double tr = 0.0, ti = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        tr += part[(q * 8 + k) * 32 + r].x;
+        ti += part[(q * 8 + k) * 32 + r].y;
+      }
+      double2* c = C + i + (int64_t)ldc * q;
+      double2 out = make_double2(alpha * tr, alpha * ti);
+      if (beta != 0.0) {
+        out.x = fma(beta, c->x, out.x);
+        out.y = fma(beta, c->y, out.y);
+      }
+      *c = out;
+    }
+  }
+}
+
 }  // namespace
 
 int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A, int lda,
@@ -412,6 +479,24 @@ int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A,
     k_zgemv_n<<<dim3((n + 31) / 32, batch), 256, 0, st>>>(n, alpha, a, lda, stride_a, v,
                                                           stride_x, beta, w, stride_y);
   return check_launch("zgemv");
+}
+
+int zgemm_skinny_batched(int n, int nr, double alpha, const cuDoubleComplex* A, int lda,
+                         int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
+                         double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
+                         const int* zmap, const int* n_batch, cudaStream_t st) {
+  if (n <= 0 || batch <= 0 || nr <= 0) return 0;
+  if (nr > kMaxRhs) return fail(EB_ERR_ARG, "zgemm_skinny: too many right-hand sides");
+  const size_t smem = sizeof(double2) * ((size_t)n * nr + 8 * 32 * (size_t)nr);
+  if (smem > 200 * 1024) return fail(EB_ERR_ARG, "zgemm_skinny: right-hand sides too large");
+  if (cudaFuncSetAttribute(k_zgemm_skinny, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return check_launch("zgemm_skinny attribute");
+  k_zgemm_skinny<<<dim3((n + 31) / 32, batch), 256, smem, st>>>(
+      n, nr, alpha, reinterpret_cast<const double2*>(A), lda, stride_a,
+      reinterpret_cast<const double2*>(B), ldb, stride_b, beta, reinterpret_cast<double2*>(C),
+      ldc, stride_c, zmap, n_batch);
+  return check_launch("zgemm_skinny");
 }
 
 }  // namespace dense

@@ -15,9 +15,12 @@
 // The driver loop (eb_gmres_solve) is native C++; the caller passes all device memory as
 // one workspace (eb_gmres_workspace_bytes), so a solve performs no allocation.
 
+#include <cuComplex.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <functional>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -32,6 +35,15 @@ int fail(int code, const char* msg);
 int check_launch(const char* what);
 int validate(const eb_batch* b);
 extern thread_local std::string g_last_error;
+
+namespace rl {
+int anchored_apply(int M, int N, const void* ringlu_ws, int64_t ringlu_stride, int n_anchors,
+                   int nr, int n_sys, const int* d_sys_anchor, const int* d_sys_col,
+                   const int* d_active, const int* d_zmap, const int* d_n_active,
+                   cuDoubleComplex* Y, cuDoubleComplex* X, cuDoubleComplex* W, int64_t mstride,
+                   const double* in, double* out, int64_t vstride, int accumulate,
+                   cudaStream_t st);
+}  // namespace rl
 
 namespace gm {
 
@@ -597,10 +609,34 @@ int64_t eb_gmres_workspace_bytes(const eb_batch* b, const eb_instance* host_tabl
   return (int64_t)plan(n_sys, n_cells, n_chunks, restart).total;
 }
 
-int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const double* J, int n_sys,
-                   const int32_t* sys_inst, const double* shifts, int adjoint,
-                   const double* rhs, double* x, const eb_gmres_options* opt, void* workspace,
-                   int64_t workspace_bytes, eb_gmres_info* info, void* stream) {
+}  // extern "C"
+
+namespace eb {
+namespace gm {
+
+// The anchored preconditioner's state (see eb_gmres_solve_anchored): the anchors' ring-LU
+// factors, the systems' anchor and column, and the anchors' multi-right-hand-side ring blocks.
+struct Anchored {
+  int M, N;
+  const void* ringlu_ws;
+  int64_t ringlu_stride;
+  int n_anchors, nr;
+  const int* d_sys_anchor;
+  const int* d_sys_col;
+  int* d_zmap;
+  int* d_n_active;
+  cuDoubleComplex *Y, *X, *W;
+  int64_t mstride;
+  std::vector<int> sys_anchor;  // host copy
+  std::vector<int> zmap;        // host staging of the active anchors
+};
+
+// The restarted GMRES of eb_gmres_solve with the block-Jacobi preconditioner (ap == nullptr) or
+// the anchored ring-LU preconditioner.
+int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J, int n_sys,
+               const int32_t* sys_inst, const double* shifts, int adjoint, const double* rhs,
+               double* x, const eb_gmres_options* opt, void* workspace, int64_t workspace_bytes,
+               eb_gmres_info* info, void* stream, Anchored* ap) {
   if ((reinterpret_cast<uintptr_t>(J) | reinterpret_cast<uintptr_t>(rhs) |
        reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(workspace)) & 15)
     return fail(EB_ERR_ARG, "gmres: arrays must be 16-byte aligned");
@@ -654,6 +690,38 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
     k_reduce<<<n_sys, 256, 0, st_>>>(d_sys, n_sys, d_active, 0, part, part_stride, out, 1);
   };
 
+  // out = P^-1 in (accumulate: out += P^-1 in) for the active systems
+  auto prec = [&](const double* in, double* out, int accumulate) {
+    if (!ap) {
+      k_prec<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, in, out,
+                                  accumulate);
+      return EB_OK;
+    }
+    return rl::anchored_apply(ap->M, ap->N, ap->ringlu_ws, ap->ringlu_stride, ap->n_anchors,
+                              ap->nr, n_sys, ap->d_sys_anchor, ap->d_sys_col, d_active,
+                              ap->d_zmap, ap->d_n_active, ap->Y, ap->X, ap->W, ap->mstride, in,
+                              out, (int64_t)ap->M * ap->N * 8, accumulate, st_);
+  };
+  // the anchored preconditioner works on the anchors that still have an active system
+  auto prec_active = [&]() {
+    if (!ap) return EB_OK;
+    std::vector<char> any(ap->n_anchors, 0);
+    for (int s = 0; s < n_sys; ++s)
+      if (active[s]) any[ap->sys_anchor[s]] = 1;
+    ap->zmap.clear();
+    for (int a = 0; a < ap->n_anchors; ++a)
+      if (any[a]) ap->zmap.push_back(a);
+    const int n_act = (int)ap->zmap.size();
+    ap->zmap.push_back(n_act);  // the count goes to d_n_active
+    if (cudaMemcpyAsync(ap->d_zmap, ap->zmap.data(), sizeof(int) * n_act, cudaMemcpyHostToDevice,
+                        st_) != cudaSuccess ||
+        cudaMemcpyAsync(ap->d_n_active, &ap->zmap[n_act], sizeof(int), cudaMemcpyHostToDevice,
+                        st_) != cudaSuccess ||
+        cudaStreamSynchronize(st_) != cudaSuccess)
+      return check_launch("gmres anchors");
+    return EB_OK;
+  };
+
   // ||b|| (kept in n2[S + s]) and the initial residual r = b - A x0 with x0 = 0.
   norms2(rhs, n2 + n_sys);
   if (!opt->use_initial_guess) cudaMemsetAsync(x, 0, sizeof(double) * 8 * n_cells, st_);
@@ -689,6 +757,7 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
       break;
     }
     cudaMemcpyAsync(d_active, active.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice, st_);
+    if ((rc = prec_active()) != EB_OK) return rc;
     ++cycles;
     k_cycle_start<<<gs, 128, 0, st_>>>(n_sys, d_active, m, n2, g, d_state);
     k_scale<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, d_state, V);
@@ -696,7 +765,7 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
     for (; j < m && total_iters < opt->max_iterations; ++j, ++total_iters) {
       double* vj = V + (int64_t)j * vstride;
       double* w = V + (int64_t)(j + 1) * vstride;
-      k_prec<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, vj, z, 0);
+      if ((rc = prec(vj, z, 0)) != EB_OK) return rc;
       k_op<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, z, nullptr, w);
       for (int pass = 0; pass < 2; ++pass) {
         double* h = pass == 0 ? h1 : h2;
@@ -728,7 +797,7 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
     // x += P^-1 (V y), then the true residual
     k_backsolve<<<gs, 128, 0, st_>>>(n_sys, d_active, m, H, g, y, d_state);
     k_combine<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, V, vstride, m, y, d_state, t);
-    k_prec<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, t, x, 1);
+    if ((rc = prec(t, x, 1)) != EB_OK) return rc;
     k_op<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, x, rhs, V);
     norms2(V, n2);
     rc = check_launch("gmres cycle");
@@ -747,6 +816,119 @@ int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const doubl
                                              : "gmres: iteration limit reached");
   }
   return EB_OK;
+}
+
+// Bytes of the anchored preconditioner's auxiliary buffer (anchor map and count, systems'
+// anchors and columns, three ring-block sets of n_anchors x M x 4N x nr complex).
+struct AuxLayout {
+  size_t off_zmap, off_nact, off_sa, off_sc, off_Y, off_X, off_W, total;
+  int64_t mstride;
+};
+AuxLayout aux_plan(int M, int N, int n_sys, int n_anchors, int nr) {
+  AuxLayout A;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = (o + bytes + 255) & ~(size_t)255;
+    return at;
+  };
+  A.mstride = (int64_t)M * 4 * N * nr;
+  A.off_zmap = take(sizeof(int) * (size_t)n_anchors);
+  A.off_nact = take(sizeof(int));
+  A.off_sa = take(sizeof(int) * (size_t)n_sys);
+  A.off_sc = take(sizeof(int) * (size_t)n_sys);
+  const size_t blocks = sizeof(cuDoubleComplex) * (size_t)A.mstride * n_anchors;
+  A.off_Y = take(blocks);
+  A.off_X = take(blocks);
+  A.off_W = take(blocks);
+  A.total = o;
+  return A;
+}
+
+}  // namespace gm
+}  // namespace eb
+
+extern "C" {
+
+int eb_gmres_solve(const eb_batch* b, const eb_instance* host_table, const double* J, int n_sys,
+                   const int32_t* sys_inst, const double* shifts, int adjoint,
+                   const double* rhs, double* x, const eb_gmres_options* opt, void* workspace,
+                   int64_t workspace_bytes, eb_gmres_info* info, void* stream) {
+  return eb::gm::gmres_core(b, host_table, J, n_sys, sys_inst, shifts, adjoint, rhs, x, opt,
+                            workspace, workspace_bytes, info, stream, nullptr);
+}
+
+int64_t eb_gmres_anchored_aux_bytes(int M, int N, int n_sys, int n_anchors,
+                                    const int32_t* sys_anchor) {
+  if (M < 1 || N < 1 || n_sys < 1 || n_anchors < 1 || !sys_anchor) return -1;
+  std::vector<int> count(n_anchors, 0);
+  int nr = 0;
+  for (int s = 0; s < n_sys; ++s) {
+    if (sys_anchor[s] < 0 || sys_anchor[s] >= n_anchors) return -1;
+    nr = std::max(nr, ++count[sys_anchor[s]]);
+  }
+  if (nr > 8) return -1;
+  return (int64_t)eb::gm::aux_plan(M, N, n_sys, n_anchors, nr).total;
+}
+
+int eb_gmres_solve_anchored(const eb_batch* b, const double* J, int n_sys, const double* shifts,
+                            const double* rhs, double* x, const eb_gmres_options* opt,
+                            int n_anchors, const int32_t* sys_anchor, const void* ringlu_workspace,
+                            int64_t ringlu_stride, void* workspace, int64_t workspace_bytes,
+                            void* aux, int64_t aux_bytes, eb_gmres_info* info, void* stream) {
+  using namespace eb::gm;
+  int rc = validate(b);
+  if (rc != EB_OK) return rc;
+  if (b->n_inst != 1 || b->d_table)
+    return fail(EB_ERR_ARG, "gmres anchored: single instance only");
+  if (!sys_anchor || !ringlu_workspace || !aux || n_anchors < 1 || n_sys < 1)
+    return fail(EB_ERR_ARG, "gmres anchored: null argument");
+  const int M = b->single.M, N = b->single.N;
+  const int64_t ws_need = eb_ringlu_workspace_bytes(M, N);
+  if (ws_need < 0 || ringlu_stride < ws_need || ringlu_stride % 256 != 0 ||
+      reinterpret_cast<uintptr_t>(ringlu_workspace) % 256 != 0)
+    return fail(EB_ERR_ARG, "gmres anchored: bad ring-LU workspace or stride");
+  std::vector<int> count(n_anchors, 0), col(n_sys, 0), sa(n_sys, 0);
+  int nr = 0;
+  for (int s = 0; s < n_sys; ++s) {
+    if (sys_anchor[s] < 0 || sys_anchor[s] >= n_anchors)
+      return fail(EB_ERR_ARG, "gmres anchored: anchor index out of range");
+    sa[s] = sys_anchor[s];
+    col[s] = count[sa[s]]++;
+    nr = std::max(nr, count[sa[s]]);
+  }
+  if (nr > 8) return fail(EB_ERR_ARG, "gmres anchored: more than 8 systems on one anchor");
+  const AuxLayout A = aux_plan(M, N, n_sys, n_anchors, nr);
+  if ((int64_t)A.total > aux_bytes || reinterpret_cast<uintptr_t>(aux) % 256 != 0)
+    return fail(EB_ERR_ARG, "gmres anchored: auxiliary buffer too small or not 256-byte aligned");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  char* ab = static_cast<char*>(aux);
+  Anchored ap;
+  ap.M = M;
+  ap.N = N;
+  ap.ringlu_ws = ringlu_workspace;
+  ap.ringlu_stride = ringlu_stride;
+  ap.n_anchors = n_anchors;
+  ap.nr = nr;
+  ap.d_sys_anchor = reinterpret_cast<const int*>(ab + A.off_sa);
+  ap.d_sys_col = reinterpret_cast<const int*>(ab + A.off_sc);
+  ap.d_zmap = reinterpret_cast<int*>(ab + A.off_zmap);
+  ap.d_n_active = reinterpret_cast<int*>(ab + A.off_nact);
+  ap.Y = reinterpret_cast<cuDoubleComplex*>(ab + A.off_Y);
+  ap.X = reinterpret_cast<cuDoubleComplex*>(ab + A.off_X);
+  ap.W = reinterpret_cast<cuDoubleComplex*>(ab + A.off_W);
+  ap.mstride = A.mstride;
+  ap.sys_anchor = sa;
+  // columns an anchor does not use stay zero through the sweeps
+  if (cudaMemsetAsync(ab + A.off_Y, 0, A.total - A.off_Y, st) != cudaSuccess ||
+      cudaMemcpyAsync(ab + A.off_sa, sa.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice,
+                      st) != cudaSuccess ||
+      cudaMemcpyAsync(ab + A.off_sc, col.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice,
+                      st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return check_launch("gmres anchored setup");
+  return gmres_core(b, nullptr, J, n_sys, nullptr, shifts, 0, rhs, x, opt, workspace,
+                    workspace_bytes, info, stream, &ap);
 }
 
 }  // extern "C"

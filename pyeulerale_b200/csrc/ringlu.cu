@@ -900,6 +900,149 @@ int ring_solve(const Group& g, bool adjoint, cudaStream_t stream) {
   return check_launch("ring solve");
 }
 
+// ---- many right-hand sides per factorisation (the anchored GMRES preconditioner) ----------
+//
+// A set of factorised shifts ("anchors", workspace of anchor a at base + a * stride) and nr
+// right-hand sides per anchor. The right-hand sides of anchor a are ring vectors stored as M ring
+// blocks of K x nr (column-major, leading dimension K) at Y + a * mstride (likewise X, W). The
+// launches cover the anchors zmap[0 .. *n_active - 1] (device arrays), so anchors whose systems
+// have all converged drop out without a change of launch shape.
+
+// Out -= Bd V for the nr columns (Bd: N real 4 x 4 blocks of the anchor's workspace at off_bd).
+__global__ void __launch_bounds__(128) k_bd_mat(int N, int nr, const char* ws0, int64_t stride,
+                                                size_t off_bd, const cuDoubleComplex* V,
+                                                cuDoubleComplex* Out, int64_t mstride,
+                                                const int* zmap, const int* n_active) {
+  if ((int)blockIdx.y >= *n_active) return;
+  const int a = zmap[blockIdx.y];
+  const double* B = reinterpret_cast<const double*>(ws0 + (int64_t)a * stride + off_bd);
+  const int K = 4 * N;
+  V += (int64_t)a * mstride;
+  Out += (int64_t)a * mstride;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K * nr; e += gridDim.x * blockDim.x) {
+    const int q = e / K, row = e - q * K, n = row >> 2, r = row & 3;
+    const double* b = B + 16 * n;
+    const cuDoubleComplex* vn = V + (int64_t)q * K + 4 * n;
+    cuDoubleComplex acc = Out[e];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double bi = b[r + 4 * i];
+      acc.x = fma(-bi, vn[i].x, acc.x);
+      acc.y = fma(-bi, vn[i].y, acc.y);
+    }
+    Out[e] = acc;
+  }
+}
+
+// System vectors (reference layout, system s at in + s * vstride doubles) -> column sys_col[s]
+// of anchor sys_anchor[s]'s ring blocks.
+__global__ void k_sys_to_multi(int M, int N, int nr, int n_sys, const int* sys_anchor,
+                               const int* sys_col, const double* in, int64_t vstride,
+                               cuDoubleComplex* Y, int64_t mstride) {
+  const int s = blockIdx.y;
+  if (s >= n_sys) return;
+  const int K = 4 * N;
+  const int64_t cells = (int64_t)M * N;
+  const double* v = in + (int64_t)s * vstride;
+  cuDoubleComplex* y = Y + (int64_t)sys_anchor[s] * mstride + (int64_t)sys_col[s] * K;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(c % M), n = (int)(c / M);
+    const double2* a = reinterpret_cast<const double2*>(v + 8 * c);
+    cuDoubleComplex* o = y + (int64_t)m * K * nr + 4 * n;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double2 z = a[k];
+      o[k] = make_cuDoubleComplex(z.x, z.y);
+    }
+  }
+}
+
+// The inverse of k_sys_to_multi for the systems with active[s] (accumulate: out += ...).
+__global__ void k_multi_to_sys(int M, int N, int nr, int n_sys, const int* sys_anchor,
+                               const int* sys_col, const int* active,
+                               const cuDoubleComplex* X, int64_t mstride, double* out,
+                               int64_t vstride, int accumulate) {
+  const int s = blockIdx.y;
+  if (s >= n_sys || !active[s]) return;
+  const int K = 4 * N;
+  const int64_t cells = (int64_t)M * N;
+  double* v = out + (int64_t)s * vstride;
+  const cuDoubleComplex* x = X + (int64_t)sys_anchor[s] * mstride + (int64_t)sys_col[s] * K;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(c % M), n = (int)(c / M);
+    const cuDoubleComplex* i = x + (int64_t)m * K * nr + 4 * n;
+    double2* o = reinterpret_cast<double2*>(v + 8 * c);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      double2 z = make_double2(i[k].x, i[k].y);
+      if (accumulate) {
+        const double2 w = o[k];
+        z = make_double2(w.x + z.x, w.y + z.y);
+      }
+      o[k] = z;
+    }
+  }
+}
+
+// X = A^-1 Y column by column for the anchors in zmap (A = the anchor's shifted Jacobian): the
+// forward sweep of ring_solve with every matrix-vector product over nr right-hand sides. Y is
+// overwritten; W is scratch.
+int ring_solve_multi(const Group& g, int nr, cuDoubleComplex* Y, cuDoubleComplex* X,
+                     cuDoubleComplex* W, int64_t mstride, const int* zmap, const int* n_active,
+                     cudaStream_t st) {
+  const Layout& L = g.L;
+  const int M = L.M, K = L.K, N = L.N;
+  const int64_t es = g.es();
+  auto blk = [&](cuDoubleComplex* base, int m) { return base + (size_t)K * nr * m; };
+  int rc = EB_OK;
+  auto gemm = [&](double alpha, const cuDoubleComplex* A, const cuDoubleComplex* B, double beta,
+                  cuDoubleComplex* C) {
+    if (rc == EB_OK)
+      rc = dense::zgemm_skinny_batched(K, nr, alpha, A, K, es, B, K, mstride, beta, C, K,
+                                       mstride, g.S, zmap, n_active, st);
+  };
+  const dim3 bdg((K * nr + 127) / 128, g.S);
+  auto bd = [&](size_t off_bd, const cuDoubleComplex* V, cuDoubleComplex* Out) {
+    k_bd_mat<<<bdg, 128, 0, st>>>(N, nr, g.base, g.stride, off_bd, V, Out, mstride, zmap,
+                                  n_active);
+  };
+  for (int m = 0; m < M; ++m) {  // Lt z = b (z in Y), W[m] = Dinv_m z[m]
+    if (m >= 1) gemm(-1.0, g.blk(L.off_L1, m), blk(Y, m - 1), 1.0, blk(Y, m));
+    if (m >= 2) bd(L.off_B2 + L.bdr * m, blk(W, m - 2), blk(Y, m));
+    if (m + 2 < M) gemm(1.0, g.blk(L.off_D, m), blk(Y, m), 0.0, blk(W, m));
+  }
+  for (int m = M - 1; m >= 0; --m) {  // Ut x = z
+    if (m + 1 < M) gemm(-1.0, g.blk(L.off_C1, m), blk(X, m + 1), 1.0, blk(Y, m));
+    if (m + 2 < M) bd(L.off_C2 + L.bdr * m, blk(X, m + 2), blk(Y, m));
+    gemm(1.0, g.blk(L.off_D, m), blk(Y, m), 0.0, blk(X, m));
+  }
+  if (rc != EB_OK) return rc;
+  return check_launch("ring solve multi");
+}
+
+// out = A_{anchor(s)}^-1 in for the systems of one instance (the anchored GMRES preconditioner):
+// gather into the anchors' ring blocks, the forward sweeps, scatter to the active systems.
+int anchored_apply(int M, int N, const void* ringlu_ws, int64_t ringlu_stride, int n_anchors,
+                   int nr, int n_sys, const int* d_sys_anchor, const int* d_sys_col,
+                   const int* d_active, const int* d_zmap, const int* d_n_active,
+                   cuDoubleComplex* Y, cuDoubleComplex* X, cuDoubleComplex* W, int64_t mstride,
+                   const double* in, double* out, int64_t vstride, int accumulate,
+                   cudaStream_t st) {
+  const Group g{plan(M, N), static_cast<char*>(const_cast<void*>(ringlu_ws)), ringlu_stride,
+                n_anchors};
+  const int gc = grid_for((int64_t)M * N, 128) / 4 + 1;
+  k_sys_to_multi<<<dim3(gc, n_sys), 128, 0, st>>>(M, N, nr, n_sys, d_sys_anchor, d_sys_col, in,
+                                                  vstride, Y, mstride);
+  int rc = ring_solve_multi(g, nr, Y, X, W, mstride, d_zmap, d_n_active, st);
+  if (rc != EB_OK) return rc;
+  k_multi_to_sys<<<dim3(gc, n_sys), 128, 0, st>>>(M, N, nr, n_sys, d_sys_anchor, d_sys_col,
+                                                  d_active, X, mstride, out, vstride,
+                                                  accumulate);
+  return check_launch("anchored preconditioner");
+}
+
 }  // namespace rl
 }  // namespace eb
 

@@ -349,20 +349,28 @@ def _device_apply(solver, name: str, jac, x, out_numel: int):
 
 def frequency_response_batched(solver, chord: float, axis_location: float,
                                reduced_frequencies, group: int = 16,
-                               tol: float = 1e-10) -> tuple[np.ndarray, np.ndarray]:
+                               tol: float = 1e-10, method: str = "direct",
+                               per_anchor: int = 4,
+                               stats: dict | None = None) -> tuple[np.ndarray, np.ndarray]:
     """``frequency_response`` with the shifts factored and solved together on the device.
 
     The pitch-to-(c_l, c_m) transfer function at s = i k V_inf / (c/2) for every reduced
     frequency k (examples/response/run.py:135-176): each shift solves
     (dR/dU - s I) dU = -(dR/dX + s dR/dV) dX/dalpha; c_l(s) = <grad_F c_l, dF/dX dX + dF/dU dU>,
-    c_m(s) likewise plus <grad_X c_m, dX>. ``group`` shifts share each factorisation call
-    (``RingLUMany``: one launch per elimination step for the whole group); right-hand sides,
-    solutions and force perturbations stay on the device, only the 2 x len(k) coefficients
-    come back. The solver must be linearized at the state of interest.
+    c_m(s) likewise plus <grad_X c_m, dX>. Right-hand sides, solutions and force perturbations
+    stay on the device, only the 2 x len(k) coefficients come back. The solver must be
+    linearized at the state of interest.
+
+    method "direct": ``group`` shifts share each factorisation call (``RingLUMany``: one launch
+    per elimination step for the whole group). method "anchored": the shifts, ordered by
+    magnitude, go in groups of ``per_anchor`` around one factorised anchor shift each, and all
+    shifts are solved by GMRES preconditioned with their anchor's factors
+    (``solver.solve_anchored``); a shift whose GMRES does not converge is solved directly.
+    ``stats`` (optional dict) receives the anchored solve's iteration counts.
     """
     import torch
 
-    from .solver import RingLUMany
+    from .solver import RingLUMany, anchor_shifts, solve_anchored
 
     ks = np.atleast_1d(np.asarray(reduced_frequencies, dtype=float))
     speed = solver.mach_number * HEAT_RATIO**0.5
@@ -382,21 +390,47 @@ def frequency_response_batched(solver, chord: float, axis_location: float,
     cl_grad = to_dev(solver.compute_lift_coefficient_wrt_forces())
     cm_grad = to_dev(solver.compute_moment_coefficient_wrt_forces())
     cm_x = complex(np.vdot(solver.compute_moment_coefficient_wrt_vertices(), dX))
-    lu = RingLUMany(solver._batch(), capacity=min(group, len(shifts)), tol=tol)
     cl = np.empty(len(shifts), dtype=complex)
     cm = np.empty(len(shifts), dtype=complex)
-    for g0 in range(0, len(shifts), lu.capacity):
-        chunk = shifts[g0:g0 + lu.capacity]
-        st = torch.from_numpy(chunk).to("cuda")[:, None]
-        rhs = torch.view_as_real(-(rx[None, :] + st * rv[None, :])).reshape(len(chunk), -1)
-        rhs = rhs.contiguous()
-        lu.factor(solver._dJ_u, chunk)
-        x, _ = lu.solve(rhs)
+
+    def rhs_of(chunk):
+        st = torch.from_numpy(np.asarray(chunk)).to("cuda")[:, None]
+        return torch.view_as_real(-(rx[None, :] + st * rv[None, :])).reshape(len(chunk), -1) \
+            .contiguous()
+
+    def coefficients(idx, x):
         dF = torch.stack([torch.view_as_complex(_device_apply(
             solver, "eb_apply_forces_wrt_states_fwd", solver._dJF_u, x[k], nf).view(-1, 2))
-            for k in range(len(chunk))]) + dFx[None, :]
-        cl[g0:g0 + len(chunk)] = (dF @ cl_grad.conj()).cpu().numpy()
-        cm[g0:g0 + len(chunk)] = (dF @ cm_grad.conj()).cpu().numpy() + cm_x
+            for k in range(len(idx))]) + dFx[None, :]
+        cl[idx] = (dF @ cl_grad.conj()).cpu().numpy()
+        cm[idx] = (dF @ cm_grad.conj()).cpu().numpy() + cm_x
+
+    if method == "direct":
+        lu = RingLUMany(solver._batch(), capacity=min(group, len(shifts)), tol=tol)
+        for g0 in range(0, len(shifts), lu.capacity):
+            chunk = shifts[g0:g0 + lu.capacity]
+            lu.factor(solver._dJ_u, chunk)
+            x, _ = lu.solve(rhs_of(chunk))
+            coefficients(np.arange(g0, g0 + len(chunk)), x)
+        return cl, cm
+    if method != "anchored":
+        raise ValueError(f"unknown method {method!r}")
+    anchors, sys_anchor = anchor_shifts(shifts, per_anchor)
+    lu = RingLUMany(solver._batch(), capacity=len(anchors), tol=tol)
+    lu.factor(solver._dJ_u, anchors)
+    x, info = solve_anchored(solver._batch(), solver._dJ_u, rhs_of(shifts), shifts, lu,
+                             sys_anchor, tol=tol, raise_on_failure=False)
+    bad = [k for k, i in enumerate(info) if not i["converged"]]
+    for g0 in range(0, len(bad), lu.capacity):  # direct solves of the unconverged shifts
+        idx = bad[g0:g0 + lu.capacity]
+        lu.factor(solver._dJ_u, shifts[idx])
+        xd, _ = lu.solve(rhs_of(shifts[idx]))
+        for j, k in enumerate(idx):
+            x[k] = xd[j]
+    del lu
+    if stats is not None:
+        stats.update(anchors=len(anchors), iterations=info.iterations, direct=len(bad))
+    coefficients(np.arange(len(shifts)), x)
     return cl, cm
 
 

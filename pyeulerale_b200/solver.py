@@ -108,6 +108,89 @@ def solve_shifted(batch: _lib.Batch, J, rhs, shifts, *, adjoint: bool = False,
     return x, info
 
 
+def _bind_anchored() -> ctypes.CDLL:
+    lib = _bind()
+    if not getattr(lib, "_anchored_bound", False):
+        P = ctypes.c_void_p
+        lib.eb_gmres_anchored_aux_bytes.restype = ctypes.c_int64
+        lib.eb_gmres_anchored_aux_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, P]
+        lib.eb_gmres_solve_anchored.restype = ctypes.c_int
+        lib.eb_gmres_solve_anchored.argtypes = [
+            ctypes.POINTER(_lib.Batch), P, ctypes.c_int, P, P, P, ctypes.POINTER(GmresOptions),
+            ctypes.c_int, P, P, ctypes.c_int64, P, ctypes.c_int64, P, ctypes.c_int64,
+            ctypes.POINTER(GmresInfo), P]
+        lib._anchored_bound = True
+    return lib
+
+
+def solve_anchored(batch: _lib.Batch, J, rhs, shifts, anchors: "RingLUMany", sys_anchor, *,
+                   tol: float = 1e-10, restart: int = 40, maxiter: int = 240,
+                   check_every: int = 5, raise_on_failure: bool = True):
+    """GMRES on ``(J - s I) x = b`` for many shifts of one instance, each right-preconditioned by
+    the ring-LU factors of its anchor (``eb_gmres_solve_anchored``); returns ``(x, SolveInfo)``.
+
+    ``anchors`` holds the anchors' factorisations (``RingLUMany.factor(J, anchor_shifts)``),
+    ``sys_anchor[s]`` the anchor of system ``s`` (at most 8 systems per anchor). ``rhs``: device
+    float64 tensor of the systems' interleaved complex right-hand sides, system-major.
+    """
+    import torch
+
+    lib = _bind_anchored()
+    n_sys = len(shifts)
+    sh = np.zeros(2 * n_sys)
+    sh[0::2] = np.real(shifts)
+    sh[1::2] = np.imag(shifts)
+    sa = np.ascontiguousarray(sys_anchor, dtype=np.int32)
+    bref = ctypes.byref(batch)
+    M, N = batch.single.M, batch.single.N
+    need = lib.eb_gmres_workspace_bytes(bref, None, n_sys, None, int(restart))
+    aux_need = lib.eb_gmres_anchored_aux_bytes(M, N, n_sys, anchors.capacity, sa.ctypes.data)
+    if need < 0 or aux_need < 0:
+        raise ValueError("invalid anchored GMRES systems")
+    workspace = torch.empty(int(need), dtype=torch.uint8, device=rhs.device)
+    aux = torch.empty(int(aux_need), dtype=torch.uint8, device=rhs.device)
+    x = torch.zeros_like(rhs)
+    opts = GmresOptions(float(tol), int(restart), int(maxiter), int(check_every), 0)
+    infos = (GmresInfo * n_sys)()
+    rc = lib.eb_gmres_solve_anchored(
+        bref, J.data_ptr(), n_sys, sh.ctypes.data, rhs.data_ptr(), x.data_ptr(),
+        ctypes.byref(opts), anchors.capacity, sa.ctypes.data, anchors.workspace.data_ptr(),
+        anchors.stride, workspace.data_ptr(), int(workspace.numel()), aux.data_ptr(),
+        int(aux.numel()), infos, torch.cuda.current_stream().cuda_stream)
+    info = SolveInfo({"iterations": i.iterations, "cycles": i.cycles,
+                      "converged": bool(i.converged), "rel_residual": i.rel_residual}
+                     for i in infos)
+    if rc != _lib.EB_OK and (raise_on_failure or rc != _lib.EB_ERR_NOCONV):
+        raise _lib.EulerB200Error("eb_gmres_solve_anchored", rc, lib.eb_last_error().decode()
+                                  + f" (rel. residuals {[i['rel_residual'] for i in info]})")
+    return x, info
+
+
+def anchor_shifts(shifts, per_anchor: int = 4):
+    """Anchors for ``solve_anchored``: the shifts ordered by magnitude in consecutive groups of
+    ``per_anchor``; a group's anchor has the geometric mean of its magnitudes (the arithmetic mean
+    if one is zero) and its middle shift's direction. Returns ``(anchors, sys_anchor)``."""
+    s = np.asarray(shifts, dtype=complex)
+    if not 1 <= per_anchor <= 8:
+        raise ValueError("per_anchor must be in 1..8")
+    order = np.argsort(np.abs(s), kind="stable")
+    n_a = -(-len(s) // per_anchor)
+    anchors = np.empty(n_a, dtype=complex)
+    sys_anchor = np.empty(len(s), dtype=np.int32)
+    for a in range(n_a):
+        idx = order[a * per_anchor:(a + 1) * per_anchor]
+        g = s[idx]
+        mid = g[len(g) // 2]
+        mags = np.abs(g)
+        if np.all(mags > 0):
+            anchors[a] = np.exp(np.mean(np.log(mags))) * mid / abs(mid)
+        else:
+            anchors[a] = np.mean(g)
+        sys_anchor[idx] = a
+    return anchors, sys_anchor
+
+
 def _bind_ringlu() -> ctypes.CDLL:
     lib = _lib.load()
     if not getattr(lib, "_ringlu_bound", False):

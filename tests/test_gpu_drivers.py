@@ -37,6 +37,51 @@ def test_frequency_response_batched_matches_plain(solver):
     assert rel_err(cm_b, cm_p) <= 1e-10, (cm_b, cm_p)
 
 
+@pytest.mark.parametrize("per_anchor", [1, 3, 8])
+def test_frequency_response_anchored_matches_direct(solver, per_anchor):
+    """GMRES preconditioned by the nearest anchor's ring-LU factors gives the direct solves'
+    transfer function (every system to 1e-10 relative residual), one to eight shifts per anchor
+    (one per anchor: the anchor is the shift itself)."""
+    from pyeulerale_b200 import drivers
+
+    ks = np.logspace(-2, 1, 16)
+    cl_d, cm_d = drivers.frequency_response_batched(solver, 1.0, 0.25, ks, group=8)
+    stats = {}
+    cl_a, cm_a = drivers.frequency_response_batched(solver, 1.0, 0.25, ks, method="anchored",
+                                                    per_anchor=per_anchor, stats=stats)
+    assert stats["anchors"] == -(-len(ks) // per_anchor)
+    assert rel_err(cl_a, cl_d) <= 1e-9, (cl_a, cl_d)
+    assert rel_err(cm_a, cm_d) <= 1e-9, (cm_a, cm_d)
+    if per_anchor == 1:  # the preconditioner is the inverse: done by the first check (5 steps)
+        assert max(stats["iterations"]) <= 5 and stats["direct"] == 0, stats
+
+
+def test_anchored_gmres_residuals_and_fallback(solver, cuda):
+    """solve_anchored reports true residuals at the tolerance; with an iteration limit too small
+    to converge it returns EB_ERR_NOCONV per system (no exception), and the driver's direct
+    fallback still gives the direct result."""
+    from pyeulerale_b200 import drivers
+    from pyeulerale_b200.solver import RingLUMany, anchor_shifts, solve_anchored
+
+    M, N = solver.num_radial, solver.num_angular
+    rng = np.random.default_rng(12)
+    shifts = 1j * np.logspace(-2, 0.5, 6)
+    rhs = cuda.from_numpy((rng.standard_normal((6, 8 * M * N)))).cuda()
+    anchors, sa = anchor_shifts(shifts, 3)
+    np.testing.assert_array_equal(sa, [0, 0, 0, 1, 1, 1])
+    lu = RingLUMany(solver._batch(), capacity=len(anchors))
+    lu.factor(solver._dJ_u, anchors)
+    x, info = solve_anchored(solver._batch(), solver._dJ_u, rhs, shifts, lu, sa)
+    assert all(i["converged"] and i["rel_residual"] <= 1e-10 for i in info), info
+    lu.factor(solver._dJ_u, shifts[:2])
+    xd, _ = lu.solve(rhs[:2].contiguous())
+    assert rel_err(x[:2].cpu().numpy(), xd.cpu().numpy()) <= 1e-8
+    lu.factor(solver._dJ_u, anchors)
+    _, info = solve_anchored(solver._batch(), solver._dJ_u, rhs, shifts, lu, sa, maxiter=1,
+                             raise_on_failure=False)
+    assert not any(i["converged"] for i in info)
+
+
 def test_adjoint_lift_gradient_dot_product(solver):
     """<dc_l/dX, dX> (one adjoint solve) == the forward tangent of c_l along dX."""
     from pyeulerale_b200 import drivers

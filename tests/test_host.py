@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
         "eb_gmres_solve", "eb_gmres_workspace_bytes", "eb_gmres_solve_noalloc",
         "eb_ringlu_factor", "eb_ringlu_solve", "eb_ringlu_workspace_bytes",
         "eb_ringlu_factor_many", "eb_ringlu_solve_many", "eb_ptc_run",
-        "eb_ptc_workspace_bytes"}
+        "eb_ptc_workspace_bytes", "eb_gmres_solve_anchored", "eb_gmres_anchored_aux_bytes"}
     assert declared <= bound, declared - bound
 
 
@@ -156,3 +156,39 @@ def test_gmres_bad_options_rejected_before_any_launch(field, value):
                                     infos, None)
     assert rc == _lib.EB_ERR_ARG
     assert "bad options" in lib.eb_last_error().decode()
+
+
+def test_anchor_shifts_groups_by_magnitude():
+    """Anchors: consecutive groups of shifts ordered by magnitude, each anchored at the group's
+    geometric-mean magnitude in its middle shift's direction; at most 8 systems per anchor."""
+    from pyeulerale_b200.solver import anchor_shifts
+
+    ks = np.logspace(-2, 1, 64)
+    shifts = 1j * ks[::-1]  # any order
+    anchors, sa = anchor_shifts(shifts, 4)
+    assert len(anchors) == 16 and np.bincount(sa).tolist() == [4] * 16
+    for a in range(16):
+        g = shifts[sa == a]
+        assert np.all(np.abs(g.real) == 0) and abs(anchors[a].real) == 0
+        assert min(abs(g)) <= abs(anchors[a]) <= max(abs(g))
+        np.testing.assert_allclose(abs(anchors[a]), np.exp(np.mean(np.log(abs(g)))), rtol=1e-14)
+    anchors, sa = anchor_shifts([0.0, 1j, 2j], 2)
+    assert sa.tolist() == [0, 0, 1] and anchors[0] == 0.5j and anchors[1] == 2j
+    with pytest.raises(ValueError):
+        anchor_shifts(shifts, 9)
+
+
+def test_anchored_aux_bytes_validates_assignment():
+    """eb_gmres_anchored_aux_bytes (host only) rejects anchors out of range and more than eight
+    systems on one anchor, and grows with the systems per anchor."""
+    from pyeulerale_b200.solver import _bind_anchored
+
+    lib = _bind_anchored()
+    def aux(sa, n_anchors):
+        a = np.ascontiguousarray(sa, dtype=np.int32)
+        return lib.eb_gmres_anchored_aux_bytes(32, 32, len(a), n_anchors, a.ctypes.data)
+    assert aux([0, 0, 1, 1], 2) > 0
+    assert aux([0] * 8, 1) > aux([0] * 4, 1) > 0
+    assert aux([0] * 9, 1) == -1
+    assert aux([0, 2], 2) == -1
+    assert aux([-1, 0], 2) == -1
