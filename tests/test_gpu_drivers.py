@@ -79,7 +79,8 @@ def test_anchored_gmres_residuals_and_fallback(solver, cuda):
     lu.factor(solver._dJ_u, anchors)
     _, info = solve_anchored(solver._batch(), solver._dJ_u, rhs, shifts, lu, sa, maxiter=1,
                              raise_on_failure=False)
-    assert not any(i["converged"] for i in info)
+    # (the middle shift of a log-spaced group is its anchor and converges at once)
+    assert not all(i["converged"] for i in info), info
 
 
 def test_adjoint_lift_gradient_dot_product(solver):
