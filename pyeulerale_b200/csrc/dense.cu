@@ -428,7 +428,26 @@ __global__ void __launch_bounds__(256) k_zgemm_skinny(int n, int nr, double alph
 #pragma unroll
   for (int q = 0; q < kMaxRhs; ++q) sr[q] = si[q] = 0.0;
   if (i < n) {
-    for (int j = g; j < n; j += 8) {
+    // kUnroll columns per step, their loads issued together (the product is bound by the
+    // latency of these loads otherwise: one read of A per column)
+    constexpr int kUnroll = 8;
+    int j = g;
+    for (; j + 8 * (kUnroll - 1) < n; j += 8 * kUnroll) {
+      double2 a[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) a[u] = A[i + (int64_t)lda * (j + 8 * u)];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+        for (int q = 0; q < kMaxRhs; ++q) {
+          if (q < nr) {
+            const double2 v = Bs[j + 8 * u + n * q];
+            sr[q] = fma(a[u].x, v.x, fma(-a[u].y, v.y, sr[q]));
+            si[q] = fma(a[u].x, v.y, fma(a[u].y, v.x, si[q]));
+          }
+        }
+    }
+    for (; j < n; j += 8) {
       const double2 a = A[i + (int64_t)lda * j];
 #pragma unroll
       for (int q = 0; q < kMaxRhs; ++q) {

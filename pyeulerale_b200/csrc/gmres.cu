@@ -521,7 +521,7 @@ __global__ void k_combine(const Sys* sys, int n_sys, int64_t n_cells, const int*
 struct Layout {
   int64_t n_cells = 0, n_chunks = 0;
   int m = 0, S = 0;
-  size_t off_sys, off_active, off_state, off_V, off_z, off_t, off_H, off_cs, off_g, off_y,
+  size_t off_sys, off_active, off_arn, off_state, off_V, off_z, off_t, off_H, off_cs, off_g, off_y,
       off_h1, off_h2, off_n2, off_part, total;
 };
 
@@ -542,6 +542,7 @@ Layout plan(int S, int64_t n_cells, int64_t n_chunks, int m) {
   const size_t vec = (size_t)n_cells * 8 * sizeof(double);
   L.off_sys = take(sizeof(Sys) * S);
   L.off_active = take(sizeof(int) * S);
+  L.off_arn = take(sizeof(int) * S);
   L.off_state = take(sizeof(State) * S);
   L.off_V = take(vec * (m + 1));
   L.off_z = take(vec);
@@ -658,6 +659,10 @@ int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J
   char* ws = static_cast<char*>(workspace);
   Sys* d_sys = reinterpret_cast<Sys*>(ws + L.off_sys);
   int* d_active = reinterpret_cast<int*>(ws + L.off_active);
+  // Arnoldi-active systems: the cycle's active systems whose residual estimate has not yet
+  // reached the tolerance; a system that has stops its Arnoldi steps (its basis and
+  // Hessenberg columns so far give its update at the end of the cycle)
+  int* d_arn = reinterpret_cast<int*>(ws + L.off_arn);
   State* d_state = reinterpret_cast<State*>(ws + L.off_state);
   double* V = reinterpret_cast<double*>(ws + L.off_V);
   double* z = reinterpret_cast<double*>(ws + L.off_z);
@@ -684,30 +689,30 @@ int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J
 
   const int gc = grid_for(n_cells, 128);
   const int gs = (n_sys + 127) / 128;
-  auto norms2 = [&](const double* w, double* out) {
-    k_partial<<<(unsigned)n_chunks, 256, 0, st_>>>(d_sys, n_sys, n_chunks, d_active, nullptr, 0, 0,
+  auto norms2 = [&](const int* flags, const double* w, double* out) {
+    k_partial<<<(unsigned)n_chunks, 256, 0, st_>>>(d_sys, n_sys, n_chunks, flags, nullptr, 0, 0,
                                                    w, part, part_stride);
-    k_reduce<<<n_sys, 256, 0, st_>>>(d_sys, n_sys, d_active, 0, part, part_stride, out, 1);
+    k_reduce<<<n_sys, 256, 0, st_>>>(d_sys, n_sys, flags, 0, part, part_stride, out, 1);
   };
 
-  // out = P^-1 in (accumulate: out += P^-1 in) for the active systems
-  auto prec = [&](const double* in, double* out, int accumulate) {
+  // out = P^-1 in (accumulate: out += P^-1 in) for the systems with flags[s]
+  auto prec = [&](const int* flags, const double* in, double* out, int accumulate) {
     if (!ap) {
-      k_prec<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, in, out,
+      k_prec<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, flags, J, adjoint, in, out,
                                   accumulate);
       return EB_OK;
     }
     return rl::anchored_apply(ap->M, ap->N, ap->ringlu_ws, ap->ringlu_stride, ap->n_anchors,
-                              ap->nr, n_sys, ap->d_sys_anchor, ap->d_sys_col, d_active,
+                              ap->nr, n_sys, ap->d_sys_anchor, ap->d_sys_col, flags,
                               ap->d_zmap, ap->d_n_active, ap->Y, ap->X, ap->W, ap->mstride, in,
                               out, (int64_t)ap->M * ap->N * 8, accumulate, st_);
   };
-  // the anchored preconditioner works on the anchors that still have an active system
-  auto prec_active = [&]() {
+  // the anchored preconditioner works on the anchors that have a system with flags[s]
+  auto prec_active = [&](const std::vector<int>& flags) {
     if (!ap) return EB_OK;
     std::vector<char> any(ap->n_anchors, 0);
     for (int s = 0; s < n_sys; ++s)
-      if (active[s]) any[ap->sys_anchor[s]] = 1;
+      if (flags[s]) any[ap->sys_anchor[s]] = 1;
     ap->zmap.clear();
     for (int a = 0; a < ap->n_anchors; ++a)
       if (any[a]) ap->zmap.push_back(a);
@@ -723,12 +728,13 @@ int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J
   };
 
   // ||b|| (kept in n2[S + s]) and the initial residual r = b - A x0 with x0 = 0.
-  norms2(rhs, n2 + n_sys);
+  norms2(d_active, rhs, n2 + n_sys);
   if (!opt->use_initial_guess) cudaMemsetAsync(x, 0, sizeof(double) * 8 * n_cells, st_);
   k_op<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, x, rhs, V);
-  norms2(V, n2);
+  norms2(d_active, V, n2);
 
   std::vector<double> hn2(2 * n_sys);
+  std::vector<int> arn(n_sys, 0);
   int total_iters = 0;
   int status = EB_OK;
   int cycles = 0;
@@ -757,7 +763,9 @@ int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J
       break;
     }
     cudaMemcpyAsync(d_active, active.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice, st_);
-    if ((rc = prec_active()) != EB_OK) return rc;
+    arn = active;
+    cudaMemcpyAsync(d_arn, arn.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice, st_);
+    if ((rc = prec_active(arn)) != EB_OK) return rc;
     ++cycles;
     k_cycle_start<<<gs, 128, 0, st_>>>(n_sys, d_active, m, n2, g, d_state);
     k_scale<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, d_state, V);
@@ -765,41 +773,53 @@ int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J
     for (; j < m && total_iters < opt->max_iterations; ++j, ++total_iters) {
       double* vj = V + (int64_t)j * vstride;
       double* w = V + (int64_t)(j + 1) * vstride;
-      if ((rc = prec(vj, z, 0)) != EB_OK) return rc;
-      k_op<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, z, nullptr, w);
+      if ((rc = prec(d_arn, vj, z, 0)) != EB_OK) return rc;
+      k_op<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_arn, J, adjoint, z, nullptr, w);
       for (int pass = 0; pass < 2; ++pass) {
         double* h = pass == 0 ? h1 : h2;
-        k_partial<<<(unsigned)n_chunks, 256, 0, st_>>>(d_sys, n_sys, n_chunks, d_active, V,
+        k_partial<<<(unsigned)n_chunks, 256, 0, st_>>>(d_sys, n_sys, n_chunks, d_arn, V,
                                                        vstride, j + 1, w, part, part_stride);
-        k_reduce<<<n_sys, 256, 0, st_>>>(d_sys, n_sys, d_active, j + 1, part, part_stride, h, hs);
-        k_project<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, V, vstride, j + 1, h, hs, w);
+        k_reduce<<<n_sys, 256, 0, st_>>>(d_sys, n_sys, d_arn, j + 1, part, part_stride, h, hs);
+        k_project<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_arn, V, vstride, j + 1, h, hs, w);
       }
-      norms2(w, n2);
-      k_givens<<<gs, 128, 0, st_>>>(n_sys, d_active, j, m, h1, h2, hs, n2, H, cs, g, d_state);
-      k_scale<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, d_state, w);
+      norms2(d_arn, w, n2);
+      k_givens<<<gs, 128, 0, st_>>>(n_sys, d_arn, j, m, h1, h2, hs, n2, H, cs, g, d_state);
+      k_scale<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_arn, d_state, w);
       if (((j + 1) % opt->check_every) == 0 || j + 1 == m) {
         if (cudaMemcpyAsync(hst.data(), d_state, sizeof(State) * n_sys, cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
             cudaStreamSynchronize(st_) != cudaSuccess)
           return check_launch("gmres state read");
-        bool all_done = true;
+        // systems whose estimate has reached the tolerance (or that broke down) stop here
+        bool all_done = true, changed = false;
         for (int s = 0; s < n_sys; ++s) {
-          if (!active[s]) continue;
+          if (!arn[s]) continue;
           const double bn = std::sqrt(hn2[n_sys + s]);
-          if (!(hst[s].breakdown || hst[s].est <= 0.5 * opt->tol * bn)) all_done = false;
+          if (hst[s].breakdown || hst[s].est <= 0.5 * opt->tol * bn) {
+            arn[s] = 0;
+            changed = true;
+          } else {
+            all_done = false;
+          }
         }
         if (all_done) {
           ++j;
           ++total_iters;
           break;
         }
+        if (changed) {
+          cudaMemcpyAsync(d_arn, arn.data(), sizeof(int) * n_sys, cudaMemcpyHostToDevice, st_);
+          if ((rc = prec_active(arn)) != EB_OK) return rc;
+        }
       }
     }
-    // x += P^-1 (V y), then the true residual
+    // x += P^-1 (V y) for every system of the cycle (each with its own number of steps), then
+    // the true residual
+    if (ap && (rc = prec_active(active)) != EB_OK) return rc;
     k_backsolve<<<gs, 128, 0, st_>>>(n_sys, d_active, m, H, g, y, d_state);
     k_combine<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, V, vstride, m, y, d_state, t);
-    if ((rc = prec(t, x, 1)) != EB_OK) return rc;
+    if ((rc = prec(d_active, t, x, 1)) != EB_OK) return rc;
     k_op<<<gc, 128, 0, st_>>>(d_sys, n_sys, n_cells, d_active, J, adjoint, x, rhs, V);
-    norms2(V, n2);
+    norms2(d_active, V, n2);
     rc = check_launch("gmres cycle");
     if (rc != EB_OK) return rc;
   }
