@@ -82,7 +82,8 @@ def parse_args():
                    help="instances of each size timed one at a time for the comparison")
     p.add_argument("--workspace-gb", type=float, default=80.0,
                    help="device memory for batched factorisations")
-    p.add_argument("--profile-region", choices=["none", "residual", "batched"], default="none",
+    p.add_argument("--profile-region", choices=["none", "residual", "batched", "anchored"],
+                   default="none",
                    help="bracket one region with cudaProfilerStart/Stop (for "
                         "ncu --profile-from-start off): the timed residual launches or the "
                         "batched frequency response")
@@ -938,9 +939,13 @@ def run_b200(args) -> None:
         stats = {}
         barrier()
         t0 = time.perf_counter()
+        if args.profile_region == "anchored":
+            torch.cuda.profiler.start()
         cl_a, cm_a = drivers.frequency_response_batched(sd, GRID["chord"], FLOW["center"][0],
                                                         ks, method="anchored",
                                                         per_anchor=args.per_anchor, stats=stats)
+        if args.profile_region == "anchored":
+            torch.cuda.profiler.stop()
         grad_a = drivers.adjoint_lift_gradient(sd)
         barrier()
         t_anch = max_over_ranks(time.perf_counter() - t0)
