@@ -52,6 +52,15 @@ __device__ __forceinline__ void mma884(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
+// A 16-byte read-only load that the compiler keeps in program order with the other such loads,
+// so that a thread's unrolled loads of a matrix are all in flight before the first is used (left
+// to itself the compiler may sink each load next to its use, one DRAM latency per column).
+__device__ __forceinline__ double2 ldg_inflight(const double2* p) {
+  double2 v;
+  asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+
 // Global -> registers for one kBK slice: each thread holds kBM * kBK / kGemmThreads complex
 // elements of A and kBK * kBN / kGemmThreads of B (zero outside the matrices).
 constexpr int kAPer = kBM * kBK / kGemmThreads;  // 8
@@ -338,7 +347,20 @@ __global__ void __launch_bounds__(256) k_zgemv_n(int n, double alpha, const doub
   const int i = blockIdx.x * 32 + r;
   double sr = 0.0, si = 0.0;
   if (i < n) {
-    for (int j = g; j < n; j += 8) {
+    constexpr int kUnroll = 8;  // column loads in flight per thread (ldg_inflight)
+    int j = g;
+    for (; j + 8 * (kUnroll - 1) < n; j += 8 * kUnroll) {
+      double2 a[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) a[u] = ldg_inflight(A + i + (int64_t)lda * (j + 8 * u));
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const double2 v = x[j + 8 * u];
+        sr = fma(a[u].x, v.x, fma(-a[u].y, v.y, sr));
+        si = fma(a[u].x, v.y, fma(a[u].y, v.x, si));
+      }
+    }
+    for (; j < n; j += 8) {
       const double2 a = A[i + (int64_t)lda * j], v = x[j];
       sr = fma(a.x, v.x, fma(-a.y, v.y, sr));
       si = fma(a.x, v.y, fma(a.y, v.x, si));
@@ -376,7 +398,20 @@ __global__ void __launch_bounds__(256) k_zgemv_c(int n, double alpha, const doub
   if (j >= n) return;
   const double2* col = A + (int64_t)lda * j;
   double sr = 0.0, si = 0.0;
-  for (int i = lane; i < n; i += 32) {  // conj(a) v
+  constexpr int kUnroll = 8;  // row loads in flight per lane (ldg_inflight)
+  int i = lane;
+  for (; i + 32 * (kUnroll - 1) < n; i += 32 * kUnroll) {  // conj(a) v
+    double2 a[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) a[u] = ldg_inflight(col + i + 32 * u);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const double2 v = x[i + 32 * u];
+      sr = fma(a[u].x, v.x, fma(a[u].y, v.y, sr));
+      si = fma(a[u].x, v.y, fma(-a[u].y, v.x, si));
+    }
+  }
+  for (; i < n; i += 32) {
     const double2 a = col[i], v = x[i];
     sr = fma(a.x, v.x, fma(a.y, v.y, sr));
     si = fma(a.x, v.y, fma(-a.y, v.x, si));
@@ -417,9 +452,22 @@ __global__ void __launch_bounds__(256) k_zgemm_skinny(int n, int nr, double alph
   A += sa * z;
   B += sb * z;
   C += sc * z;
-  for (int e = threadIdx.x; e < n * nr; e += blockDim.x) {
-    const int q = e / n, j = e - q * n;
-    Bs[e] = B[j + (int64_t)ldb * q];
+  const int total = n * nr;
+  for (int e0 = 0; e0 < total; e0 += 8 * 256) {  // eight loads in flight per thread
+    double2 b[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + 256 * u + (int)threadIdx.x;
+      if (e < total) {
+        const int q = e / n, j = e - q * n;
+        b[u] = ldg_inflight(B + j + (int64_t)ldb * q);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + 256 * u + (int)threadIdx.x;
+      if (e < total) Bs[e] = b[u];
+    }
   }
   __syncthreads();
   const int r = threadIdx.x & 31, g = threadIdx.x >> 5;
@@ -435,7 +483,7 @@ __global__ void __launch_bounds__(256) k_zgemm_skinny(int n, int nr, double alph
     for (; j + 8 * (kUnroll - 1) < n; j += 8 * kUnroll) {
       double2 a[kUnroll];
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) a[u] = A[i + (int64_t)lda * (j + 8 * u)];
+      for (int u = 0; u < kUnroll; ++u) a[u] = ldg_inflight(A + i + (int64_t)lda * (j + 8 * u));
 #pragma unroll
       for (int u = 0; u < kUnroll; ++u)
 #pragma unroll
