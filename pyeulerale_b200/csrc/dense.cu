@@ -441,14 +441,18 @@ __global__ void __launch_bounds__(256) k_zgemv_c(int n, double alpha, const doub
 // rank order through distributed shared memory and writes C. Spreading a product over the
 // cluster puts eight SMs' loads in flight where one CTA per 32 rows left each SM streaming
 // its 256 KB share alone. Batch entry z (grid z) uses A + zmap[z] sa etc. (zmap == nullptr: z
-// itself); entries z >= *n_batch exit (the whole cluster alike).
+// itself); entries z >= *n_batch exit (the whole cluster alike). With bd != nullptr the
+// epilogue also subtracts Bd V, Bd being n / 4 real 4 x 4 blocks (column-major) at
+// bd + zmap[z] bd_stride bytes and V (n x nr, leading dimension ldc) at V + zmap[z] sv: the ring
+// LU's block-diagonal coupling, fused into the product that precedes it.
 constexpr int kMaxRhs = 8;
 constexpr int kSkCluster = 8;
 
 __global__ void __cluster_dims__(1, kSkCluster, 1) __launch_bounds__(256)
     k_zgemm_skinny(int n, int nr, double alpha, const double2* A, int lda, int64_t sa,
                    const double2* B, int ldb, int64_t sb, double beta, double2* C, int ldc,
-                   int64_t sc, const int* zmap, const int* n_batch) {
+                   int64_t sc, const int* zmap, const int* n_batch, const char* bd,
+                   int64_t bd_stride, const double2* V, int64_t sv) {
   extern __shared__ __align__(16) unsigned char sk_smem[];
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
@@ -457,6 +461,8 @@ __global__ void __cluster_dims__(1, kSkCluster, 1) __launch_bounds__(256)
   A += sa * z;
   B += sb * z;
   C += sc * z;
+  const double* Bd = bd ? reinterpret_cast<const double*>(bd + bd_stride * z) : nullptr;
+  if (V) V += sv * z;
   const int rank = (int)cluster.block_rank();
   const int share = (((n + kSkCluster - 1) / kSkCluster) + 7) / 8 * 8;  // columns per CTA
   const int j0 = rank * share, j1 = min(n, j0 + share);
@@ -552,6 +558,17 @@ __global__ void __cluster_dims__(1, kSkCluster, 1) __launch_bounds__(256)
           o.x = fma(beta, out->x, o.x);
           o.y = fma(beta, out->y, o.y);
         }
+        if (Bd) {  // - Bd V for row = 4 blk + rr4
+          const int blk = row >> 2, rr4 = row & 3;
+          const double* b = Bd + 16 * blk;
+          const double2* v = V + (int64_t)ldc * q + 4 * blk;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const double bk = b[rr4 + 4 * k];
+            o.x = fma(-bk, v[k].x, o.x);
+            o.y = fma(-bk, v[k].y, o.y);
+          }
+        }
         *out = o;
       }
     }
@@ -580,7 +597,9 @@ int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A,
 int zgemm_skinny_batched(int n, int nr, double alpha, const cuDoubleComplex* A, int lda,
                          int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
                          double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
-                         const int* zmap, const int* n_batch, cudaStream_t st) {
+                         const int* zmap, const int* n_batch, cudaStream_t st, const void* bd,
+                         int64_t bd_stride, const cuDoubleComplex* V, int64_t stride_v) {
+  if (bd && n % 4 != 0) return fail(EB_ERR_ARG, "zgemm_skinny: block diagonal needs n % 4 == 0");
   if (n <= 0 || batch <= 0 || nr <= 0) return 0;
   if (nr > kMaxRhs) return fail(EB_ERR_ARG, "zgemm_skinny: too many right-hand sides");
   const int share = (((n + kSkCluster - 1) / kSkCluster) + 7) / 8 * 8;
@@ -592,7 +611,8 @@ int zgemm_skinny_batched(int n, int nr, double alpha, const cuDoubleComplex* A, 
   k_zgemm_skinny<<<dim3((n + 31) / 32, kSkCluster, batch), 256, smem, st>>>(
       n, nr, alpha, reinterpret_cast<const double2*>(A), lda, stride_a,
       reinterpret_cast<const double2*>(B), ldb, stride_b, beta, reinterpret_cast<double2*>(C),
-      ldc, stride_c, zmap, n_batch);
+      ldc, stride_c, zmap, n_batch, static_cast<const char*>(bd), bd_stride,
+      reinterpret_cast<const double2*>(V), stride_v);
   return check_launch("zgemm_skinny");
 }
 

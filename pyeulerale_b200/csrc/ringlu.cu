@@ -908,32 +908,6 @@ int ring_solve(const Group& g, bool adjoint, cudaStream_t stream) {
 // launches cover the anchors zmap[0 .. *n_active - 1] (device arrays), so anchors whose systems
 // have all converged drop out without a change of launch shape.
 
-// Out -= Bd V for the nr columns (Bd: N real 4 x 4 blocks of the anchor's workspace at off_bd).
-__global__ void __launch_bounds__(128) k_bd_mat(int N, int nr, const char* ws0, int64_t stride,
-                                                size_t off_bd, const cuDoubleComplex* V,
-                                                cuDoubleComplex* Out, int64_t mstride,
-                                                const int* zmap, const int* n_active) {
-  if ((int)blockIdx.y >= *n_active) return;
-  const int a = zmap[blockIdx.y];
-  const double* B = reinterpret_cast<const double*>(ws0 + (int64_t)a * stride + off_bd);
-  const int K = 4 * N;
-  V += (int64_t)a * mstride;
-  Out += (int64_t)a * mstride;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K * nr; e += gridDim.x * blockDim.x) {
-    const int q = e / K, row = e - q * K, n = row >> 2, r = row & 3;
-    const double* b = B + 16 * n;
-    const cuDoubleComplex* vn = V + (int64_t)q * K + 4 * n;
-    cuDoubleComplex acc = Out[e];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const double bi = b[r + 4 * i];
-      acc.x = fma(-bi, vn[i].x, acc.x);
-      acc.y = fma(-bi, vn[i].y, acc.y);
-    }
-    Out[e] = acc;
-  }
-}
-
 // System vectors (reference layout, system s at in + s * vstride doubles) -> column sys_col[s]
 // of anchor sys_anchor[s]'s ring blocks.
 __global__ void k_sys_to_multi(int M, int N, int nr, int n_sys, const int* sys_anchor,
@@ -993,29 +967,33 @@ int ring_solve_multi(const Group& g, int nr, cuDoubleComplex* Y, cuDoubleComplex
                      cuDoubleComplex* W, int64_t mstride, const int* zmap, const int* n_active,
                      cudaStream_t st) {
   const Layout& L = g.L;
-  const int M = L.M, K = L.K, N = L.N;
+  const int M = L.M, K = L.K;
   const int64_t es = g.es();
   auto blk = [&](cuDoubleComplex* base, int m) { return base + (size_t)K * nr * m; };
   int rc = EB_OK;
+  // C = alpha A B + beta C [- Bd V: the block-diagonal coupling at off_bd, fused into the
+  // product's epilogue]
   auto gemm = [&](double alpha, const cuDoubleComplex* A, const cuDoubleComplex* B, double beta,
-                  cuDoubleComplex* C) {
+                  cuDoubleComplex* C, size_t off_bd = 0, const cuDoubleComplex* V = nullptr) {
     if (rc == EB_OK)
       rc = dense::zgemm_skinny_batched(K, nr, alpha, A, K, es, B, K, mstride, beta, C, K,
-                                       mstride, g.S, zmap, n_active, st);
-  };
-  const dim3 bdg((K * nr + 127) / 128, g.S);
-  auto bd = [&](size_t off_bd, const cuDoubleComplex* V, cuDoubleComplex* Out) {
-    k_bd_mat<<<bdg, 128, 0, st>>>(N, nr, g.base, g.stride, off_bd, V, Out, mstride, zmap,
-                                  n_active);
+                                       mstride, g.S, zmap, n_active, st,
+                                       V ? g.base + off_bd : nullptr, g.stride, V, mstride);
   };
   for (int m = 0; m < M; ++m) {  // Lt z = b (z in Y), W[m] = Dinv_m z[m]
-    if (m >= 1) gemm(-1.0, g.blk(L.off_L1, m), blk(Y, m - 1), 1.0, blk(Y, m));
-    if (m >= 2) bd(L.off_B2 + L.bdr * m, blk(W, m - 2), blk(Y, m));
+    if (m >= 2)
+      gemm(-1.0, g.blk(L.off_L1, m), blk(Y, m - 1), 1.0, blk(Y, m), L.off_B2 + L.bdr * m,
+           blk(W, m - 2));
+    else if (m == 1)
+      gemm(-1.0, g.blk(L.off_L1, m), blk(Y, m - 1), 1.0, blk(Y, m));
     if (m + 2 < M) gemm(1.0, g.blk(L.off_D, m), blk(Y, m), 0.0, blk(W, m));
   }
   for (int m = M - 1; m >= 0; --m) {  // Ut x = z
-    if (m + 1 < M) gemm(-1.0, g.blk(L.off_C1, m), blk(X, m + 1), 1.0, blk(Y, m));
-    if (m + 2 < M) bd(L.off_C2 + L.bdr * m, blk(X, m + 2), blk(Y, m));
+    if (m + 2 < M)
+      gemm(-1.0, g.blk(L.off_C1, m), blk(X, m + 1), 1.0, blk(Y, m), L.off_C2 + L.bdr * m,
+           blk(X, m + 2));
+    else if (m + 1 < M)
+      gemm(-1.0, g.blk(L.off_C1, m), blk(X, m + 1), 1.0, blk(Y, m));
     gemm(1.0, g.blk(L.off_D, m), blk(Y, m), 0.0, blk(X, m));
   }
   if (rc != EB_OK) return rc;
