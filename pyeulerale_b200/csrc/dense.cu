@@ -14,6 +14,7 @@
 // both), with no register staging; it issues the same MMAs in the same order, so the two
 // variants give identical results.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -431,6 +432,150 @@ __global__ void __launch_bounds__(256) k_zgemv_c(int n, double alpha, const doub
   }
 }
 
+// C = alpha A B + beta C with A n x n and B, C n x nr (nr <= kMaxRhs right-hand sides): the
+// multi-right-hand-side form of k_zgemv_n (one read of A serves all nr columns). A cluster of
+// kSkCluster CTAs takes 32 rows: CTA c of the cluster sums the columns of its contiguous share,
+// thread (r, g) of its 256 the columns j = g (mod 8) of that share for row r and every
+// right-hand side, with eight column loads in flight; the eight warps' partial sums are added
+// in a fixed order in shared memory, and the cluster's leader adds the CTAs' partial sums in
+// rank order through distributed shared memory and writes C. Spreading a product over the
+// cluster puts eight SMs' loads in flight where one CTA per 32 rows left each SM streaming
+// its 256 KB share alone. Batch entry z (grid z) uses A + zmap[z] sa etc. (zmap == nullptr: z
+// itself); entries z >= *n_batch exit (the whole cluster alike). With bd != nullptr the
+// epilogue also subtracts Bd V, Bd being n / 4 real 4 x 4 blocks (column-major) at
+// bd + zmap[z] bd_stride bytes and V (n x nr, leading dimension ldc) at V + zmap[z] sv: the ring
+// LU's block-diagonal coupling, fused into the product that precedes it.
+constexpr int kMaxRhs = 8;
+constexpr int kSkCluster = 8;
+
+__global__ void __cluster_dims__(1, kSkCluster, 1) __launch_bounds__(256)
+    k_zgemm_skinny(int n, int nr, double alpha, const double2* A, int lda, int64_t sa,
+                   const double2* B, int ldb, int64_t sb, double beta, double2* C, int ldc,
+                   int64_t sc, const int* zmap, const int* n_batch, const char* bd,
+                   int64_t bd_stride, const double2* V, int64_t sv) {
+  extern __shared__ __align__(16) unsigned char sk_smem[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  if (n_batch && (int)blockIdx.z >= *n_batch) return;  // uniform over the cluster
+  const int64_t z = zmap ? zmap[blockIdx.z] : blockIdx.z;
+  A += sa * z;
+  B += sb * z;
+  C += sc * z;
+  const double* Bd = bd ? reinterpret_cast<const double*>(bd + bd_stride * z) : nullptr;
+  if (V) V += sv * z;
+  const int rank = (int)cluster.block_rank();
+  const int share = (((n + kSkCluster - 1) / kSkCluster) + 7) / 8 * 8;  // columns per CTA
+  const int j0 = rank * share, j1 = min(n, j0 + share);
+  const int cols = max(j1 - j0, 0);
+  double2* Bs = reinterpret_cast<double2*>(sk_smem);  // cols x nr (this CTA's rows of B)
+  double2* part = Bs + (size_t)share * nr;            // 8 x 32 x nr, then the CTA's 32 x nr
+  const int total = cols * nr;
+  for (int e0 = 0; e0 < total; e0 += 8 * 256) {  // eight loads in flight per thread
+    double2 b[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + 256 * u + (int)threadIdx.x;
+      if (e < total) {
+        const int q = e / cols, j = e - q * cols;
+        b[u] = ldg_inflight(B + j0 + j + (int64_t)ldb * q);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + 256 * u + (int)threadIdx.x;
+      if (e < total) Bs[e] = b[u];
+    }
+  }
+  __syncthreads();
+  const int r = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + r;
+  double sr[kMaxRhs], si[kMaxRhs];
+#pragma unroll
+  for (int q = 0; q < kMaxRhs; ++q) sr[q] = si[q] = 0.0;
+  if (i < n) {
+    constexpr int kUnroll = 8;
+    int j = g;
+    for (; j + 8 * (kUnroll - 1) < cols; j += 8 * kUnroll) {
+      double2 a[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u)
+        a[u] = ldg_inflight(A + i + (int64_t)lda * (j0 + j + 8 * u));
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+        for (int q = 0; q < kMaxRhs; ++q) {
+          if (q < nr) {
+            const double2 v = Bs[j + 8 * u + cols * q];
+            sr[q] = fma(a[u].x, v.x, fma(-a[u].y, v.y, sr[q]));
+            si[q] = fma(a[u].x, v.y, fma(a[u].y, v.x, si[q]));
+          }
+        }
+    }
+    for (; j < cols; j += 8) {
+      const double2 a = A[i + (int64_t)lda * (j0 + j)];
+#pragma unroll
+      for (int q = 0; q < kMaxRhs; ++q) {
+        if (q < nr) {
+          const double2 v = Bs[j + cols * q];
+          sr[q] = fma(a.x, v.x, fma(-a.y, v.y, sr[q]));
+          si[q] = fma(a.x, v.y, fma(a.y, v.x, si[q]));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kMaxRhs; ++q)
+    if (q < nr) part[(q * 8 + g) * 32 + r] = make_double2(sr[q], si[q]);
+  __syncthreads();
+  // the CTA's partial sums (warps in order) into part[q * 32 + r] (after the 8 x 32 x nr block)
+  double2* mine = part + 8 * 32 * nr;
+  for (int e = threadIdx.x; e < 32 * nr; e += 256) {
+    const int q = e >> 5, rr = e & 31;
+    double tr = 0.0, ti = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      tr += part[(q * 8 + k) * 32 + rr].x;
+      ti += part[(q * 8 + k) * 32 + rr].y;
+    }
+    mine[e] = make_double2(tr, ti);
+  }
+  cluster.sync();  // every CTA's partial sums are visible to the leader
+  if (rank == 0) {
+    for (int e = threadIdx.x; e < 32 * nr; e += 256) {
+      const int q = e >> 5, rr = e & 31;
+      const int row = blockIdx.x * 32 + rr;
+      double tr = 0.0, ti = 0.0;
+      for (int c = 0; c < kSkCluster; ++c) {
+        const double2* other = cluster.map_shared_rank(mine, c);
+        const double2 v = other[e];
+        tr += v.x;
+        ti += v.y;
+      }
+      if (row < n) {
+        double2* out = C + row + (int64_t)ldc * q;
+        double2 o = make_double2(alpha * tr, alpha * ti);
+        if (beta != 0.0) {
+          o.x = fma(beta, out->x, o.x);
+          o.y = fma(beta, out->y, o.y);
+        }
+        if (Bd) {  // - Bd V for row = 4 blk + rr4
+          const int blk = row >> 2, rr4 = row & 3;
+          const double* b = Bd + 16 * blk;
+          const double2* v = V + (int64_t)ldc * q + 4 * blk;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const double bk = b[rr4 + 4 * k];
+            o.x = fma(-bk, v[k].x, o.x);
+            o.y = fma(-bk, v[k].y, o.y);
+          }
+        }
+        *out = o;
+      }
+    }
+  }
+  cluster.sync();  // the leader has read every CTA's shared memory before any exits
+}
+
 }  // namespace
 
 int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A, int lda,
@@ -447,6 +592,28 @@ int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A,
     k_zgemv_n<<<dim3((n + 31) / 32, batch), 256, 0, st>>>(n, alpha, a, lda, stride_a, v,
                                                           stride_x, beta, w, stride_y);
   return check_launch("zgemv");
+}
+
+int zgemm_skinny_batched(int n, int nr, double alpha, const cuDoubleComplex* A, int lda,
+                         int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
+                         double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
+                         const int* zmap, const int* n_batch, cudaStream_t st, const void* bd,
+                         int64_t bd_stride, const cuDoubleComplex* V, int64_t stride_v) {
+  if (bd && n % 4 != 0) return fail(EB_ERR_ARG, "zgemm_skinny: block diagonal needs n % 4 == 0");
+  if (n <= 0 || batch <= 0 || nr <= 0) return 0;
+  if (nr > kMaxRhs) return fail(EB_ERR_ARG, "zgemm_skinny: too many right-hand sides");
+  const int share = (((n + kSkCluster - 1) / kSkCluster) + 7) / 8 * 8;
+  const size_t smem = sizeof(double2) * ((size_t)share * nr + 9 * 32 * (size_t)nr);
+  if (smem > 200 * 1024) return fail(EB_ERR_ARG, "zgemm_skinny: right-hand sides too large");
+  if (cudaFuncSetAttribute(k_zgemm_skinny, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return check_launch("zgemm_skinny attribute");
+  k_zgemm_skinny<<<dim3((n + 31) / 32, kSkCluster, batch), 256, smem, st>>>(
+      n, nr, alpha, reinterpret_cast<const double2*>(A), lda, stride_a,
+      reinterpret_cast<const double2*>(B), ldb, stride_b, beta, reinterpret_cast<double2*>(C),
+      ldc, stride_c, zmap, n_batch, static_cast<const char*>(bd), bd_stride,
+      reinterpret_cast<const double2*>(V), stride_v);
+  return check_launch("zgemm_skinny");
 }
 
 }  // namespace dense

@@ -29,5 +29,18 @@ int zgemv_batched(int conj_trans, int n, double alpha, const cuDoubleComplex* A,
                   int64_t stride_a, const cuDoubleComplex* x, int64_t stride_x, double beta,
                   cuDoubleComplex* y, int64_t stride_y, int batch, cudaStream_t st);
 
+// C_z = alpha A_z B_z + beta C_z with A_z n x n and B_z, C_z n x nr (nr <= 8 right-hand
+// sides), column-major; batch entry z uses A + zmap[z] stride_a (etc.; zmap == nullptr: z), and
+// entries z >= *n_batch (device int; n_batch == nullptr: all) do nothing. beta == 0 does not
+// read C. With bd != nullptr, C_z also takes - Bd_z V_z: Bd_z = n / 4 real column-major 4 x 4
+// blocks at (const char*) bd + zmap[z] bd_stride, V_z (n x nr, leading dimension ldc) at
+// V + zmap[z] stride_v. Returns an EB_* status.
+int zgemm_skinny_batched(int n, int nr, double alpha, const cuDoubleComplex* A, int lda,
+                         int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
+                         double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
+                         const int* zmap, const int* n_batch, cudaStream_t st,
+                         const void* bd = nullptr, int64_t bd_stride = 0,
+                         const cuDoubleComplex* V = nullptr, int64_t stride_v = 0);
+
 }  // namespace dense
 }  // namespace eb

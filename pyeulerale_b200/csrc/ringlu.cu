@@ -39,7 +39,6 @@
 // the pivot rows. After K steps the working array W holds T P (T = product of the elementary
 // transformations), and the inverse is Dinv[j, p_k] = W[p_j, k] (one permuting copy).
 
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -962,210 +961,43 @@ __global__ void k_multi_to_sys(int M, int N, int nr, int n_sys, const int* sys_a
 }
 
 // X = A^-1 Y column by column for the anchors in zmap (A = the anchor's shifted Jacobian): the
-// forward sweep of ring_solve with every matrix-vector product over nr right-hand sides, as one
-// persistent launch. A cluster of kSwCluster CTAs runs one anchor's whole sweep: CTA c owns the
-// rows [c R, (c + 1) R) of every ring product (R = K / kSwCluster rounded up) and a cluster
-// barrier separates dependent products, so the 4 M products of a sweep need no launch each and
-// the anchors' clusters run side by side. Within a CTA, warp (row block, column group) sums
-// its columns of A for 32 rows with eight column loads in flight; the column groups' partial
-// sums are added in a fixed order. Y is overwritten; W is scratch.
-namespace sweep {
-
-constexpr int kSwCluster = 8;
-constexpr int kSwThreads = 512;
-constexpr int kSwWarps = kSwThreads / 32;
-constexpr int kSwMaxRhs = 8;
-
-struct Params {
-  int M, N, nr;
-  const char* ws;
-  int64_t stride;
-  size_t blk, bdr, off_D, off_L1, off_C1, off_B2, off_C2;
-  double2 *Y, *X, *W;
-  int64_t mstride;
-  const int* zmap;
-  const int* n_active;
-  int row_blocks;  // warps per column group: 32-row blocks of a CTA's share (power of two)
-};
-
-__device__ __forceinline__ double2 ld_ro(const double2* p) {  // factors: read-only here
-  double2 v;
-  asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "l"(p));
-  return v;
-}
-
-// C[r0:r1] = alpha A B + beta C[r0:r1] (- Bd V[r0:r1]) for this CTA's rows; A K x K (ld K, the
-// factors), B and C and V K x nr (ld K, vectors written in this launch: read through L2).
-__device__ void product(const Params& P, int K, int r0, int r1, const double2* A,
-                        const double2* B, double alpha, double beta, double2* C,
-                        const double* Bd, const double2* V, double2* Bs, double2* part) {
-  const int nr = P.nr, tid = threadIdx.x;
-  for (int e = tid; e < K * nr; e += kSwThreads) {
-    const int q = e / K, j = e - q * K;
-    Bs[e] = __ldcg(B + j + (int64_t)K * q);
-  }
-  __syncthreads();
-  const int RB = P.row_blocks, G = kSwWarps / RB;
-  const int warp = tid >> 5, lane = tid & 31;
-  const int rb = warp % RB, gg = warp / RB;
-  const int i = r0 + rb * 32 + lane;
-  double sr[kSwMaxRhs], si[kSwMaxRhs];
-#pragma unroll
-  for (int q = 0; q < kSwMaxRhs; ++q) sr[q] = si[q] = 0.0;
-  if (i < r1) {
-    constexpr int kU = 8;
-    int j = gg;
-    for (; j + G * (kU - 1) < K; j += G * kU) {
-      double2 a[kU];
-#pragma unroll
-      for (int u = 0; u < kU; ++u) a[u] = ld_ro(A + i + (int64_t)K * (j + G * u));
-#pragma unroll
-      for (int u = 0; u < kU; ++u)
-#pragma unroll
-        for (int q = 0; q < kSwMaxRhs; ++q) {
-          if (q < nr) {
-            const double2 v = Bs[j + G * u + K * q];
-            sr[q] = fma(a[u].x, v.x, fma(-a[u].y, v.y, sr[q]));
-            si[q] = fma(a[u].x, v.y, fma(a[u].y, v.x, si[q]));
-          }
-        }
-    }
-    for (; j < K; j += G) {
-      const double2 a = ld_ro(A + i + (int64_t)K * j);
-#pragma unroll
-      for (int q = 0; q < kSwMaxRhs; ++q) {
-        if (q < nr) {
-          const double2 v = Bs[j + K * q];
-          sr[q] = fma(a.x, v.x, fma(-a.y, v.y, sr[q]));
-          si[q] = fma(a.x, v.y, fma(a.y, v.x, si[q]));
-        }
-      }
-    }
-  }
-  const int rows = RB * 32;
-#pragma unroll
-  for (int q = 0; q < kSwMaxRhs; ++q)
-    if (q < nr) part[(q * G + gg) * rows + rb * 32 + lane] = make_double2(sr[q], si[q]);
-  __syncthreads();
-  const int nloc = max(r1 - r0, 0);
-  for (int e = tid; e < nloc * nr; e += kSwThreads) {
-    const int q = e / nloc, lr = e - q * nloc, row = r0 + lr;
-    double tr = 0.0, ti = 0.0;
-    for (int k = 0; k < G; ++k) {
-      const double2 v = part[(q * G + k) * rows + lr];
-      tr += v.x;
-      ti += v.y;
-    }
-    double2* c = C + row + (int64_t)K * q;
-    double2 o = make_double2(alpha * tr, alpha * ti);
-    if (beta != 0.0) {
-      const double2 old = __ldcg(c);
-      o.x = fma(beta, old.x, o.x);
-      o.y = fma(beta, old.y, o.y);
-    }
-    if (Bd) {  // - Bd V: row 4 blk + rr4 of the block diagonal
-      const int blk = row >> 2, rr4 = row & 3;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const double bk = Bd[16 * blk + rr4 + 4 * k];
-        const double2 v = __ldcg(V + (int64_t)K * q + 4 * blk + k);
-        o.x = fma(-bk, v.x, o.x);
-        o.y = fma(-bk, v.y, o.y);
-      }
-    }
-    *c = o;
-  }
-}
-
-__global__ void __cluster_dims__(kSwCluster, 1, 1) __launch_bounds__(kSwThreads, 1)
-    k_ring_sweep_multi(Params P) {
-  extern __shared__ __align__(16) unsigned char sw_smem[];
-  namespace cg = cooperative_groups;
-  cg::cluster_group cluster = cg::this_cluster();
-  if ((int)blockIdx.z >= *P.n_active) return;  // uniform over the cluster
-  const int a = P.zmap[blockIdx.z];
-  const int M = P.M, K = 4 * P.N, nr = P.nr;
-  const char* base = P.ws + (int64_t)a * P.stride;
-  const int rank = (int)cluster.block_rank();
-  const int R = (K + kSwCluster - 1) / kSwCluster;
-  const int r0 = rank * R, r1 = min(K, r0 + R);
-  double2* Bs = reinterpret_cast<double2*>(sw_smem);
-  double2* part = Bs + (size_t)K * nr;
-  double2* Y = P.Y + (int64_t)a * P.mstride;
-  double2* X = P.X + (int64_t)a * P.mstride;
-  double2* W = P.W + (int64_t)a * P.mstride;
-  auto vec = [&](double2* v, int m) { return v + (size_t)K * nr * m; };
-  auto mat = [&](size_t off, int m) {
-    return reinterpret_cast<const double2*>(base + off + P.blk * (size_t)m);
-  };
-  auto bd = [&](size_t off, int m) {
-    return reinterpret_cast<const double*>(base + off + P.bdr * (size_t)m);
-  };
-  for (int m = 0; m < M; ++m) {  // Lt z = b (z in Y), W[m] = Dinv_m z[m]
-    if (m >= 1) {
-      product(P, K, r0, r1, mat(P.off_L1, m), vec(Y, m - 1), -1.0, 1.0, vec(Y, m),
-              m >= 2 ? bd(P.off_B2, m) : nullptr, m >= 2 ? vec(W, m - 2) : nullptr, Bs, part);
-      cluster.sync();
-    }
-    if (m + 2 < M) {
-      product(P, K, r0, r1, mat(P.off_D, m), vec(Y, m), 1.0, 0.0, vec(W, m), nullptr, nullptr,
-              Bs, part);
-      cluster.sync();
-    }
-  }
-  for (int m = M - 1; m >= 0; --m) {  // Ut x = z
-    if (m + 1 < M) {
-      product(P, K, r0, r1, mat(P.off_C1, m), vec(X, m + 1), -1.0, 1.0, vec(Y, m),
-              m + 2 < M ? bd(P.off_C2, m) : nullptr, m + 2 < M ? vec(X, m + 2) : nullptr, Bs,
-              part);
-      cluster.sync();
-    }
-    product(P, K, r0, r1, mat(P.off_D, m), vec(Y, m), 1.0, 0.0, vec(X, m), nullptr, nullptr,
-            Bs, part);
-    cluster.sync();
-  }
-}
-
-}  // namespace sweep
-
+// forward sweep of ring_solve with every matrix-vector product over nr right-hand sides. Y is
+// overwritten; W is scratch.
 int ring_solve_multi(const Group& g, int nr, cuDoubleComplex* Y, cuDoubleComplex* X,
                      cuDoubleComplex* W, int64_t mstride, const int* zmap, const int* n_active,
                      cudaStream_t st) {
-  using namespace sweep;
   const Layout& L = g.L;
-  const int K = L.K;
-  if (nr < 1 || nr > kSwMaxRhs) return fail(EB_ERR_ARG, "ring sweep: 1 to 8 right-hand sides");
-  const int R = (K + kSwCluster - 1) / kSwCluster;
-  int rb = 1;
-  while (rb * 32 < R) rb *= 2;
-  if (rb > kSwWarps) return fail(EB_ERR_ARG, "ring sweep: grid too large");
-  const size_t smem = sizeof(double2) * ((size_t)K * nr + (size_t)nr * kSwWarps * 32);
-  if (smem > 220 * 1024) return fail(EB_ERR_ARG, "ring sweep: right-hand sides too large");
-  Params P;
-  P.M = L.M;
-  P.N = L.N;
-  P.nr = nr;
-  P.ws = g.base;
-  P.stride = g.stride;
-  P.blk = L.blk;
-  P.bdr = L.bdr;
-  P.off_D = L.off_D;
-  P.off_L1 = L.off_L1;
-  P.off_C1 = L.off_C1;
-  P.off_B2 = L.off_B2;
-  P.off_C2 = L.off_C2;
-  P.Y = reinterpret_cast<double2*>(Y);
-  P.X = reinterpret_cast<double2*>(X);
-  P.W = reinterpret_cast<double2*>(W);
-  P.mstride = mstride;
-  P.zmap = zmap;
-  P.n_active = n_active;
-  P.row_blocks = rb;
-  if (cudaFuncSetAttribute(k_ring_sweep_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
-    return check_launch("ring sweep attribute");
-  k_ring_sweep_multi<<<dim3(kSwCluster, 1, g.S), kSwThreads, smem, st>>>(P);
-  return check_launch("ring sweep");
+  const int M = L.M, K = L.K;
+  const int64_t es = g.es();
+  auto blk = [&](cuDoubleComplex* base, int m) { return base + (size_t)K * nr * m; };
+  int rc = EB_OK;
+  // C = alpha A B + beta C [- Bd V: the block-diagonal coupling at off_bd, fused into the
+  // product's epilogue]
+  auto gemm = [&](double alpha, const cuDoubleComplex* A, const cuDoubleComplex* B, double beta,
+                  cuDoubleComplex* C, size_t off_bd = 0, const cuDoubleComplex* V = nullptr) {
+    if (rc == EB_OK)
+      rc = dense::zgemm_skinny_batched(K, nr, alpha, A, K, es, B, K, mstride, beta, C, K,
+                                       mstride, g.S, zmap, n_active, st,
+                                       V ? g.base + off_bd : nullptr, g.stride, V, mstride);
+  };
+  for (int m = 0; m < M; ++m) {  // Lt z = b (z in Y), W[m] = Dinv_m z[m]
+    if (m >= 2)
+      gemm(-1.0, g.blk(L.off_L1, m), blk(Y, m - 1), 1.0, blk(Y, m), L.off_B2 + L.bdr * m,
+           blk(W, m - 2));
+    else if (m == 1)
+      gemm(-1.0, g.blk(L.off_L1, m), blk(Y, m - 1), 1.0, blk(Y, m));
+    if (m + 2 < M) gemm(1.0, g.blk(L.off_D, m), blk(Y, m), 0.0, blk(W, m));
+  }
+  for (int m = M - 1; m >= 0; --m) {  // Ut x = z
+    if (m + 2 < M)
+      gemm(-1.0, g.blk(L.off_C1, m), blk(X, m + 1), 1.0, blk(Y, m), L.off_C2 + L.bdr * m,
+           blk(X, m + 2));
+    else if (m + 1 < M)
+      gemm(-1.0, g.blk(L.off_C1, m), blk(X, m + 1), 1.0, blk(Y, m));
+    gemm(1.0, g.blk(L.off_D, m), blk(Y, m), 0.0, blk(X, m));
+  }
+  if (rc != EB_OK) return rc;
+  return check_launch("ring solve multi");
 }
 
 // out = A_{anchor(s)}^-1 in for the systems of one instance (the anchored GMRES preconditioner):
