@@ -70,9 +70,10 @@ def parse_args():
                    help="frequency-response shifts timed one at a time (plain path)")
     p.add_argument("--batched-shifts", type=int, default=64,
                    help="frequency-response shifts timed through the batched driver")
-    p.add_argument("--parts", default="residual,vjp,linear,second_order,resolvent,uneven",
+    p.add_argument("--parts",
+                   default="residual,vjp,linear,second_order,adjoint257,resolvent,uneven",
                    help="comma-separated parts to run besides the residual "
-                        "(vjp, linear, second_order, resolvent, uneven)")
+                        "(vjp, linear, second_order, adjoint257, resolvent, uneven)")
     p.add_argument("--uneven-instances", type=int, default=48)
     p.add_argument("--uneven-sizes", default="65,129,257,513x257",
                    help="O-grid point counts the uneven instances draw from: n (n x n) or "
@@ -887,6 +888,84 @@ def run_b200(args) -> None:
                 (second["value"] / world) / second["cpu_reference_method"]["value"]
         del sd2
 
+    # the adjoint workload at full size: NACA-0012 257x257 O-grid (chord 1, far field 20
+    # chords), Ma 0.6, alpha 2 deg, the PTC state (to rel 1e-4: past 2.8e-5 the reference's PTC
+    # law leaves the basin on this transonic case) plus a seeded 1e-3 perturbation and a smooth
+    # grid-velocity field; each operation per call: the matrix-free VJP of R on the device, and
+    # through the drop-in class (host arrays, the reference's API) the stored-Jacobian VJPs of
+    # R and F, a second-order gradient and the adjoint lift gradient
+    adj257 = None
+    if "adjoint257" in parts:
+        from pyeulerale_b200 import SpatialDiscretization, drivers
+        from pyeulerale_b200 import grid as G
+
+        X7 = G.naca_ogrid(257, 257, thickness=0.12, chord=1.0, far_radius=20.0,
+                          first_spacing=0.01)
+        s7 = SpatialDiscretization(X7, mach_number=0.6, angle_of_attack=2.0,
+                                   coefficient_length=1.0, coefficient_center=(0.25, 0.0))
+        t0 = time.perf_counter()
+        hist7 = drivers.ptc(s7, rtol=1e-4, max_iter=20)
+        t_ptc7 = time.perf_counter() - t0
+        arng = np.random.default_rng(257)
+        s7.states[:] = s7.states * (1.0 + 1e-3 * arng.standard_normal(s7.states.shape))
+        s7.velocities[:] = G.smooth_velocities(X7, arng)
+        s7.compute_odes()
+        s7.compute_forces()
+        t0 = time.perf_counter()
+        s7.linearize()
+        t_lin7 = time.perf_counter() - t0
+        M7, N7 = s7.num_radial, s7.num_angular
+
+        def unit(shape):
+            a = arng.standard_normal(shape) + 1j * arng.standard_normal(shape)
+            return np.asfortranarray(a / np.linalg.norm(a))
+
+        w7, wf7, d7 = unit((4, M7, N7)), unit((2, N7)), unit((4, M7, N7))
+        dw7 = torch.from_numpy(np.ascontiguousarray(w7.ravel(order="F")).view(np.float64)).cuda()
+        g7 = [torch.empty(n, **f64) for n in (8 * M7 * N7, 4 * (M7 + 1) * (N7 + 1),
+                                              4 * (M7 + 1) * (N7 + 1), 2)]
+
+        def matrix_free():
+            s7._call("eb_apply_odes_adjoint", s7._dX.data_ptr(), s7._dV.data_ptr(),
+                     s7._dU.data_ptr(), dw7.data_ptr(), 1, *[g.data_ptr() for g in g7])
+            torch.cuda.synchronize()
+
+        ops = {
+            "vjp_matrix_free": matrix_free,
+            "vjp_states": lambda: s7.apply_odes_wrt_states_rev(w7),
+            "vjp_vertices": lambda: s7.apply_odes_wrt_vertices_rev(w7),
+            "vjp_velocities": lambda: s7.apply_odes_wrt_velocities_rev(w7),
+            "vjp_mach": lambda: s7.apply_odes_wrt_mach_rev(w7),
+            "forces_vjp_states": lambda: s7.apply_forces_wrt_states_rev(wf7),
+            "forces_vjp_vertices": lambda: s7.apply_forces_wrt_vertices_rev(wf7),
+            "second_order_states_states":
+                lambda: s7.compute_odes_wrt_states_inner_product_wrt_states(w7, d7),
+            "adjoint_lift_gradient": lambda: drivers.adjoint_lift_gradient(s7),
+        }
+        times = {}
+        for name, fn in ops.items():
+            fn()
+            barrier()
+            n = 2 if name == "adjoint_lift_gradient" else 5
+            t0 = time.perf_counter()
+            for _ in range(n):
+                fn()
+            barrier()
+            times[name] = max_over_ranks(time.perf_counter() - t0) / n
+        adj257 = {"value": 1.0 / times["vjp_matrix_free"],
+                  "unit": "matrix-free VJPs/s (dR/dU, dR/dX, dR/dV, dR/dMa of <w, R>, one "
+                          "257x257 instance, device arrays)",
+                  "workload": "NACA-0012 257x257 O-grid, Ma 0.6, alpha 2 deg, PTC state + 1e-3 "
+                              "perturbation, smooth grid velocities",
+                  "ms_per_call": {k: v * 1e3 for k, v in times.items()},
+                  "note": "per call through the drop-in class with host arrays in and out, "
+                          "except vjp_matrix_free (device arrays); the adjoint lift gradient "
+                          "includes the ring-LU factorisation at shift 0",
+                  "ptc": {"iterations": hist7.iterations, "final_rel_residual":
+                          hist7.rel_norms[-1], "seconds": t_ptc7},
+                  "linearize_seconds": t_lin7}
+        del s7, g7, dw7
+
     # resolvent: the frequency response of the steady state (PTC from free stream), 64 shifts
     # s = i k V / (c / 2), k log-spaced on [0.01, 10], plus the adjoint lift gradient; batched
     # (anchored GMRES, the headline; and the direct ring LU of every shift, shift_group shifts
@@ -1131,6 +1210,7 @@ def run_b200(args) -> None:
                       "mma_probe": "eb_fp64_mma_probe: 4 CTAs x 8 warps per SM, 8 independent "
                                    f"m8n8k4 FP64 accumulators of {mma_iters} MMAs per warp"},
         "second_order": second,
+        "adjoint257": adj257,
         "resolvent": res,
         "uneven": uneven,
     }
