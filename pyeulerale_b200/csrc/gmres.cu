@@ -42,7 +42,7 @@ int anchored_apply(int M, int N, const void* ringlu_ws, int64_t ringlu_stride, i
                    const int* d_active, const int* d_zmap, const int* d_n_active,
                    cuDoubleComplex* Y, cuDoubleComplex* X, cuDoubleComplex* W, int64_t mstride,
                    const double* in, double* out, int64_t vstride, int accumulate,
-                   cudaStream_t st);
+                   void** graph, cudaStream_t st);
 }  // namespace rl
 
 namespace gm {
@@ -630,6 +630,7 @@ struct Anchored {
   int64_t mstride;
   std::vector<int> sys_anchor;  // host copy
   std::vector<int> zmap;        // host staging of the active anchors
+  void* graph = nullptr;        // the captured sweep (a cudaGraphExec_t), destroyed at the end
 };
 
 // The restarted GMRES of eb_gmres_solve with the block-Jacobi preconditioner (ap == nullptr) or
@@ -705,7 +706,7 @@ int gmres_core(const eb_batch* b, const eb_instance* host_table, const double* J
     return rl::anchored_apply(ap->M, ap->N, ap->ringlu_ws, ap->ringlu_stride, ap->n_anchors,
                               ap->nr, n_sys, ap->d_sys_anchor, ap->d_sys_col, flags,
                               ap->d_zmap, ap->d_n_active, ap->Y, ap->X, ap->W, ap->mstride, in,
-                              out, (int64_t)ap->M * ap->N * 8, accumulate, st_);
+                              out, (int64_t)ap->M * ap->N * 8, accumulate, &ap->graph, st_);
   };
   // the anchored preconditioner works on the anchors that have a system with flags[s]
   auto prec_active = [&](const std::vector<int>& flags) {
@@ -947,8 +948,10 @@ int eb_gmres_solve_anchored(const eb_batch* b, const double* J, int n_sys, const
                       st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return check_launch("gmres anchored setup");
-  return gmres_core(b, nullptr, J, n_sys, nullptr, shifts, 0, rhs, x, opt, workspace,
-                    workspace_bytes, info, stream, &ap);
+  rc = gmres_core(b, nullptr, J, n_sys, nullptr, shifts, 0, rhs, x, opt, workspace,
+                  workspace_bytes, info, stream, &ap);
+  if (ap.graph) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(ap.graph));
+  return rc;
 }
 
 }  // extern "C"

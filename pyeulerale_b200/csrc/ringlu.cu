@@ -1002,18 +1002,53 @@ int ring_solve_multi(const Group& g, int nr, cuDoubleComplex* Y, cuDoubleComplex
 
 // out = A_{anchor(s)}^-1 in for the systems of one instance (the anchored GMRES preconditioner):
 // gather into the anchors' ring blocks, the forward sweeps, scatter to the active systems.
+bool graphs_enabled();
+int ptc_stream(cudaStream_t& out);
+
+// The sweep's launch sequence depends only on the buffers, the factors and the sizes (the active
+// anchors are read on the device), so the first apply of a solve captures it into a CUDA graph
+// (*graph) that every later apply replays: one launch instead of 2 (2 M - 1). The caller
+// destroys the graph when the solve ends. With EB_RINGLU_GRAPHS=0, or if the capture fails, the
+// sweep is launched directly.
+int sweep_graph(const Group& g, int nr, cuDoubleComplex* Y, cuDoubleComplex* X,
+                cuDoubleComplex* W, int64_t mstride, const int* zmap, const int* n_active,
+                void** graph, cudaStream_t st) {
+  if (!graph || !graphs_enabled())
+    return ring_solve_multi(g, nr, Y, X, W, mstride, zmap, n_active, st);
+  if (!*graph) {
+    cudaStream_t cs = nullptr;
+    int rc = ptc_stream(cs);
+    if (rc != EB_OK) return rc;
+    cudaGraph_t gr = nullptr;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+      const int rc_cap = ring_solve_multi(g, nr, Y, X, W, mstride, zmap, n_active, cs);
+      const cudaError_t e = cudaStreamEndCapture(cs, &gr);
+      cudaGraphExec_t ex = nullptr;
+      if (rc_cap == EB_OK && e == cudaSuccess && gr &&
+          cudaGraphInstantiate(&ex, gr, 0) == cudaSuccess)
+        *graph = ex;
+      if (gr) cudaGraphDestroy(gr);
+    }
+    cudaGetLastError();  // a failed capture leaves no error behind: the direct launches follow
+  }
+  if (!*graph) return ring_solve_multi(g, nr, Y, X, W, mstride, zmap, n_active, st);
+  if (cudaGraphLaunch(static_cast<cudaGraphExec_t>(*graph), st) != cudaSuccess)
+    return check_launch("anchored sweep graph");
+  return EB_OK;
+}
+
 int anchored_apply(int M, int N, const void* ringlu_ws, int64_t ringlu_stride, int n_anchors,
                    int nr, int n_sys, const int* d_sys_anchor, const int* d_sys_col,
                    const int* d_active, const int* d_zmap, const int* d_n_active,
                    cuDoubleComplex* Y, cuDoubleComplex* X, cuDoubleComplex* W, int64_t mstride,
                    const double* in, double* out, int64_t vstride, int accumulate,
-                   cudaStream_t st) {
+                   void** graph, cudaStream_t st) {
   const Group g{plan(M, N), static_cast<char*>(const_cast<void*>(ringlu_ws)), ringlu_stride,
                 n_anchors};
   const int gc = grid_for((int64_t)M * N, 128) / 4 + 1;
   k_sys_to_multi<<<dim3(gc, n_sys), 128, 0, st>>>(M, N, nr, n_sys, d_sys_anchor, d_sys_col, in,
                                                   vstride, Y, mstride);
-  int rc = ring_solve_multi(g, nr, Y, X, W, mstride, d_zmap, d_n_active, st);
+  int rc = sweep_graph(g, nr, Y, X, W, mstride, d_zmap, d_n_active, graph, st);
   if (rc != EB_OK) return rc;
   k_multi_to_sys<<<dim3(gc, n_sys), 128, 0, st>>>(M, N, nr, n_sys, d_sys_anchor, d_sys_col,
                                                   d_active, X, mstride, out, vstride,

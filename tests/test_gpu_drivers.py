@@ -83,6 +83,27 @@ def test_anchored_gmres_residuals_and_fallback(solver, cuda):
     assert not all(i["converged"] for i in info), info
 
 
+def test_anchored_sweep_graph_matches_direct_launches(solver, cuda, monkeypatch):
+    """The anchored preconditioner's sweep replayed from its CUDA graph gives the same bits as
+    the sweep launched directly (EB_RINGLU_GRAPHS=0)."""
+    from pyeulerale_b200.solver import RingLUMany, anchor_shifts, solve_anchored
+
+    M, N = solver.num_radial, solver.num_angular
+    rng = np.random.default_rng(21)
+    shifts = 1j * np.logspace(-1, -0.6, 6)
+    rhs = cuda.from_numpy(rng.standard_normal((6, 8 * M * N))).cuda()
+    anchors, sa = anchor_shifts(shifts, 3)
+    lu = RingLUMany(solver._batch(), capacity=len(anchors))
+    lu.factor(solver._dJ_u, anchors)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("EB_RINGLU_GRAPHS", flag)
+        x, info = solve_anchored(solver._batch(), solver._dJ_u, rhs, shifts, lu, sa)
+        out.append((x.cpu().numpy(), info.iterations))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+
+
 def test_adjoint_lift_gradient_dot_product(solver):
     """<dc_l/dX, dX> (one adjoint solve) == the forward tangent of c_l along dX."""
     from pyeulerale_b200 import drivers
