@@ -350,8 +350,8 @@ def _device_apply(solver, name: str, jac, x, out_numel: int):
 def frequency_response_batched(solver, chord: float, axis_location: float,
                                reduced_frequencies, group: int = 16,
                                tol: float = 1e-10, method: str = "direct",
-                               per_anchor: int = 4,
-                               stats: dict | None = None) -> tuple[np.ndarray, np.ndarray]:
+                               per_anchor: int = 3, stats: dict | None = None,
+                               lift_gradient: bool = False):
     """``frequency_response`` with the shifts factored and solved together on the device.
 
     The pitch-to-(c_l, c_m) transfer function at s = i k V_inf / (c/2) for every reduced
@@ -368,6 +368,10 @@ def frequency_response_batched(solver, chord: float, axis_location: float,
     (``solver.solve_anchored``) to tol / 100; a shift whose GMRES does not converge is solved
     directly.
     ``stats`` (optional dict) receives the anchored solve's iteration counts.
+
+    ``lift_gradient=True`` (anchored method) also returns the adjoint lift gradient
+    (``adjoint_lift_gradient``): shift 0 is factored in the same batched call as the anchors and
+    its adjoint solve uses those factors. Returns ``(cl, cm)`` or ``(cl, cm, gradient)``.
     """
     import torch
 
@@ -417,13 +421,22 @@ def frequency_response_batched(solver, chord: float, axis_location: float,
     if method != "anchored":
         raise ValueError(f"unknown method {method!r}")
     anchors, sys_anchor = anchor_shifts(shifts, per_anchor)
-    lu = RingLUMany(solver._batch(), capacity=len(anchors), tol=tol)
-    lu.factor(solver._dJ_u, anchors)
+    factored = list(anchors) + ([0.0] if lift_gradient else [])  # shift 0: the adjoint's
+    lu = RingLUMany(solver._batch(), capacity=len(factored), tol=tol)
+    lu.factor(solver._dJ_u, factored)
     # GMRES to tol / 100: the direct solves stop at tol too, and two solutions within tol of
     # the same system differ by the system's conditioning times tol; the margin keeps the
     # transfer function within ~tol of the direct one
     x, info = solve_anchored(solver._batch(), solver._dJ_u, rhs_of(shifts), shifts, lu,
                              sys_anchor, tol=tol * 1e-2, raise_on_failure=False)
+    grad = None
+    if lift_gradient:  # the adjoint lift gradient on the shift-0 factors, before any re-factoring
+        g = solver.compute_lift_coefficient_wrt_forces().astype(complex)
+        b = solver._cvec(solver.apply_forces_wrt_states_rev(d_forces=g))
+        lam, _ = lu.solve_one(len(anchors), b, adjoint=True)
+        lam_h = np.reshape(lam.cpu().numpy().view(np.complex128), solver.odes.shape, order="F")
+        grad = np.asfortranarray((solver.apply_forces_wrt_vertices_rev(d_forces=g)
+                                  - solver.apply_odes_wrt_vertices_rev(d_odes=lam_h)).real)
     bad = [k for k, i in enumerate(info) if not i["converged"]]
     for g0 in range(0, len(bad), lu.capacity):  # direct solves of the unconverged shifts
         idx = bad[g0:g0 + lu.capacity]
@@ -435,7 +448,7 @@ def frequency_response_batched(solver, chord: float, axis_location: float,
     if stats is not None:
         stats.update(anchors=len(anchors), iterations=info.iterations, direct=len(bad))
     coefficients(np.arange(len(shifts)), x)
-    return cl, cm
+    return (cl, cm, grad) if lift_gradient else (cl, cm)
 
 
 def adjoint_lift_gradient(solver) -> np.ndarray:

@@ -331,6 +331,25 @@ class RingLUMany:
                                       self._lib.eb_last_error().decode())
         self.J = Js
 
+    def solve_one(self, k: int, rhs, adjoint: bool = False):
+        """Solves the system of shift ``k`` alone (``eb_ringlu_solve`` on its workspace) for one
+        device right-hand side; returns ``(x, rel_residual)``."""
+        if self.J is None or not 0 <= k < len(self.shifts):
+            raise ValueError("no factors for that shift")
+        torch = self._torch
+        x = torch.empty_like(rhs)
+        rel = ctypes.c_double()
+        s = self.shifts[k]
+        rc = self._lib.eb_ringlu_solve(ctypes.byref(self.batch), self.J[k].data_ptr(), s.real,
+                                       s.imag, 1 if adjoint else 0,
+                                       self.workspace.data_ptr() + k * self.stride, self.stride,
+                                       rhs.data_ptr(), x.data_ptr(), self.tol, self.max_refine,
+                                       ctypes.byref(rel),
+                                       torch.cuda.current_stream().cuda_stream)
+        if rc != _lib.EB_OK:
+            raise _lib.EulerB200Error("eb_ringlu_solve", rc, self._lib.eb_last_error().decode())
+        return x, rel.value
+
     def solve(self, rhs, adjoint: bool = False, out=None):
         """Solves system ``s`` for ``rhs[s]`` (a sequence of, or a stacked, device tensor);
         returns ``(x, rel_residuals)`` with ``x`` stacked like ``rhs``."""

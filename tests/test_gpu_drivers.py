@@ -56,6 +56,20 @@ def test_frequency_response_anchored_matches_direct(solver, per_anchor):
         assert max(stats["iterations"]) <= 5 and stats["direct"] == 0, stats
 
 
+def test_anchored_lift_gradient_matches_adjoint_driver(solver):
+    """The lift gradient from the shift-0 factors of the anchored call equals
+    adjoint_lift_gradient's, and the transfer function is the one without it."""
+    from pyeulerale_b200 import drivers
+
+    ks = np.logspace(-2, 1, 9)
+    cl, cm, grad = drivers.frequency_response_batched(solver, 1.0, 0.25, ks, method="anchored",
+                                                      lift_gradient=True)
+    cl0, cm0 = drivers.frequency_response_batched(solver, 1.0, 0.25, ks, method="anchored")
+    assert rel_err(cl, cl0) <= 1e-10 and rel_err(cm, cm0) <= 1e-10
+    ref = drivers.adjoint_lift_gradient(solver)
+    assert rel_err(grad, ref) <= 1e-9, rel_err(grad, ref)
+
+
 def test_anchored_gmres_residuals_and_fallback(solver, cuda):
     """solve_anchored reports true residuals at the tolerance; with an iteration limit too small
     to converge it returns EB_ERR_NOCONV per system (no exception), and the driver's direct
