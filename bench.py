@@ -470,7 +470,7 @@ def time_zgemm(K: int, batch: int, stream, sp, reps: int = 10) -> dict:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / reps
 
-    for v, name in ((0, "register_staged"), (1, "cp_async")):
+    for v, name in ((0, "register_staged"), (1, "cp_async"), (2, "cp_async_64x32")):
         def call(v=v):
             _lib.call("eb_zgemm_strided_batched", K, K, K, -1.0, A.data_ptr(), K, K * K,
                       B.data_ptr(), K, K * K, 1.0, C.data_ptr(), K, K * K, batch, v, sp)

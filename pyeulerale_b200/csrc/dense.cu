@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "../../include/euler_b200.h"
 #include "dense.cuh"
@@ -186,16 +187,18 @@ __global__ void __launch_bounds__(kGemmThreads)
       }
 }
 
-// ---- cp.async variant -------------------------------------------------------------------
-constexpr int kStages = 3;
+// ---- cp.async variants --------------------------------------------------------------------
 // pitches in complex elements: A rows [k][m] 2 modulo 8, B rows [n][k] 4 modulo 8, so that the
 // 16-byte fragment loads of each quarter-warp fall on distinct banks
 constexpr int kPitchA = kBM + 2;
 constexpr int kPitchB = kBK + 4;
 
+// BN: tile columns (64: warps of 32 x 32; 32: warps of 32 x 16, half the registers and shared
+// memory, four CTAs per SM, twice the tiles); Stages: slices in flight.
+template <int BN, int Stages>
 struct AsyncSmem {
-  double2 a[kStages][kBK][kPitchA];
-  double2 b[kStages][kBN][kPitchB];
+  double2 a[Stages][kBK][kPitchA];
+  double2 b[Stages][BN][kPitchB];
 };
 
 // 16-byte global -> shared copy; valid == false fills zeros (src is then not read).
@@ -213,31 +216,34 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(Pending) : "memory");
 }
 
+template <int BN, int Stages>
 __global__ void __launch_bounds__(kGemmThreads)
     k_zgemm_nn_async(int M, int N, int K, double alpha, const double2* A, int lda, int64_t sa,
                      const double2* B, int ldb, int64_t sb, double beta, double2* C, int ldc,
                      int64_t sc) {
+  constexpr int NJ = BN / 16;                        // 8-column fragments per warp
+  constexpr int kBPerT = kBK * BN / kGemmThreads;   // B elements per thread and slice
   extern __shared__ __align__(16) unsigned char zg_smem[];
-  AsyncSmem& S = *reinterpret_cast<AsyncSmem*>(zg_smem);
+  AsyncSmem<BN, Stages>& S = *reinterpret_cast<AsyncSmem<BN, Stages>*>(zg_smem);
   const int64_t z = blockIdx.z;
   A += sa * z;
   B += sb * z;
   C += sc * z;
   const int tid = threadIdx.x;
-  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
   const int lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * (BN / 2);
   const int fr = lane >> 2, fc = lane & 3;
-  double re[4][4][2], im[4][4][2];
+  double re[4][NJ][2], im[4][NJ][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
+    for (int j = 0; j < NJ; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
   const int slices = (K + kBK - 1) / kBK;
-  // slice s into buffer s % kStages (one commit group per call, empty past the last slice)
+  // slice s into buffer s % Stages (one commit group per call, empty past the last slice)
   auto issue = [&](int s) {
     if (s < slices) {
-      const int buf = s % kStages, k0 = s * kBK;
+      const int buf = s % Stages, k0 = s * kBK;
 #pragma unroll
       for (int q = 0; q < kAPer; ++q) {  // A: consecutive threads along m
         const int e = tid + kGemmThreads * q, m = e % kBM, k = e / kBM;
@@ -246,7 +252,7 @@ __global__ void __launch_bounds__(kGemmThreads)
         cp_async16(&S.a[buf][k][m], ok ? A + gm + (int64_t)lda * gk : A, ok);
       }
 #pragma unroll
-      for (int q = 0; q < kBPer; ++q) {  // B: consecutive threads along k
+      for (int q = 0; q < kBPerT; ++q) {  // B: consecutive threads along k
         const int e = tid + kGemmThreads * q, k = e % kBK, n = e / kBK;
         const int gk = k0 + k, gn = n0 + n;
         const bool ok = gk < K && gn < N;
@@ -256,15 +262,15 @@ __global__ void __launch_bounds__(kGemmThreads)
     cp_async_commit();
   };
 #pragma unroll
-  for (int s = 0; s < kStages - 1; ++s) issue(s);
+  for (int s = 0; s < Stages - 1; ++s) issue(s);
   for (int s = 0; s < slices; ++s) {
-    cp_async_wait<kStages - 2>();  // slice s has landed (this thread's copies)
-    __syncthreads();               // ... everyone's; and slice s - 1's buffer is free
-    issue(s + kStages - 1);
-    const int buf = s % kStages;
+    cp_async_wait<Stages - 2>();  // slice s has landed (this thread's copies)
+    __syncthreads();              // ... everyone's; and slice s - 1's buffer is free
+    issue(s + Stages - 1);
+    const int buf = s % Stages;
 #pragma unroll
     for (int kk = 0; kk < kBK; kk += 4) {
-      double2 a[4], b[4];
+      double2 a[4], b[NJ];
       double a_n[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -272,18 +278,18 @@ __global__ void __launch_bounds__(kGemmThreads)
         a_n[i] = -a[i].y;
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = S.b[buf][wn + 8 * j + fr][kk + fc];
+      for (int j = 0; j < NJ; ++j) b[j] = S.b[buf][wn + 8 * j + fr][kk + fc];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < NJ; ++j) {
           mma884(re[i][j], a[i].x, b[j].x);
           mma884(im[i][j], a[i].x, b[j].y);
         }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < NJ; ++j) {
           mma884(re[i][j], a_n[i], b[j].y);
           mma884(im[i][j], a[i].y, b[j].x);
         }
@@ -293,7 +299,7 @@ __global__ void __launch_bounds__(kGemmThreads)
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int gm = m0 + wm + 8 * i + fr, gn = n0 + wn + 8 * j + 2 * fc + h;
@@ -317,13 +323,21 @@ int zgemm_nn_batched(int M, int N, int K, double alpha, const cuDoubleComplex* A
                      double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,
                      cudaStream_t st, int variant) {
   if (M <= 0 || N <= 0 || batch <= 0) return 0;
-  if (variant < 0) variant = kDefaultVariant;
-  auto kernel = variant == kAsync ? k_zgemm_nn_async : k_zgemm_nn;
-  const int smem = variant == kAsync ? (int)sizeof(AsyncSmem) : (int)sizeof(GemmSmem);
+  if (variant < 0) {  // the default, or EB_ZGEMM=v<k> (measurements of the variants in place)
+    const char* e = std::getenv("EB_ZGEMM");
+    variant = (e && e[0] == 'v' && e[1] >= '0' && e[1] <= '2') ? e[1] - '0' : kDefaultVariant;
+  }
+  auto kernel = variant == kAsync      ? k_zgemm_nn_async<64, 3>
+                : variant == kAsyncNarrow ? k_zgemm_nn_async<32, 2>
+                                          : k_zgemm_nn;
+  const int smem = variant == kAsync        ? (int)sizeof(AsyncSmem<64, 3>)
+                   : variant == kAsyncNarrow ? (int)sizeof(AsyncSmem<32, 2>)
+                                             : (int)sizeof(GemmSmem);
+  const int bn = variant == kAsyncNarrow ? 32 : kBN;
   if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return check_launch("zgemm attribute");
-  const dim3 grid((M + kBM - 1) / kBM, (N + kBN - 1) / kBN, batch);
+  const dim3 grid((M + kBM - 1) / kBM, (N + bn - 1) / bn, batch);
   kernel<<<grid, kGemmThreads, smem, st>>>(
       M, N, K, alpha, reinterpret_cast<const double2*>(A), lda, stride_a,
       reinterpret_cast<const double2*>(B), ldb, stride_b, beta, reinterpret_cast<double2*>(C),
@@ -624,7 +638,7 @@ extern "C" int eb_zgemm_strided_batched(int M, int N, int K, double alpha, const
                                         int64_t stride_b, double beta, double* C, int ldc,
                                         int64_t stride_c, int batch, int variant, void* stream) {
   if (M < 0 || N < 0 || K < 0 || batch < 0 || lda < (M > 1 ? M : 1) ||
-      ldb < (K > 1 ? K : 1) || ldc < (M > 1 ? M : 1) || variant < -1 || variant > 1 ||
+      ldb < (K > 1 ? K : 1) || ldc < (M > 1 ? M : 1) || variant < -1 || variant > 2 ||
       (M > 0 && N > 0 && batch > 0 && (!A || !B || !C)))
     return eb::fail(EB_ERR_ARG, "zgemm: bad sizes, leading dimensions, variant or pointers");
   return eb::dense::zgemm_nn_batched(

@@ -10,13 +10,14 @@
 namespace eb {
 namespace dense {
 
-// GEMM kernel variants (identical results): register-staged double buffer, cp.async ring.
-constexpr int kStaged = 0, kAsync = 1;
+// GEMM kernel variants (identical results): register-staged double buffer, cp.async ring of
+// three slices on 64 x 64 tiles, cp.async ring of two slices on 64 x 32 tiles (four CTAs per SM).
+constexpr int kStaged = 0, kAsync = 1, kAsyncNarrow = 2;
 constexpr int kDefaultVariant = kAsync;
 
 // C_z = alpha A_z B_z + beta C_z for z < batch, column-major, A_z = A + z stride_a (elements)
-// etc.; alpha, beta real; beta == 0 does not read C. variant < 0 takes the default. Returns an
-// EB_* status.
+// etc.; alpha, beta real; beta == 0 does not read C. variant < 0 takes the default (or the one
+// EB_ZGEMM=v<k> names). Returns an EB_* status.
 int zgemm_nn_batched(int M, int N, int K, double alpha, const cuDoubleComplex* A, int lda,
                      int64_t stride_a, const cuDoubleComplex* B, int ldb, int64_t stride_b,
                      double beta, cuDoubleComplex* C, int ldc, int64_t stride_c, int batch,

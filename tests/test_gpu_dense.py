@@ -40,11 +40,12 @@ def test_zgemm_matches_numpy_and_variants_agree(cuda, M, N, K, alpha, beta):
     batch = 3
     A, B, C = crandn(rng, (batch, M, K)), crandn(rng, (batch, K, N)), crandn(rng, (batch, M, N))
     want = alpha * np.einsum("zmk,zkn->zmn", A, B) + beta * C
-    got = [zgemm(cuda, M, N, K, alpha, A, B, beta, C, v) for v in (0, 1)]
+    got = [zgemm(cuda, M, N, K, alpha, A, B, beta, C, v) for v in (0, 1, 2)]
     scale = np.sqrt(K) * np.max(np.abs(want))
     for g in got:
         assert np.max(np.abs(g - want)) <= 1e-14 * scale
     np.testing.assert_array_equal(got[0], got[1])
+    np.testing.assert_array_equal(got[0], got[2])
     np.testing.assert_array_equal(zgemm(cuda, M, N, K, alpha, A, B, beta, C, -1), got[1])
 
 
@@ -53,7 +54,7 @@ def test_zgemm_beta_zero_ignores_c(cuda):
     rng = np.random.default_rng(5)
     A, B = crandn(rng, (2, 40, 24)), crandn(rng, (2, 24, 72))
     C = np.full((2, 40, 72), np.nan + 0j)
-    for v in (0, 1):
+    for v in (0, 1, 2):
         got = zgemm(cuda, 40, 72, 24, 1.0, A, B, 0.0, C, v)
         assert np.all(np.isfinite(got))
 
@@ -64,7 +65,7 @@ def test_zgemm_bad_arguments_rejected(cuda):
     t = cuda.zeros(64, dtype=cuda.float64, device="cuda")
     p = t.data_ptr()
     for args in [(4, 4, 4, 1.0, p, 3, 16, p, 4, 16, 0.0, p, 4, 16, 1, 0),   # lda < M
-                 (4, 4, 4, 1.0, p, 4, 16, p, 4, 16, 0.0, p, 4, 16, 1, 2),   # variant
+                 (4, 4, 4, 1.0, p, 4, 16, p, 4, 16, 0.0, p, 4, 16, 1, 3),   # variant
                  (-1, 4, 4, 1.0, p, 4, 16, p, 4, 16, 0.0, p, 4, 16, 1, 0)]:  # size
         with pytest.raises(_lib.EulerB200Error) as err:
             _lib.call("eb_zgemm_strided_batched", *args, None)
