@@ -332,7 +332,7 @@ int eb_fp64_mma_probe(int64_t iterations, int sms, double* sink, void* stream);
 /* The ring LU's dense product as a library call: C_z = alpha A_z B_z + beta C_z for z < batch,
  * complex double (interleaved), column-major, no transposes, A_z = A + z stride_a complex
  * elements (likewise B, C); alpha and beta real, beta == 0 does not read C. variant: -1 the
- * default, 0 the register-staged double buffer, 1 the cp.async three-stage ring on 64 x 64
+ * default (2), 0 the register-staged double buffer, 1 the cp.async three-stage ring on 64 x 64
  * tiles, 2 a two-stage ring on 64 x 32 tiles (identical results). In the reference the dense products of its solves are SuperLU's and BLAS's
  * (core.py:533-599). */
 int eb_zgemm_strided_batched(int M, int N, int K, double alpha, const double* A, int lda,

@@ -13,7 +13,7 @@ namespace dense {
 // GEMM kernel variants (identical results): register-staged double buffer, cp.async ring of
 // three slices on 64 x 64 tiles, cp.async ring of two slices on 64 x 32 tiles (four CTAs per SM).
 constexpr int kStaged = 0, kAsync = 1, kAsyncNarrow = 2;
-constexpr int kDefaultVariant = kAsync;
+constexpr int kDefaultVariant = kAsyncNarrow;  // 32.5 against 26.3 TFLOP/s on 512^3 x 16
 
 // C_z = alpha A_z B_z + beta C_z for z < batch, column-major, A_z = A + z stride_a (elements)
 // etc.; alpha, beta real; beta == 0 does not read C. variant < 0 takes the default (or the one
