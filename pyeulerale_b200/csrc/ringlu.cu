@@ -1007,7 +1007,7 @@ int ptc_stream(cudaStream_t& out);
 
 // The sweep's launch sequence depends only on the buffers, the factors and the sizes (the active
 // anchors are read on the device), so the first apply of a solve captures it into a CUDA graph
-// (*graph) that every later apply replays: one launch instead of 2 (2 M - 1). The caller
+// (*graph) that every later apply replays: one launch instead of 4 (M - 1). The caller
 // destroys the graph when the solve ends. With EB_RINGLU_GRAPHS=0, or if the capture fails, the
 // sweep is launched directly.
 int sweep_graph(const Group& g, int nr, cuDoubleComplex* Y, cuDoubleComplex* X,
